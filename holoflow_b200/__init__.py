@@ -1,0 +1,126 @@
+"""holoflow_b200: B200 (sm_100a) laser Doppler reconstruction — Python binding of the C ABI.
+
+The product is the shared library ``_lib/libholoflow_b200.so`` (CUDA kernels + C ABI declared in
+``include/holoflow_b200.h`` + the C++ node layer).  This module only loads it with ctypes and
+declares the prototypes; every call goes straight through the C ABI.  There is no fallback: if the
+library is missing or cannot be loaded, importing this package raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "_lib" / "libholoflow_b200.so"
+
+# status codes / enums (include/holoflow_b200.h)
+HF_OK, HF_ERR_INVALID, HF_ERR_CUDA, HF_ERR_UNSUPPORTED, HF_ERR_NOMEM, HF_ERR_TIMEOUT = 0, -1, -2, -3, -4, -5
+HF_ERR_STATE, HF_ERR_CANCELLED = -6, -7
+HF_U8, HF_U16, HF_F32, HF_CF32, HF_MONO12P = 0, 1, 2, 3, 16
+HF_CONV_REAL, HF_CONV_SCALED, HF_CONV_MODULUS, HF_CONV_ARGUMENT = 0, 1, 2, 3
+HF_NORM_BACKWARD, HF_NORM_FORWARD, HF_NORM_ORTHO = 0, 1, 2
+HF_PROP_NONE, HF_PROP_FRESNEL, HF_PROP_ANGULAR_SPECTRUM = 0, 1, 2
+HF_M0, HF_M1, HF_M2 = 1, 2, 4
+HF_FORM_PLAIN, HF_FORM_CHOSEN = 0, 1
+
+
+class HfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class HfDesc(C.Structure):
+    _fields_ = [
+        ("height", C.c_int32), ("width", C.c_int32), ("frames", C.c_int32), ("hop", C.c_int32),
+        ("z_begin", C.c_int32), ("z_end", C.c_int32), ("input_dtype", C.c_int32),
+        ("propagation", C.c_int32), ("clutter_rank", C.c_int32), ("moment_mask", C.c_int32),
+        ("fftshift", C.c_int32), ("form", C.c_int32), ("max_batch", C.c_int32),
+        ("lambda_", C.c_float), ("pitch", C.c_float), ("z", C.c_float), ("fs", C.c_float),
+        ("pad_w", C.c_int32), ("pad_h", C.c_int32), ("as_filter", C.c_int32),
+        ("r_inner", C.c_uint32), ("r_outer", C.c_uint32), ("s_inner", C.c_uint32),
+        ("s_outer", C.c_uint32),
+    ]
+
+
+_vp, _i32, _i64, _f32, _sz = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_size_t
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "hf_last_error": (C.c_char_p, []),
+    "hf_version": (C.c_int, []),
+    "hf_launch_count": (_i64, []),
+    "hf_reset_launch_count": (None, []),
+    "hf_unpack12": (C.c_int, [_vp, _vp, C.c_int, _i64, _vp]),
+    "hf_pack12": (C.c_int, [_vp, _vp, _i64, _vp]),
+    "hf_convert": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, _i64, _vp, _vp]),
+    "hf_temporal_dft": (C.c_int, [_vp, C.c_int, _i64, C.c_int, _i64, C.c_int, C.c_int, C.c_int, _vp, _vp]),
+    "hf_covariance_workspace_bytes": (_sz, [C.c_int, _i64]),
+    "hf_covariance": (C.c_int, [_vp, C.c_int, _i64, C.c_int, _i64, _vp, _vp, _vp]),
+    "hf_eigh_jacobi_f64": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _i64, _vp]),
+    "hf_pca_project": (C.c_int, [_vp, _i64, C.c_int, _i64, _vp, C.c_int, C.c_int, _vp, _vp]),
+    "hf_band_matrix": (C.c_int, [_vp, _i64, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),
+    "hf_fresnel_plan_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_int, _f32, _f32, _f32, C.c_int,
+                                         C.c_int, C.POINTER(_vp), _vp]),
+    "hf_fresnel_plan_set_z": (C.c_int, [_vp, _f32, _vp]),
+    "hf_fresnel_exec": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _vp, _i64, _i64, _i64, _vp]),
+    "hf_fresnel_plan_destroy": (C.c_int, [_vp]),
+    "hf_as_plan_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_int, _f32, _f32, _f32, C.c_int, C.c_int,
+                                    C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.POINTER(_vp), _vp]),
+    "hf_as_exec": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "hf_as_plan_destroy": (C.c_int, [_vp]),
+    "hf_mean_axis": (C.c_int, [_vp, C.c_int, _i64, _i64, _i64, _vp, _vp]),
+    "hf_mean_abs_axis": (C.c_int, [_vp, C.c_int, _i64, _i64, _i64, _vp, _vp]),
+    "hf_band_moments": (C.c_int, [_vp, C.c_int, C.c_int, _i64, C.POINTER(C.c_float), C.c_int, _vp, _vp]),
+    "hf_plan_create": (C.c_int, [C.POINTER(HfDesc), C.POINTER(_vp), _vp]),
+    "hf_plan_destroy": (C.c_int, [_vp]),
+    "hf_plan_set_z": (C.c_int, [_vp, _f32, _vp]),
+    "hf_plan_output_shape": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
+    "hf_plan_device_bytes": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "hf_pipeline_exec": (C.c_int, [_vp, _vp, _i64, _i64, C.c_int, _vp, _vp]),
+    "hf_pipeline_inspect": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+}
+
+_lib = None
+
+
+def load(path: os.PathLike | str | None = None) -> C.CDLL:
+    """Load the shared library (raises if it is absent: there is no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"holoflow_b200: {p} not built (run __graft_entry__.build())")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue  # symbol checks are done by the tests
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def lib() -> C.CDLL:
+    return load()
+
+
+def check(rc: int) -> None:
+    if rc != HF_OK:
+        raise HfError(rc, lib().hf_last_error().decode(errors="replace"))
+
+
+def declared_symbols(header: os.PathLike | str | None = None) -> list[str]:
+    """Every hf_* function declared in include/*.h (parsed from the header text)."""
+    import re
+    root = _HERE.parent / "include"
+    names: list[str] = []
+    files = [pathlib.Path(header)] if header else sorted(root.glob("*.h"))
+    for h in files:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"\b(hf_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))

@@ -1,0 +1,38 @@
+// Launch interface of the PCA / SVD-clutter-filter kernels (k_pca.cu).
+#pragma once
+
+#include "frames.cuh"
+
+namespace hf {
+
+// Per-window Gram matrix of the frames, G = X^T X (T x T, float64), X = [T][P].
+//  partial: float32 [nwin][nblk][T*T] block partials of the shifted Gram, and
+//  sums:    float64 [nwin][nblk][T] exact per-frame sums used to undo the shift.
+struct CovArgs {
+  FrameRing ring;
+  int       T;
+  int64_t   P;
+  float     shift;   // samples are accumulated as (x - shift); 2048 for 12-bit data
+  float    *partial;
+  double   *sums;
+  int       nblk;    // CTAs per window (partials per window)
+};
+
+size_t cov_workspace_bytes(int T, int64_t P, int nwin);
+// Full Gram computation: block partials -> deterministic float64 reduction -> gram[nwin][T][T].
+int launch_covariance(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, void *ws,
+                      double *gram, cudaStream_t s);
+
+// FP64 cyclic Jacobi, one CTA per matrix (n <= 128).  Eigenvalues ascending, eigenvector j in
+// column j of evecs (row-major).
+int launch_jacobi(const double *a, double *evecs, double *evals, int *info, int n, int64_t batch,
+                  cudaStream_t s);
+
+// W = (I - V V^T) D[:, z0:z1] as complex64 [batch][T][nz]; V = last `rank` columns of evecs.
+int launch_band_matrix(const double *evecs, int64_t batch, int T, int rank, int z0, int z1,
+                       float2 *wmat, cudaStream_t s);
+
+int launch_pca_project(const float *in, int64_t batch, int T, int64_t P, const double *evecs,
+                       int begin, int end, float *out, cudaStream_t s);
+
+} // namespace hf

@@ -1,0 +1,202 @@
+"""Python wrappers over the C ABI for device tensors (torch is used for device memory and streams
+only).  Each wrapper mirrors one C entry point; errors raise :class:`holoflow_b200.HfError`."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import torch
+
+from . import (HF_CF32, HF_F32, HF_M0, HF_M1, HF_M2, HF_MONO12P, HF_PROP_FRESNEL, HF_U16, HF_U8,
+               HfDesc, check, lib)
+
+_DT = {torch.uint8: HF_U8, torch.int16: HF_U16, torch.float32: HF_F32, torch.complex64: HF_CF32}
+
+
+def _stream(stream: Optional[torch.cuda.Stream] = None) -> C.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ptr(t: Optional[torch.Tensor]) -> C.c_void_p:
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def unpack12(packed: torch.Tensor, npix: int, out_dtype: int = HF_F32, out: Optional[torch.Tensor] = None):
+    if out is None:
+        shape, dt = (npix,), {HF_U16: torch.int16, HF_F32: torch.float32, HF_CF32: torch.complex64}[out_dtype]
+        out = torch.empty(shape, dtype=dt, device=packed.device)
+    check(lib().hf_unpack12(_ptr(packed), _ptr(out), out_dtype, npix, _stream()))
+    return out
+
+
+def pack12(values_u16: torch.Tensor) -> torch.Tensor:
+    n = values_u16.numel()
+    out = torch.empty(n * 3 // 2, dtype=torch.uint8, device=values_u16.device)
+    check(lib().hf_pack12(_ptr(values_u16), _ptr(out), n, _stream()))
+    return out
+
+
+def temporal_dft(frames: torch.Tensor, dtype: int, batch: int, T: int, P: int, z0: int, z1: int,
+                 norm: int = 0) -> torch.Tensor:
+    out = torch.empty((batch, z1 - z0, P), dtype=torch.complex64, device=frames.device)
+    check(lib().hf_temporal_dft(_ptr(frames), dtype, batch, T, P, z0, z1, norm, _ptr(out), _stream()))
+    return out
+
+
+def covariance(frames: torch.Tensor, dtype: int, batch: int, T: int, P: int) -> torch.Tensor:
+    ws_bytes = lib().hf_covariance_workspace_bytes(T, P) * batch
+    ws = torch.empty(max(ws_bytes, 16), dtype=torch.uint8, device=frames.device)
+    gram = torch.empty((batch, T, T), dtype=torch.float64, device=frames.device)
+    check(lib().hf_covariance(_ptr(frames), dtype, batch, T, P, _ptr(gram), _ptr(ws), _stream()))
+    return gram
+
+
+def eigh_jacobi(a: torch.Tensor):
+    batch, n, _ = a.shape
+    evecs = torch.empty_like(a)
+    evals = torch.empty((batch, n), dtype=torch.float64, device=a.device)
+    info = torch.empty((batch,), dtype=torch.int32, device=a.device)
+    check(lib().hf_eigh_jacobi_f64(_ptr(a.contiguous()), _ptr(evecs), _ptr(evals), _ptr(info), n, batch,
+                                   _stream()))
+    return evals, evecs, info
+
+
+@dataclass
+class PipelineConfig:
+    height: int
+    width: int
+    frames: int
+    hop: int
+    z_begin: int
+    z_end: int
+    input_dtype: int = HF_MONO12P
+    propagation: int = HF_PROP_FRESNEL
+    clutter_rank: int = 0
+    moment_mask: int = HF_M0 | HF_M1 | HF_M2
+    fftshift: int = 0
+    form: int = 0
+    max_batch: int = 1
+    lam: float = 852e-9
+    pitch: float = 12e-6
+    z: float = 0.25
+    fs: float = 37e3
+    pad_w: int = 0
+    pad_h: int = 0
+    as_filter: int = 0
+    r_inner: int = 0
+    r_outer: int = 0
+    s_inner: int = 0
+    s_outer: int = 0
+
+    def desc(self) -> HfDesc:
+        return HfDesc(self.height, self.width, self.frames, self.hop, self.z_begin, self.z_end,
+                      self.input_dtype, self.propagation, self.clutter_rank, self.moment_mask,
+                      self.fftshift, self.form, self.max_batch, self.lam, self.pitch, self.z, self.fs,
+                      self.pad_w, self.pad_h, self.as_filter, self.r_inner, self.r_outer,
+                      self.s_inner, self.s_outer)
+
+    @property
+    def frame_bytes(self) -> int:
+        P = self.height * self.width
+        return {HF_MONO12P: 3 * P // 2, HF_U16: 2 * P, HF_U8: P, HF_F32: 4 * P}[self.input_dtype]
+
+
+class Pipeline:
+    """Owns an hf_plan; ``run(ring, first_frame, nwin)`` reconstructs nwin windows of a device ring."""
+
+    def __init__(self, cfg: PipelineConfig, stream: Optional[torch.cuda.Stream] = None):
+        self.cfg = cfg
+        self._plan = C.c_void_p()
+        d = cfg.desc()
+        check(lib().hf_plan_create(C.byref(d), C.byref(self._plan), _stream(stream)))
+        oh, ow, nm = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().hf_plan_output_shape(self._plan, C.byref(oh), C.byref(ow), C.byref(nm)))
+        self.out_shape = (nm.value, oh.value, ow.value)
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        check(lib().hf_plan_device_bytes(self._plan, C.byref(b)))
+        return b.value
+
+    def set_z(self, z: float, stream=None) -> None:
+        check(lib().hf_plan_set_z(self._plan, z, _stream(stream)))
+
+    def run(self, ring: torch.Tensor, ring_frames: int, first_frame: int, nwin: int,
+            out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty((nwin, *self.out_shape), dtype=torch.float32, device=ring.device)
+        check(lib().hf_pipeline_exec(self._plan, _ptr(ring), ring_frames, first_frame, nwin, _ptr(out),
+                                     _stream(stream)))
+        return out
+
+    def inspect(self, w: int = 0):
+        T, nz = self.cfg.frames, self.cfg.z_end - self.cfg.z_begin
+        gram = torch.empty((T, T), dtype=torch.float64, device="cuda") if self.cfg.clutter_rank else None
+        wm = torch.empty((T, nz), dtype=torch.complex64, device="cuda")
+        check(lib().hf_pipeline_inspect(self._plan, w, _ptr(gram), _ptr(wm), _stream()))
+        return gram, wm
+
+    def close(self) -> None:
+        if self._plan:
+            lib().hf_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FresnelPlan:
+    def __init__(self, batch, H, W, in_dtype, lam, dx, z, output_magnitude=False, skip_phase_shift=True):
+        self._p = C.c_void_p()
+        self.shape = (batch, H, W)
+        self.magnitude = output_magnitude
+        check(lib().hf_fresnel_plan_create(batch, H, W, in_dtype, lam, dx, z, int(output_magnitude),
+                                           int(skip_phase_shift), C.byref(self._p), _stream()))
+
+    def set_z(self, z):
+        check(lib().hf_fresnel_plan_set_z(self._p, z, _stream()))
+
+    def __call__(self, x: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        B, H, W = self.shape
+        if out is None:
+            out = torch.empty((B, H, W), dtype=torch.float32 if self.magnitude else torch.complex64,
+                              device=x.device)
+        sx = x.stride()
+        so = out.stride()
+        check(lib().hf_fresnel_exec(self._p, _ptr(x), sx[0], sx[1], sx[2], _ptr(out), so[0], so[1], so[2],
+                                    _stream()))
+        return out
+
+    def __del__(self):
+        try:
+            lib().hf_fresnel_plan_destroy(self._p)
+        except Exception:
+            pass
+
+
+class AngularSpectrumPlan:
+    def __init__(self, batch, H, W, in_dtype, lam, dx, z, padding=None, filt=None):
+        self._p = C.c_void_p()
+        pw, ph = (padding["width"], padding["height"]) if padding else (0, 0)
+        f = filt or {}
+        self.out_shape = (batch, ph or H, pw or W)
+        check(lib().hf_as_plan_create(batch, H, W, in_dtype, lam, dx, z, pw, ph, int(filt is not None),
+                                      f.get("r_inner", 0), f.get("r_outer", 0), f.get("s_inner", 0),
+                                      f.get("s_outer", 0), C.byref(self._p), _stream()))
+
+    def __call__(self, x: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty(self.out_shape, dtype=torch.complex64, device=x.device)
+        check(lib().hf_as_exec(self._p, _ptr(x), _ptr(out), _stream()))
+        return out
+
+    def __del__(self):
+        try:
+            lib().hf_as_plan_destroy(self._p)
+        except Exception:
+            pass

@@ -1,0 +1,206 @@
+/*
+ * holoflow_b200 — C ABI of the B200 (sm_100a) laser Doppler reconstruction library.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns an int status
+ * (HF_OK = 0, negative = error class; the text is in hf_last_error(), thread-local), never
+ * throws, and only enqueues work on the stream it is given (no host synchronisation unless the
+ * comment says so).  Device pointers must be device-accessible memory of the current device.
+ *
+ * Each function names the Holoflow interface it replaces (paths relative to the Holoflow source
+ * tree).  The C++ node layer (include/holoflow/core/*.hh, kinds registered under the reference's
+ * kind strings) is built on top of these calls.
+ */
+#ifndef HOLOFLOW_B200_H
+#define HOLOFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *hf_stream_t; /* identical to cudaStream_t */
+
+/* ---- status codes ------------------------------------------------------------------------- */
+enum {
+  HF_OK              = 0,
+  HF_ERR_INVALID     = -1, /* bad argument / shape / setting (reference: std::invalid_argument) */
+  HF_ERR_CUDA        = -2, /* CUDA runtime error (reference: curaii::CudaError)                  */
+  HF_ERR_UNSUPPORTED = -3, /* valid request this build does not implement                        */
+  HF_ERR_NOMEM       = -4, /* device allocation failed / admission refused                      */
+  HF_ERR_TIMEOUT     = -5, /* a bounded device wait expired (status word set by a kernel)       */
+  HF_ERR_STATE       = -6, /* object used in the wrong state                                     */
+  HF_ERR_CANCELLED   = -7  /* cooperative cancellation observed                                  */
+};
+
+/* ---- element types (first four in the order of holoflow::core::DType, tensor.hh:29-34) ----- */
+enum {
+  HF_U8      = 0,
+  HF_U16     = 1,
+  HF_F32     = 2,
+  HF_CF32    = 3,
+  HF_MONO12P = 16 /* 12-bit, 2 pixels in 3 bytes, LSB-first: b0=p0[7:0], b1=p0[11:8]|p1[3:0]<<4,
+                     b2=p1[11:4]; a frame of P pixels (P even) is 3P/2 bytes                      */
+};
+
+/* Conversion strategies (ConversionSettings::Strategy, holotask/syncs/conversion.hh:27-67) */
+enum { HF_CONV_REAL = 0, HF_CONV_SCALED = 1, HF_CONV_MODULUS = 2, HF_CONV_ARGUMENT = 3 };
+
+/* FFT normalisation (holonp FftNorm, holonp/src/fft.cu:100-109) */
+enum { HF_NORM_BACKWARD = 0, HF_NORM_FORWARD = 1, HF_NORM_ORTHO = 2 };
+
+/* Spatial propagation methods (holovibes Settings::spacial_method) */
+enum { HF_PROP_NONE = 0, HF_PROP_FRESNEL = 1, HF_PROP_ANGULAR_SPECTRUM = 2 };
+
+/* Moment selection bits (holovibes MomentType M0/M1/M2, graph_builder.cc:604-631) */
+enum { HF_M0 = 1, HF_M1 = 2, HF_M2 = 4 };
+
+/* Numeric form of the pipeline: all-FP32 ("plain") or tensor-core ("chosen") */
+enum { HF_FORM_PLAIN = 0, HF_FORM_CHOSEN = 1 };
+
+/* ---- library ------------------------------------------------------------------------------ */
+const char *hf_last_error(void);
+int         hf_version(void);
+/* Number of kernel launches this thread's calls have enqueued since the last reset. */
+int64_t     hf_launch_count(void);
+void        hf_reset_launch_count(void);
+
+/* ---- a1: 12-bit unpack (new: the reference has no 12-bit path, holofile.cc:247-250) -------- */
+/* packed: 3*npix/2 bytes, npix even.  out_dtype: HF_U16, HF_F32 or HF_CF32 (imag = 0). */
+int hf_unpack12(const uint8_t *packed, void *out, int out_dtype, int64_t npix, hf_stream_t s);
+/* Inverse of hf_unpack12 for uint16 values < 4096 (acquisition / test support). */
+int hf_pack12(const uint16_t *in, uint8_t *packed, int64_t npix, hf_stream_t s);
+
+/* ---- a2: Conversion (ConversionTask::execute, holotask/src/syncs/conversion.cu:237-258) ----- */
+/* Supported (in_dtype, out_dtype, strategy) triples are those of conversion.cu:138-150.
+ * HF_CONV_SCALED needs `minmax_ws`: device scratch of at least 64 bytes. */
+int hf_convert(const void *in, int in_dtype, void *out, int out_dtype, int strategy, int64_t n,
+               void *minmax_ws, hf_stream_t s);
+
+/* ---- a5/a6/a7: temporal FFT / RFFT along the frame axis + band slice ------------------------
+ * Replaces holonp FFT (fft.cu:234-252) / RFFT (rfft.cu:150-160) on axis 1 of [B, T, H, W]
+ * followed by Slice+Copy of bins [z0, z1) (graph_builder.cc:264-267).
+ * in: [batch][T][P] of in_dtype (HF_U8, HF_U16, HF_MONO12P, HF_F32 or HF_CF32; MONO12P frames
+ * are 3P/2 bytes).  out: [batch][z1-z0][P] complex64, bin k = scale * sum_t x_t e^{-2 pi i t k/T}.
+ */
+int hf_temporal_dft(const void *in, int in_dtype, int64_t batch, int T, int64_t P, int z0, int z1,
+                    int norm, void *out, hf_stream_t s);
+
+/* ---- a8: PCA / SVD clutter filter (PcaTask, holotask/src/syncs/pca.cc:68-119) -------------
+ * hf_covariance: gram[b] = X_b^T X_b (T x T, float64, row-major, symmetric), X_b = [T][P] frames
+ * of in_dtype (HF_U8, HF_U16, HF_MONO12P, HF_F32).  No centring, no 1/N (pca.cc:92-98).
+ * `ws` must hold hf_covariance_workspace_bytes(T, P) bytes per batch item. */
+size_t hf_covariance_workspace_bytes(int T, int64_t P);
+int    hf_covariance(const void *in, int in_dtype, int64_t batch, int T, int64_t P, double *gram,
+                     void *ws, hf_stream_t s);
+
+/* Symmetric eigendecomposition (PcaHeevSolver::launch, pca_heev.cc:101-121) by FP64 cyclic
+ * Jacobi, one CTA per matrix, n <= 128.  a: [batch][n][n] row-major symmetric; on return
+ * evecs[b] holds eigenvector j in COLUMN j (row-major [n][n]), evals[b] ascending.  info[b] = 0 on
+ * convergence, else the number of sweeps run (non-converged). */
+int hf_eigh_jacobi_f64(const double *a, double *evecs, double *evals, int *info, int n,
+                       int64_t batch, hf_stream_t s);
+
+/* Projection onto eigenvectors [begin, end) (pca.cc:106-116): out[b][c][p] =
+ * sum_t X_b[t][p] * evecs_b[t][begin + c].  in: float32 [batch][T][P]. */
+int hf_pca_project(const float *in, int64_t batch, int T, int64_t P, const double *evecs,
+                   int begin, int end, float *out, hf_stream_t s);
+
+/* Per-window filter+DFT matrix W = (I - V V^T) D[:, z0:z1] (V = the `rank` eigenvectors with the
+ * largest eigenvalues, last columns of `evecs`), D the unnormalised DFT; float32 complex
+ * [batch][T][z1-z0].  rank = 0 gives the plain band DFT matrix. */
+int hf_band_matrix(const double *evecs, int64_t batch, int T, int rank, int z0, int z1,
+                   void *wmat, hf_stream_t s);
+
+/* ---- a9: Fresnel diffraction (FresnelDiffraction, fresnel_diffraction.cu:410-441) ----------
+ * out = FFT2_forward(in * L) over (H, W), L[r][c] = exp(i pi/(lambda z) (x^2 + y^2)),
+ * x = ((c + (S-W)/2) - S/2) dx, S = max(H, W); unnormalised, no fftshift.  If output_magnitude
+ * the output is float32 |.|; otherwise complex, times L again unless skip_phase_shift.
+ * Element strides (in elements of the input / output type) describe [batch][H][W] views;
+ * the W stride must be 1 for the fast path (other strides use the general kernels). */
+typedef struct hf_fresnel_plan hf_fresnel_plan;
+int hf_fresnel_plan_create(int64_t batch, int H, int W, int in_dtype, float lambda, float dx,
+                           float z, int output_magnitude, int skip_phase_shift,
+                           hf_fresnel_plan **plan, hf_stream_t s);
+/* z-only update without re-planning (FresnelDiffractionFactory::update, .cu:634-668). */
+int hf_fresnel_plan_set_z(hf_fresnel_plan *plan, float z, hf_stream_t s);
+int hf_fresnel_exec(hf_fresnel_plan *plan, const void *in, int64_t in_batch_stride,
+                    int64_t in_row_stride, int64_t in_col_stride, void *out,
+                    int64_t out_batch_stride, int64_t out_row_stride, int64_t out_col_stride,
+                    hf_stream_t s);
+int hf_fresnel_plan_destroy(hf_fresnel_plan *plan);
+
+/* ---- a10: Angular spectrum (AngularSpectrum, angular_spectrum.cu:408-431) -----------------
+ * out = IFFT2(FFT2(pad_center(in)) * TF), TF = swap_corners(exp(i 2 pi z/lambda sqrt(max(0,
+ * 1 - lambda^2 (u^2+v^2)))) * w^2), both transforms unnormalised.  in: [batch][H][W] HF_F32 or
+ * HF_CF32 (C-contiguous); out: [batch][OH][OW] complex64.  pad_w/pad_h = 0 for no padding;
+ * in == out is allowed for CF32 without padding.  use_filter selects the raised-sine annulus
+ * (r_inner, r_outer, s_inner, s_outer) of multiply_filter_2d_kernel. */
+typedef struct hf_as_plan hf_as_plan;
+int hf_as_plan_create(int64_t batch, int H, int W, int in_dtype, float lambda, float dx, float z,
+                      int pad_w, int pad_h, int use_filter, uint32_t r_inner, uint32_t r_outer,
+                      uint32_t s_inner, uint32_t s_outer, hf_as_plan **plan, hf_stream_t s);
+int hf_as_exec(hf_as_plan *plan, const void *in, void *out, hf_stream_t s);
+int hf_as_plan_destroy(hf_as_plan *plan);
+
+/* ---- a11/a12/a13: Mean, MeanAbs and weighted band moments ---------------------------------
+ * hf_mean_axis: mean over the middle axis of a [outer][n][inner] view (Mean with one reduced
+ * axis, holonp/src/mean.cu:268-305): F32 -> F32, CF32 -> CF32, U8/U16 -> F32.
+ * hf_mean_abs_axis: the same with |.| (MeanAbs, mean_abs.cu:240-275), F32 or CF32 -> F32.
+ * hf_band_moments: from |S| planes [nz][P] (F32) or S planes (CF32), writes the selected
+ * moments (M0 = mean |S_k|, M1 = mean f_k |S_k|, M2 = mean f_k^2 |S_k|, with f_k^2 formed in
+ * float32; graph_builder.cc:612-631) as consecutive [P] float planes in M0, M1, M2 order. */
+int hf_mean_axis(const void *in, int in_dtype, int64_t outer, int64_t n, int64_t inner, void *out,
+                 hf_stream_t s);
+int hf_mean_abs_axis(const void *in, int in_dtype, int64_t outer, int64_t n, int64_t inner,
+                     float *out, hf_stream_t s);
+int hf_band_moments(const void *planes, int in_dtype, int nz, int64_t P, const float *freqs,
+                    int moment_mask, float *out, hf_stream_t s);
+
+/* ---- a14: the fused per-window path ------------------------------------------------------ */
+typedef struct hf_desc {
+  int32_t height, width;     /* frame size                                                    */
+  int32_t frames;            /* T: frames per window                                           */
+  int32_t hop;               /* S: frames between consecutive windows                          */
+  int32_t z_begin, z_end;    /* band bins [z0, z1) of the T-point DFT                          */
+  int32_t input_dtype;       /* HF_MONO12P, HF_U16, HF_U8 or HF_F32                            */
+  int32_t propagation;       /* HF_PROP_*                                                      */
+  int32_t clutter_rank;      /* eigenvectors removed by the SVD clutter filter (0 = none)      */
+  int32_t moment_mask;       /* HF_M0 | HF_M1 | HF_M2                                          */
+  int32_t fftshift;          /* fftshift the moment images (graph_builder.cc:633-635)          */
+  int32_t form;              /* HF_FORM_PLAIN or HF_FORM_CHOSEN                                */
+  int32_t max_batch;         /* windows per hf_pipeline_exec call (>= 1)                       */
+  float   lambda, pitch, z;  /* wavelength, pixel pitch (dx = dy), propagation distance [m]    */
+  float   fs;                /* sampling rate of the moment weights [Hz] (reference: 37e3)     */
+  int32_t pad_w, pad_h;      /* angular-spectrum padding (0 = none)                           */
+  int32_t as_filter;         /* angular-spectrum raised-sine annulus on/off                   */
+  uint32_t r_inner, r_outer, s_inner, s_outer;
+} hf_desc;
+
+typedef struct hf_plan hf_plan;
+/* Allocates every device buffer the path needs for max_batch windows (reference create()). */
+int hf_plan_create(const hf_desc *desc, hf_plan **plan, hf_stream_t s);
+int hf_plan_destroy(hf_plan *plan);
+/* Rebuilds the lens / transfer function for a new z (reference z-only update()). */
+int hf_plan_set_z(hf_plan *plan, float z, hf_stream_t s);
+/* Output image size of the plan (AS padding enlarges it) and the number of moment planes. */
+int hf_plan_output_shape(const hf_plan *plan, int32_t *out_h, int32_t *out_w, int32_t *n_moments);
+/* Bytes of device memory the plan holds. */
+int hf_plan_device_bytes(const hf_plan *plan, size_t *bytes);
+
+/* Runs `nwin` (<= max_batch) windows.  Window w consists of frames
+ * ring + ((first_frame + w*hop + t) mod ring_frames) * frame_bytes, t = 0..T-1, i.e. windows of
+ * a device ring of `ring_frames` frames; out: [nwin][n_moments][OH][OW] float32. */
+int hf_pipeline_exec(hf_plan *plan, const void *ring, int64_t ring_frames, int64_t first_frame,
+                     int nwin, float *out, hf_stream_t s);
+
+/* Debug/inspection: after hf_pipeline_exec, copy window `w`'s T x T Gram matrix (float64) and
+ * its filter+DFT matrix W (complex64 [T][Nz]) to device buffers (either may be NULL). */
+int hf_pipeline_inspect(hf_plan *plan, int w, double *gram, void *wmat, hf_stream_t s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HOLOFLOW_B200_H */

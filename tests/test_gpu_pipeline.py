@@ -1,0 +1,104 @@
+"""GPU parity of the fused per-window path (hf_pipeline_exec) against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import synth as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(cuda, frames_u16, cfg_kw, nwin, first=0, fmt="mono12p"):
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    n = frames_u16.shape[0]
+    if fmt == "mono12p":
+        ring = torch.from_numpy(O.pack12(frames_u16.reshape(-1))).to(cuda)
+        dt = hf.HF_MONO12P
+    else:
+        ring = torch.from_numpy(frames_u16.view(np.int16)).to(cuda)
+        dt = hf.HF_U16
+    cfg = pl.PipelineConfig(input_dtype=dt, max_batch=nwin, **cfg_kw)
+    p = pl.Pipeline(cfg)
+    out = p.run(ring, n, first, nwin)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), p
+
+
+def _oracle_cfg(kw):
+    prop = {1: "fresnel", 2: "angular_spectrum", 0: "none"}[kw.get("propagation", 1)]
+    pad = {"width": kw["pad_w"], "height": kw["pad_h"]} if kw.get("pad_w") else None
+    return O.PathConfig(kw["height"], kw["width"], kw["frames"], kw["hop"], kw["z_begin"], kw["z_end"],
+                        fs=kw.get("fs", 37e3), propagation=prop, lam=kw.get("lam", 852e-9),
+                        pitch=kw.get("pitch", 12e-6), z=kw.get("z", 0.25),
+                        clutter_rank=kw.get("clutter_rank", 0), fftshift=bool(kw.get("fftshift", 0)),
+                        as_padding=pad)
+
+
+def _check(got, frames, kw, nwin, tol):
+    ocfg = _oracle_cfg(kw)
+    for w in range(nwin):
+        win = frames[w * kw["hop"]: w * kw["hop"] + kw["frames"]]
+        exp = O.reconstruct_window(win, ocfg)
+        mask = kw.get("moment_mask", 7)
+        exp = exp[[m for m in range(3) if mask & (1 << m)]]
+        for m in range(exp.shape[0]):
+            err = O.rel_l2(got[w, m], exp[m])
+            assert err < tol, (w, m, err)
+
+
+def test_pipeline_config1_mini_fresnel_svd(cuda):
+    z0, z1 = O.band_bins(4e3, 33e3, 67e3, 64)
+    kw = dict(height=256, width=256, frames=64, hop=16, z_begin=z0, z_end=z1, fs=67e3, z=0.25,
+              clutter_rank=4)
+    frames = S.Interferograms(S.config1(64 + 2 * 16, height=256, width=256)).frames(0, 96)
+    got, _ = _run(cuda, frames, kw, 3)
+    _check(got, frames, kw, 3, 1e-4)
+
+
+def test_pipeline_config0_angular_spectrum(cuda):
+    z0, z1 = O.band_bins(6e3, 18e3, 37e3, 32)
+    kw = dict(height=512, width=512, frames=32, hop=32, z_begin=z0, z_end=z1, fs=37e3, z=0.30,
+              propagation=2)
+    frames = S.Interferograms(S.config0(64)).frames(0, 64)
+    got, _ = _run(cuda, frames, kw, 2, fmt="u16")
+    _check(got, frames, kw, 2, 1e-4)
+
+
+def test_pipeline_variants_fftshift_m0_none_padding(cuda):
+    frames = S.Interferograms(S.config0(48)).frames(0, 48)[:, :128, :128].copy()
+    base = dict(height=128, width=128, frames=32, hop=16, z_begin=6, z_end=16, fs=37e3, z=0.3)
+    for extra in (dict(fftshift=1), dict(moment_mask=1), dict(propagation=0), dict(clutter_rank=2),
+                  dict(propagation=2, pad_w=256, pad_h=256), dict(propagation=2, fftshift=1, moment_mask=5)):
+        kw = {**base, **extra}
+        got, _ = _run(cuda, frames, kw, 2)
+        _check(got, frames, kw, 2, 1e-4)
+
+
+def test_pipeline_ring_wraparound(cuda):
+    """Windows that wrap around the end of the device ring equal the unwrapped ones."""
+    frames = S.Interferograms(S.config0(64)).frames(0, 64)[:, :128, :128].copy()
+    kw = dict(height=128, width=128, frames=32, hop=16, z_begin=6, z_end=16, z=0.3)
+    a, _ = _run(cuda, frames, kw, 1, first=16)
+    rolled = np.roll(frames, -40, axis=0)  # frame 16 now sits at index 40 (wraps)
+    b, _ = _run(cuda, rolled, kw, 1, first=40)
+    assert np.array_equal(a, b)
+
+
+def test_pipeline_full_config1_window(cuda):
+    """Config 1 at full size (1024^2, T = 64, hop 16, top-4 clutter removal, Fresnel, 4-33 kHz)."""
+    z0, z1 = O.band_bins(4e3, 33e3, 67e3, 64)
+    kw = dict(height=1024, width=1024, frames=64, hop=16, z_begin=z0, z_end=z1, fs=67e3, z=0.25,
+              clutter_rank=4)
+    frames = S.Interferograms(S.config1(64)).frames(0, 64)
+    got, _ = _run(cuda, frames, kw, 1)
+    _check(got, frames, kw, 1, 1e-4)
+
+
+def test_pipeline_rejects_bad_desc(cuda):
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    with pytest.raises(hf.HfError) as e:
+        pl.Pipeline(pl.PipelineConfig(height=64, width=64, frames=32, hop=8, z_begin=10, z_end=5))
+    assert e.value.code == hf.HF_ERR_INVALID
