@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the laser Doppler path on the full-size workload (1024^2 x 64 M0 images/s).
+
+Workload (the reference's headline configuration): 1024x1024 frames of 12-bit values packed
+2 pixels / 3 bytes, windows of T = 64 frames every 16 frames, fs = 67 kHz, top-4 SVD clutter
+removal, single-FFT Fresnel propagation (z = 0.25 m, 852 nm, 12 um), M0/M1/M2 over 4-33 kHz
+(bins 4..31).  A step reconstructs `--batch` consecutive windows of a device frame ring that is
+larger than L2 (403 MB), so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form plain|chosen]
+
+One process per GPU (torchrun for N > 1): every rank reconstructs its own independent stream
+(replicas; the path has no cross-GPU exchange), timing is the max over ranks of CUDA-event time.
+Rank 0 prints one JSON line.  `--impl reference` times the CPU restatement of the path (the
+reference has no CPU implementation of its own) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+H = W = 1024
+T, HOP, FS = 64, 16, 67e3
+Z0, Z1 = 4, 32                  # 4-33 kHz at df = fs/T = 1046.875 Hz
+RANK_CLUTTER = 4
+RING_FRAMES = 256               # 403 MB of packed frames (> 126 MB L2)
+METRIC = "1024²×64 M0 images/s and p99 frame-to-image latency, chosen vs plain form"
+WORKLOAD = "config1: 1024x1024 12-bit packed, T=64 hop=16, fs=67kHz, top-4 SVD clutter filter, Fresnel z=0.25m, M0/M1/M2 4-33kHz"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="best", choices=["plain", "chosen", "best"])
+    ap.add_argument("--batch", type=int, default=8, help="windows per step")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-window DRAM bytes of each stage from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "ncu_traffic_config1.txt"
+    out = {}
+    if p.exists():
+        for line in p.read_text().splitlines():
+            parts = line.split()
+            if len(parts) == 2 and not line.startswith("#"):
+                try:
+                    out[parts[0]] = float(parts[1])
+                except ValueError:
+                    pass
+    return out
+
+
+def algorithmic_bytes_per_window(nmom=3):
+    P, nz = H * W, Z1 - Z0
+    packed = 1.5 * P * T
+    return {
+        "covariance": packed,
+        "eigen_filter": 2 * 8 * T * T,
+        "band_dft": packed + 8 * P * nz,
+        "fft_rows": 2 * 8 * P * nz,
+        "fft_cols_moments": 8 * P * nz + 4 * P * nmom,
+        "band_dft_rows": packed + 8 * P * nz,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(sample_windows=1):
+    """The CPU restatement of the path (oracle port, float64 NumPy/SciPy, all host threads) on one
+    config-1 window; returns (windows/s, seconds, threads)."""
+    from oracle import oracle as O
+    from oracle import synth as S
+    frames = S.Interferograms(S.config1(T)).frames(0, T)
+    cfg = O.PathConfig(H, W, T, HOP, Z0, Z1, fs=FS, z=0.25, clutter_rank=RANK_CLUTTER)
+    O.reconstruct_window(frames, cfg)  # warm caches / thread pools
+    t0 = time.perf_counter()
+    for _ in range(sample_windows):
+        O.reconstruct_window(frames, cfg)
+    dt = time.perf_counter() - t0
+    return sample_windows / dt, dt, os.cpu_count()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from oracle import synth as S
+    frames = S.Interferograms(S.config1(T)).frames(0, T)
+    cfg = O.PathConfig(H, W, T, HOP, Z0, Z1, fs=FS, z=0.25, clutter_rank=RANK_CLUTTER)
+    for _ in range(args.warmup):
+        O.reconstruct_window(frames, cfg)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.reconstruct_window(frames, cfg)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    sample = "1 full config-1 window (64 x 1024^2 frames) per step, float64 oracle port"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "images/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * dt / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "windows_per_step": 1, "device": "cpu"},
+        "cpu_baseline": {"value": round(v, 4), "unit": "images/s", "cores": os.cpu_count(),
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 4), "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    from holoflow_b200 import synth as sy
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    B = args.batch
+    form = hf.HF_FORM_CHOSEN if args.form == "chosen" else hf.HF_FORM_PLAIN
+    cfg = pl.PipelineConfig(height=H, width=W, frames=T, hop=HOP, z_begin=Z0, z_end=Z1, fs=FS, z=0.25,
+                            clutter_rank=RANK_CLUTTER, max_batch=B, form=form)
+    # synthetic frames: 64 distinct frames generated on the device, tiled over the ring
+    gen = sy.DeviceInterferograms(sy.config1_scene(acquisition=rank), device=dev)
+    base = gen.frames(0, 64)
+    fb = cfg.frame_bytes
+    ring = torch.empty(RING_FRAMES * fb, dtype=torch.uint8, device=dev)
+    packed = pl.pack12(base.reshape(-1)).view(64, fb)
+    for i in range(RING_FRAMES // 64):
+        ring.view(RING_FRAMES, fb)[i * 64:(i + 1) * 64] = packed
+    del base
+    pipe = pl.Pipeline(cfg)
+    nmom = pipe.out_shape[0]
+    out = torch.empty((B, *pipe.out_shape), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(s):
+        first = (s * B * HOP) % RING_FRAMES
+        pipe.run(ring, RING_FRAMES, first, B, out)
+
+    for s in range(args.warmup):
+        step(s)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    pipe.timing(True)
+    lib = hf.lib()
+    lib.hf_reset_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for s in range(args.steps):
+            step(args.warmup + s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.hf_launch_count()
+    ms = e0.elapsed_time(e1)
+    stages = pipe.stage_times()
+    pipe.timing(False)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps * B / (ms / 1000.0)
+
+    # roofline of the dominant stage (algorithmic bytes / its CUDA-event time)
+    peak, peak_kind = peaks()
+    algo = algorithmic_bytes_per_window(nmom)
+    dom = max(stages, key=lambda k: stages[k][0]) if stages else None
+    roof = None
+    if dom:
+        per_launch_ms = stages[dom][0] / max(stages[dom][1], 1)
+        bytes_launch = algo.get(dom, 0.0) * B
+        achieved = bytes_launch / (per_launch_ms / 1000.0) / 1e9
+        tr = traffic_table().get(dom)
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": (tr * B) if tr else None,
+                "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": round(per_launch_ms, 4),
+                "stages_ms_per_step": {k: round(v[0] / max(v[1], 1), 4) for k, v in stages.items()}}
+
+    # end to end through the camera-stream API: pinned host frames in, host moments out
+    e2e = None
+    if not args.no_e2e:
+        nstep_frames = B * HOP
+        host_frames = torch.empty(nstep_frames * fb, dtype=torch.uint8, pin_memory=True)
+        reps = (nstep_frames + 63) // 64
+        host_frames.view(nstep_frames, fb).copy_(torch.cat([packed] * reps)[:nstep_frames].cpu())
+        host_out = torch.empty((B, *pipe.out_shape), dtype=torch.float32, pin_memory=True)
+        cam = pl.CameraStream(pipe, T + (B + 1) * HOP + nstep_frames)
+        cam.push(host_frames, T - HOP)  # prefill: the first window needs T - hop older frames
+        lat = []
+        for s in range(args.warmup):
+            cam.push(host_frames, nstep_frames)
+            cam.process(B, host_out)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for s in range(args.steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            cam.push(host_frames, nstep_frames)
+            n = cam.process(B, host_out)
+            b.record(stream)
+            lat.append((a, b))
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1)
+        if world > 1:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        step_lat = sorted(a.elapsed_time(b) for a, b in lat)
+        p50 = step_lat[len(step_lat) // 2]
+        p99 = step_lat[min(len(step_lat) - 1, int(round(0.99 * (len(step_lat) - 1))))]
+        e2e = {"value": round(world * args.steps * B / (ems / 1000.0), 2), "unit": "images/s",
+               "h2d_bytes_per_step": nstep_frames * fb, "d2h_bytes_per_step": B * nmom * H * W * 4,
+               "latency_ms_p50": round(p50, 3), "latency_ms_p99": round(p99, 3),
+               "latency_definition": "step of new frames pushed from pinned host memory to its "
+                                     "moment images in pinned host memory (serial H2D, compute, D2H)"}
+        cam.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, dt, cores = cpu_baseline()
+        cpu = {"value": round(v, 4), "unit": "images/s", "cores": cores, "kind": "port",
+               "sample": "1 full config-1 window (64 x 1024^2), float64 NumPy/SciPy oracle port, %.2f s" % dt}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "images/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (device-generated interferograms, seeded)",
+            "config": {"workload": WORKLOAD, "form": "chosen" if form else "plain",
+                       "windows_per_step": B, "ring_frames": RING_FRAMES,
+                       "l2": "inputs larger than L2 (403 MB frame ring + 235 MB band planes per window)",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

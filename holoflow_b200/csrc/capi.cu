@@ -1,5 +1,6 @@
 // C ABI of the library: status/error plumbing, stage entry points and the plans (fused
 // per-window pipeline, Fresnel and angular-spectrum nodes).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -96,9 +97,41 @@ struct hf_plan {
   int       *info = nullptr;
   void      *cov_ws = nullptr;
   size_t     bytes = 0;
+  // optional per-stage CUDA-event timing (hf_plan_timing / hf_plan_stage_times)
+  static constexpr int kSets = 128, kMarks = HF_MAX_STAGES + 1;
+  bool        timing = false;
+  int         nexec = 0;
+  cudaEvent_t ev[kSets][kMarks] = {};
+  int         marks[kSets] = {};
+  const char *stage_name[HF_MAX_STAGES] = {};
+  int         nstages = 0;
 };
 
+// Marks a stage boundary when timing is on (event k of the current exec's set).
+static void mark(hf_plan *p, cudaStream_t s, int k, const char *name_of_prev) {
+  if (!p->timing || p->nexec >= hf_plan::kSets)
+    return;
+  cudaEventRecord(p->ev[p->nexec][k], s);
+  p->marks[p->nexec] = k + 1;
+  if (k > 0 && name_of_prev)
+    p->stage_name[k - 1] = name_of_prev;
+}
+
+static int finish_exec(hf_plan *p) {
+  if (p->timing && p->nexec < hf_plan::kSets) {
+    p->nstages = p->marks[p->nexec] - 1;
+    ++p->nexec;
+  }
+  return HF_OK;
+}
+
 static void plan_free(hf_plan *p) {
+  for (int i = 0; i < hf_plan::kSets; ++i)
+    for (int k = 0; k < hf_plan::kMarks; ++k)
+      if (p->ev[i][k]) {
+        cudaEventDestroy(p->ev[i][k]);
+        p->ev[i][k] = nullptr;
+      }
   dev_free(p->lens);
   dev_free(p->tf);
   dev_free(p->band);
@@ -272,13 +305,17 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
   FrameRing      fr{reinterpret_cast<const uint8_t *>(ring), ring_frames, first_frame % ring_frames,
                (int64_t)d.hop, p->frame_bytes};
   const int T = d.frames;
+  int       mk = 0;
+  mark(p, s, mk++, nullptr);
 
   // 1. SVD clutter filter: Gram -> FP64 Jacobi -> W = (I - V V^T) D_band
   BandArgs ba{};
   if (d.clutter_rank > 0) {
     HF_TRY(launch_covariance(fr, d.input_dtype, T, p->P, nwin, p->cov_ws, p->gram, s));
+    mark(p, s, mk++, "covariance");
     HF_TRY(launch_jacobi(p->gram, p->evecs, p->evals, p->info, T, nwin, s));
     HF_TRY(launch_band_matrix(p->evecs, nwin, T, d.clutter_rank, d.z_begin, d.z_end, p->wmat, s));
+    mark(p, s, mk++, "eigen_filter");
     ba.wmat        = p->wmat;
     ba.wmat_stride = (int64_t)T * p->nz;
   } else {
@@ -302,6 +339,7 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
   ba.out_win   = (int64_t)p->nz * p->P;
   ba.scale     = 1.0f;
   HF_TRY(launch_band_dft(ba, d.input_dtype, nwin, s));
+  mark(p, s, mk++, "band_dft");
 
   const int64_t oplane = (int64_t)p->OH * p->OW;
   const int64_t owin   = (int64_t)p->nmom * oplane;
@@ -312,7 +350,8 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
     for (int w = 0; w < nwin; ++w)
       HF_TRY(launch_band_moments(p->band + w * ba.out_win, HF_CF32, p->nz, p->P, mw, d.moment_mask,
                                  out + w * owin, s));
-    return HF_OK;
+    mark(p, s, mk++, "moments");
+    return finish_exec(p);
   }
 
   if (d.propagation == HF_PROP_FRESNEL) {
@@ -335,6 +374,7 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
     rp.out_plane = p->P;
     rp.out_row = d.width;
     HF_TRY(launch_row_pass(rp, nwin, s));
+    mark(p, s, mk++, "fft_rows");
     ColPass cp{};
     cp.in = rp.out;
     cp.in_win = ba.out_win;
@@ -350,7 +390,9 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
       cp.out_plane = oplane;
       cp.out_row = p->OW;
       cp.out_col = 1;
-      return launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s);
+      HF_TRY(launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s));
+      mark(p, s, mk++, "fft_cols_moments");
+      return finish_exec(p);
     }
     // general sizes: complex column DFT back into `band`, then the moment reduction
     cp.out = p->band;
@@ -368,7 +410,8 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
       HF_TRY(launch_band_moments(p->band + w * ba.out_win, HF_CF32, p->nz, p->P, mw,
                                  d.moment_mask, out + w * owin, s));
     }
-    return HF_OK;
+    mark(p, s, mk++, "fft_cols_moments");
+    return finish_exec(p);
   }
 
   // angular spectrum: rows forward (with placement) -> columns fwd x TF inv -> rows inverse + moments
@@ -392,6 +435,7 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
   rp.out_plane = oplane;
   rp.out_row = p->OW;
   HF_TRY(launch_row_pass(rp, nwin, s));
+  mark(p, s, mk++, "fft_rows");
   ColPass cp{};
   cp.in = p->band2;
   cp.in_win = rp.out_win;
@@ -408,13 +452,55 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
   cp.tf = p->tf;
   cp.inverse = 0;
   HF_TRY(launch_col_pass(cp, COL_TF_SANDWICH, nullptr, nwin, s));
+  mark(p, s, mk++, "fft_cols_tf");
   ColPass rm = cp;
   rm.out = out;
   rm.out_win = owin;
   rm.out_plane = oplane;
   rm.out_row = p->OW;
   rm.inverse = 1;
-  return launch_row_moments(rm, p->mom, nwin, s);
+  HF_TRY(launch_row_moments(rm, p->mom, nwin, s));
+  mark(p, s, mk++, "fft_rows_moments");
+  return finish_exec(p);
+}
+
+int hf_plan_timing(hf_plan *p, int enable) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr, "hf_plan_timing: null plan");
+  if (enable) {
+    for (int i = 0; i < hf_plan::kSets; ++i)
+      for (int k = 0; k < hf_plan::kMarks; ++k)
+        if (!p->ev[i][k])
+          HF_CUDA(cudaEventCreate(&p->ev[i][k]));
+  }
+  p->timing = enable != 0;
+  p->nexec  = 0;
+  return HF_OK;
+}
+
+int hf_plan_stage_times(hf_plan *p, float *ms, const char **names, int *nstages, int *nexec) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr && ms != nullptr && nstages != nullptr, "hf_plan_stage_times: null argument");
+  const int ns = p->nstages;
+  for (int k = 0; k < HF_MAX_STAGES; ++k)
+    ms[k] = 0.f;
+  for (int i = 0; i < p->nexec; ++i) {
+    for (int k = 0; k + 1 < p->marks[i] && k < ns; ++k) {
+      float t = 0.f;
+      cudaError_t e = cudaEventElapsedTime(&t, p->ev[i][k], p->ev[i][k + 1]);
+      if (e == cudaErrorNotReady)
+        return fail(HF_ERR_STATE, "hf_plan_stage_times: synchronise the stream first");
+      HF_CUDA(e);
+      ms[k] += t;
+    }
+  }
+  if (names)
+    for (int k = 0; k < ns; ++k)
+      names[k] = p->stage_name[k];
+  *nstages = ns;
+  if (nexec)
+    *nexec = p->nexec;
+  return HF_OK;
 }
 
 int hf_pipeline_inspect(hf_plan *p, int w, double *gram, void *wmat, hf_stream_t s) {
@@ -780,6 +866,109 @@ int hf_as_plan_destroy(hf_as_plan *p) {
   dev_free(p->tf);
   dev_free(p->scratch);
   delete p;
+  return HF_OK;
+}
+
+} // extern "C"
+
+// ================================================================================================
+// Camera stream: device-resident frame ring + window cursor bound to a plan
+// ================================================================================================
+struct hf_stream {
+  hf_plan *plan        = nullptr;
+  uint8_t *ring        = nullptr;
+  int64_t  ring_frames = 0;
+  int64_t  pushed      = 0; // frames appended since creation
+  int64_t  next_win    = 0; // index of the next window to reconstruct
+  float   *dev_out     = nullptr; // staging for host outputs [max_batch][nmom][OH][OW]
+  size_t   bytes       = 0;
+};
+
+extern "C" {
+
+int hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **out) {
+  clear_error();
+  HF_CHECK_ARG(plan != nullptr && out != nullptr, "hf_stream_create: null argument");
+  *out = nullptr;
+  const int64_t need = plan->d.frames + (int64_t)(plan->d.max_batch - 1) * plan->d.hop;
+  HF_CHECK_ARG(ring_frames >= need, "hf_stream_create: ring must hold max_batch overlapping windows");
+  auto *st = new (std::nothrow) hf_stream();
+  if (!st)
+    return fail(HF_ERR_NOMEM, "hf_stream_create: host allocation failed");
+  st->plan        = plan;
+  st->ring_frames = ring_frames;
+  int rc = dev_alloc(&st->ring, (size_t)(ring_frames * plan->frame_bytes), st->bytes);
+  if (rc == HF_OK)
+    rc = dev_alloc(&st->dev_out, (size_t)plan->d.max_batch * plan->nmom * plan->OH * plan->OW, st->bytes);
+  if (rc != HF_OK) {
+    dev_free(st->ring);
+    dev_free(st->dev_out);
+    delete st;
+    return rc;
+  }
+  *out = st;
+  return HF_OK;
+}
+
+int hf_stream_destroy(hf_stream *st) {
+  if (!st)
+    return HF_OK;
+  cudaDeviceSynchronize();
+  dev_free(st->ring);
+  dev_free(st->dev_out);
+  delete st;
+  return HF_OK;
+}
+
+int64_t hf_stream_ready(const hf_stream *st) {
+  if (!st)
+    return 0;
+  const hf_desc &d = st->plan->d;
+  if (st->pushed < d.frames)
+    return 0;
+  const int64_t complete = (st->pushed - d.frames) / d.hop + 1;
+  return complete - st->next_win;
+}
+
+int hf_stream_push(hf_stream *st, const void *frames, int64_t nframes, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(st != nullptr && (frames != nullptr || nframes == 0) && nframes >= 0,
+               "hf_stream_push: bad argument");
+  const hf_desc &d     = st->plan->d;
+  const int64_t  keep0 = st->next_win * d.hop; // first frame still needed
+  HF_CHECK_ARG(st->pushed + nframes - keep0 <= st->ring_frames,
+               "hf_stream_push: ring overrun (process ready windows first)");
+  const int64_t fb  = st->plan->frame_bytes;
+  const auto   *src = reinterpret_cast<const uint8_t *>(frames);
+  int64_t       done = 0;
+  while (done < nframes) {
+    const int64_t slot = (st->pushed + done) % st->ring_frames;
+    const int64_t n    = std::min(nframes - done, st->ring_frames - slot);
+    HF_CUDA(cudaMemcpyAsync(st->ring + slot * fb, src + done * fb, (size_t)(n * fb), cudaMemcpyDefault, s));
+    done += n;
+  }
+  st->pushed += nframes;
+  return HF_OK;
+}
+
+int hf_stream_process(hf_stream *st, int max_windows, float *out, int out_is_host, int *nwin,
+                      hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(st != nullptr && out != nullptr, "hf_stream_process: null argument");
+  const int64_t ready = hf_stream_ready(st);
+  const int     n     = (int)std::min<int64_t>({ready, (int64_t)max_windows, (int64_t)st->plan->d.max_batch});
+  if (nwin)
+    *nwin = n;
+  if (n <= 0)
+    return HF_OK;
+  float *dst = out_is_host ? st->dev_out : out;
+  HF_TRY(hf_pipeline_exec(st->plan, st->ring, st->ring_frames,
+                          (st->next_win * st->plan->d.hop) % st->ring_frames, n, dst, s));
+  if (out_is_host) {
+    const size_t bytes = (size_t)n * st->plan->nmom * st->plan->OH * st->plan->OW * sizeof(float);
+    HF_CUDA(cudaMemcpyAsync(out, st->dev_out, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  st->next_win += n;
   return HF_OK;
 }
 

@@ -138,6 +138,17 @@ class Pipeline:
         check(lib().hf_pipeline_inspect(self._plan, w, _ptr(gram), _ptr(wm), _stream()))
         return gram, wm
 
+    def timing(self, enable: bool) -> None:
+        check(lib().hf_plan_timing(self._plan, int(enable)))
+
+    def stage_times(self):
+        """{stage: (total ms, execs)} of the execs recorded since timing(True)."""
+        ms = (C.c_float * 8)()
+        names = (C.c_char_p * 8)()
+        ns, ne = C.c_int(), C.c_int()
+        check(lib().hf_plan_stage_times(self._plan, ms, names, C.byref(ns), C.byref(ne)))
+        return {names[k].decode(): (ms[k], ne.value) for k in range(ns.value)}
+
     def close(self) -> None:
         if self._plan:
             lib().hf_plan_destroy(self._plan)
@@ -198,5 +209,37 @@ class AngularSpectrumPlan:
     def __del__(self):
         try:
             lib().hf_as_plan_destroy(self._p)
+        except Exception:
+            pass
+
+
+class CameraStream:
+    """A device ring + window cursor bound to a Pipeline (hf_stream_*)."""
+
+    def __init__(self, pipeline: Pipeline, ring_frames: int):
+        self.pipeline = pipeline
+        self._s = C.c_void_p()
+        check(lib().hf_stream_create(pipeline._plan, ring_frames, C.byref(self._s)))
+
+    def push(self, frames: torch.Tensor, nframes: int, stream=None) -> None:
+        check(lib().hf_stream_push(self._s, _ptr(frames), nframes, _stream(stream)))
+
+    def ready(self) -> int:
+        return lib().hf_stream_ready(self._s)
+
+    def process(self, max_windows: int, out: torch.Tensor, stream=None) -> int:
+        n = C.c_int()
+        check(lib().hf_stream_process(self._s, max_windows, _ptr(out), int(not out.is_cuda), C.byref(n),
+                                      _stream(stream)))
+        return n.value
+
+    def close(self):
+        if self._s:
+            lib().hf_stream_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

@@ -1,0 +1,79 @@
+"""Device-side synthetic laser Doppler interferograms (acquisition simulator).
+
+Generates 12-bit frames on the GPU with torch for benchmarks and the streaming simulator:
+an off-axis plane reference wave (1.5 degree tilt), a circular-Gaussian speckle object on a
+centred disk propagated by an angular spectrum over ``z_obj``, a smooth Doppler map in
+[0, f_max] and frames I_t = |R + O0 exp(i 2 pi f_d t / fs)|^2 scaled to mean 2048 with Poisson
+shot noise, clipped to [0, 4095].  Frames are returned as uint16 values in an int16 tensor or
+packed to the 12-bit stream by the library's hf_pack12.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import torch
+
+
+@dataclass
+class Scene:
+    height: int
+    width: int
+    fs: float
+    disk_px: int
+    z_obj: float
+    lam: float = 852e-9
+    pitch: float = 12e-6
+    tilt_deg: float = 1.5
+    f_max: float = 18e3
+    seed: int = 1000
+
+
+class DeviceInterferograms:
+    def __init__(self, scene: Scene, device="cuda"):
+        self.s = scene
+        self.dev = torch.device(device)
+        g = torch.Generator(device=self.dev).manual_seed(scene.seed)
+        H, W = scene.height, scene.width
+        yy, xx = torch.meshgrid(torch.arange(H, device=self.dev, dtype=torch.float64),
+                                torch.arange(W, device=self.dev, dtype=torch.float64), indexing="ij")
+        disk = (torch.hypot(xx - W / 2.0, yy - H / 2.0) <= scene.disk_px / 2.0).to(torch.float64)
+        re = torch.randn((H, W), generator=g, device=self.dev, dtype=torch.float64)
+        im = torch.randn((H, W), generator=g, device=self.dev, dtype=torch.float64)
+        speck = torch.complex(re, im) / math.sqrt(2.0) * disk
+        fx = torch.fft.fftfreq(W, d=scene.pitch, device=self.dev, dtype=torch.float64)
+        fy = torch.fft.fftfreq(H, d=scene.pitch, device=self.dev, dtype=torch.float64)
+        arg = 1.0 - (scene.lam * fx[None, :]) ** 2 - (scene.lam * fy[:, None]) ** 2
+        kz = 2 * math.pi / scene.lam * torch.sqrt(torch.clamp(arg, min=0.0))
+        tf = torch.exp(1j * scene.z_obj * (kz - 2 * math.pi / scene.lam)) * (arg > 0)
+        o0 = torch.fft.ifft2(torch.fft.fft2(speck) * tf)
+        self.o0 = o0 / torch.sqrt(torch.mean(torch.abs(o0) ** 2))
+        x = torch.arange(W, device=self.dev, dtype=torch.float64) * scene.pitch
+        self.ref = torch.exp(1j * 2 * math.pi * math.sin(math.radians(scene.tilt_deg)) * x / scene.lam)[None, :]
+        noise = torch.rand((H, W), generator=g, device=self.dev, dtype=torch.float64)
+        sigma = max(H, W) / 16.0
+        gy = torch.exp(-0.5 * (torch.fft.fftfreq(H, device=self.dev, dtype=torch.float64) * 2 * math.pi * sigma) ** 2)
+        gx = torch.exp(-0.5 * (torch.fft.fftfreq(W, device=self.dev, dtype=torch.float64) * 2 * math.pi * sigma) ** 2)
+        fd = torch.fft.ifft2(torch.fft.fft2(noise) * gy[:, None] * gx[None, :]).real
+        self.fd = (fd - fd.min()) / torch.clamp(fd.max() - fd.min(), min=1e-30) * scene.f_max
+        self._g = torch.Generator(device=self.dev).manual_seed(scene.seed * 7919 + 13)
+
+    def frames(self, t0: int, n: int) -> torch.Tensor:
+        """uint16 values in an int16 tensor [n, H, W] for absolute times t0 .. t0+n-1."""
+        s = self.s
+        out = torch.empty((n, s.height, s.width), dtype=torch.int16, device=self.dev)
+        for i in range(n):
+            ot = self.o0 * torch.exp(1j * 2 * math.pi * self.fd * ((t0 + i) / s.fs))
+            inten = torch.abs(self.ref + ot) ** 2
+            inten = (inten * (2048.0 / inten.mean())).to(torch.float32)
+            noisy = torch.poisson(inten, generator=self._g)
+            out[i] = torch.clamp(noisy, 0, 4095).to(torch.int32).to(torch.int16)
+        return out
+
+
+def config1_scene(height=1024, width=1024, acquisition=0) -> Scene:
+    return Scene(height, width, 67e3, int(round(900 * width / 1024)), 0.25, seed=1000 + 1 + 17 * acquisition)
+
+
+def config0_scene(acquisition=0) -> Scene:
+    return Scene(512, 512, 37e3, 400, 0.30, seed=1000 + 17 * acquisition)

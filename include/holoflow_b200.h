@@ -195,9 +195,32 @@ int hf_plan_device_bytes(const hf_plan *plan, size_t *bytes);
 int hf_pipeline_exec(hf_plan *plan, const void *ring, int64_t ring_frames, int64_t first_frame,
                      int nwin, float *out, hf_stream_t s);
 
+/* Per-stage device timing of hf_pipeline_exec, measured with CUDA events recorded on the exec
+ * stream between stages (up to 128 execs after hf_plan_timing(plan, 1), which also resets the
+ * record).  hf_plan_stage_times sums, per stage, the elapsed milliseconds over the recorded execs
+ * (call after synchronising the stream); names[k] (optional) receives static stage names. */
+#define HF_MAX_STAGES 8
+int hf_plan_timing(hf_plan *plan, int enable);
+int hf_plan_stage_times(hf_plan *plan, float *ms, const char **names, int *nstages, int *nexec);
+
 /* Debug/inspection: after hf_pipeline_exec, copy window `w`'s T x T Gram matrix (float64) and
  * its filter+DFT matrix W (complex64 [T][Nz]) to device buffers (either may be NULL). */
 int hf_pipeline_inspect(hf_plan *plan, int w, double *gram, void *wmat, hf_stream_t s);
+
+/* ---- a3/a4: per-camera stream (replaces BatchQueue's host ring, batch_queue.cc:92-174, with a
+ * device-resident ring; overlapping windows hop < T are allowed) --------------------------------
+ * A stream owns a device ring of `ring_frames` frames of the plan's input format and a window
+ * cursor.  hf_stream_push appends frames (host or device memory; copies are enqueued on `s`;
+ * HF_ERR_INVALID if it would overwrite frames of a window not yet processed).  hf_stream_process
+ * reconstructs up to min(max_windows, max_batch) ready windows in one hf_pipeline_exec; `out` is
+ * device memory, or pinned host memory when out_is_host (a D2H copy is enqueued on `s`). */
+typedef struct hf_stream hf_stream;
+int     hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **stream);
+int     hf_stream_destroy(hf_stream *stream);
+int     hf_stream_push(hf_stream *stream, const void *frames, int64_t nframes, hf_stream_t s);
+int64_t hf_stream_ready(const hf_stream *stream);
+int     hf_stream_process(hf_stream *stream, int max_windows, float *out, int out_is_host, int *nwin,
+                          hf_stream_t s);
 
 #ifdef __cplusplus
 }
