@@ -82,6 +82,7 @@ _PROTOS = {
     "hf_pipeline_exec": (C.c_int, [_vp, _vp, _i64, _i64, C.c_int, _vp, _vp]),
     "hf_pipeline_inspect": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "hf_plan_timing": (C.c_int, [_vp, C.c_int]),
+    "hf_plan_status": (C.c_int, [_vp, C.POINTER(C.c_int), C.c_int]),
     "hf_stream_create": (C.c_int, [_vp, _i64, C.POINTER(_vp)]),
     "hf_stream_destroy": (C.c_int, [_vp]),
     "hf_stream_push": (C.c_int, [_vp, _vp, _i64, _vp]),

@@ -95,7 +95,9 @@ struct hf_plan {
   float2    *wmat = nullptr, *wmat_plain = nullptr;
   double    *gram = nullptr, *evecs = nullptr, *evals = nullptr;
   int       *info = nullptr;
+  int       *status = nullptr; // device status word: nonzero when a bounded device wait expired
   void      *cov_ws = nullptr;
+  bool       cov_tc = false;   // tensor-core Gram matrix (chosen form)
   size_t     bytes = 0;
   // optional per-stage CUDA-event timing (hf_plan_timing / hf_plan_stage_times)
   static constexpr int kSets = 128, kMarks = HF_MAX_STAGES + 1;
@@ -142,6 +144,7 @@ static void plan_free(hf_plan *p) {
   dev_free(p->evecs);
   dev_free(p->evals);
   dev_free(p->info);
+  dev_free(p->status);
   if (p->cov_ws)
     cudaFree(p->cov_ws);
   p->cov_ws = nullptr;
@@ -239,8 +242,12 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
           (rc = dev_alloc(&p->info, (size_t)B, p->bytes)) ||
           (rc = dev_alloc(&p->wmat, (size_t)(B * T * p->nz), p->bytes)))
         break;
+      p->cov_tc = d.form == HF_FORM_CHOSEN && cov_tc_supported(d.input_dtype, T, p->P, p->frame_bytes);
+      size_t wsb = cov_workspace_bytes(T, p->P, (int)B) + cov_workspace_bytes(T, p->P, 1);
+      if (p->cov_tc)
+        wsb = std::max(wsb, cov_tc_workspace_bytes(T, p->P, (int)B) + cov_tc_workspace_bytes(T, p->P, 1));
       uint8_t *ws = nullptr;
-      if ((rc = dev_alloc(&ws, cov_workspace_bytes(T, p->P, (int)B) + cov_workspace_bytes(T, p->P, 1), p->bytes)))
+      if ((rc = dev_alloc(&ws, wsb, p->bytes)))
         break;
       p->cov_ws = ws;
     } else {
@@ -249,6 +256,10 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       if ((rc = launch_band_matrix(nullptr, 1, d.frames, 0, d.z_begin, d.z_end, p->wmat_plain, stream)))
         break;
     }
+    if ((rc = dev_alloc(&p->status, 1, p->bytes)))
+      break;
+    if ((rc = cuda_status(cudaMemsetAsync(p->status, 0, sizeof(int), stream), "status reset")))
+      break;
     rc = plan_tables(p, stream);
   } while (0);
   if (rc != HF_OK) {
@@ -311,7 +322,10 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
   // 1. SVD clutter filter: Gram -> FP64 Jacobi -> W = (I - V V^T) D_band
   BandArgs ba{};
   if (d.clutter_rank > 0) {
-    HF_TRY(launch_covariance(fr, d.input_dtype, T, p->P, nwin, p->cov_ws, p->gram, s));
+    if (p->cov_tc)
+      HF_TRY(launch_covariance_tc(fr, d.input_dtype, T, p->P, nwin, p->cov_ws, p->gram, p->status, s));
+    else
+      HF_TRY(launch_covariance(fr, d.input_dtype, T, p->P, nwin, p->cov_ws, p->gram, s));
     mark(p, s, mk++, "covariance");
     HF_TRY(launch_jacobi(p->gram, p->evecs, p->evals, p->info, T, nwin, s));
     HF_TRY(launch_band_matrix(p->evecs, nwin, T, d.clutter_rank, d.z_begin, d.z_end, p->wmat, s));
@@ -500,6 +514,16 @@ int hf_plan_stage_times(hf_plan *p, float *ms, const char **names, int *nstages,
   *nstages = ns;
   if (nexec)
     *nexec = p->nexec;
+  return HF_OK;
+}
+
+int hf_plan_status(hf_plan *p, int *status, int reset) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr && status != nullptr, "hf_plan_status: null argument");
+  HF_CUDA(cudaDeviceSynchronize());
+  HF_CUDA(cudaMemcpy(status, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (reset)
+    HF_CUDA(cudaMemset(p->status, 0, sizeof(int)));
   return HF_OK;
 }
 

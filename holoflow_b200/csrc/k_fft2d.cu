@@ -21,6 +21,33 @@ namespace {
 // ------------------------------------------------------------------------------------------------
 // Row pass: one warp per row, grid-stride over the rows of every plane of a window.
 // ------------------------------------------------------------------------------------------------
+// Loads row `row` of a window's planes (zero outside the placed input) into lane registers:
+// x[n1] = sample (n2 = lane) + 32 * n1, optionally pre-multiplied.
+template <int N1>
+__device__ __forceinline__ void row_load(const RowPass &a, int w, int64_t row, int lane, float2 *x) {
+  const int plane = (int)(row / a.H), r = (int)(row % a.H);
+  const int ir    = r - a.oy;
+  const bool in_rows = ir >= 0 && ir < a.IH;
+  const int64_t ibase = w * a.in_win + plane * a.in_plane + (int64_t)ir * a.in_row;
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    const int col = lane + 32 * n1;
+    const int ic  = col - a.ox;
+    float2    v   = make_float2(0.f, 0.f);
+    if (in_rows && ic >= 0 && ic < a.IW) {
+      const int64_t off = ibase + (int64_t)ic * a.in_col;
+      v = a.in_real ? make_float2(__ldg(reinterpret_cast<const float *>(a.in) + off), 0.f)
+                    : __ldg(reinterpret_cast<const float2 *>(a.in) + off);
+      if (a.pre != nullptr)
+        v = cmul(v, __ldg(a.pre + (int64_t)r * (N1 * 32) + col));
+    }
+    x[n1] = v;
+  }
+}
+
+// Row pass: one warp per row, grid-stride over the rows of every plane of a window.  The next
+// row's loads are issued before the current row is transformed (register double buffer), so
+// each warp keeps one row of HBM traffic in flight while it computes.
 template <int N1, bool INV> __global__ void __launch_bounds__(256) row_pass_kernel(RowPass a) {
   constexpr int N = N1 * 32;
   extern __shared__ __align__(16) float smf[];
@@ -32,33 +59,21 @@ template <int N1, bool INV> __global__ void __launch_bounds__(256) row_pass_kern
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   float2   *xb   = xball + warp * XBuf<N1>::kSize;
   const int w    = blockIdx.y;
-  const int64_t nrows = (int64_t)a.nplanes * a.H;
-  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
-       row += (int64_t)gridDim.x * nwarps) {
+  const int64_t nrows  = (int64_t)a.nplanes * a.H;
+  const int64_t stride = (int64_t)gridDim.x * nwarps;
+  int64_t row = (int64_t)blockIdx.x * nwarps + warp;
+  float2  nxt[N1];
+  if (row < nrows)
+    row_load<N1>(a, w, row, lane, nxt);
+  for (; row < nrows; row += stride) {
+    float2 x[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1)
+      x[n1] = nxt[n1];
+    if (row + stride < nrows)
+      row_load<N1>(a, w, row + stride, lane, nxt);
     const int plane = (int)(row / a.H), r = (int)(row % a.H);
     float2   *orow  = a.out + w * a.out_win + plane * a.out_plane + r * a.out_row;
-    const int ir    = r - a.oy;
-    if (ir < 0 || ir >= a.IH) {
-      for (int i = lane; i < N; i += 32)
-        orow[i] = make_float2(0.f, 0.f);
-      continue;
-    }
-    float2 x[N1];
-    const int64_t ibase = w * a.in_win + plane * a.in_plane + (int64_t)ir * a.in_row;
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      const int col = lane + 32 * n1;
-      const int ic  = col - a.ox;
-      float2    v   = make_float2(0.f, 0.f);
-      if (ic >= 0 && ic < a.IW) {
-        const int64_t off = ibase + (int64_t)ic * a.in_col;
-        v = a.in_real ? make_float2(__ldg(reinterpret_cast<const float *>(a.in) + off), 0.f)
-                      : __ldg(reinterpret_cast<const float2 *>(a.in) + off);
-        if (a.pre != nullptr)
-          v = cmul(v, __ldg(a.pre + (int64_t)r * N + col));
-      }
-      x[n1] = v;
-    }
     four_step_a<N1, INV>(x, lane, tw, xb);
     __syncwarp();
     for (int k1 = lane; k1 < N1; k1 += 32) {
@@ -99,14 +114,30 @@ __global__ void __launch_bounds__(32 * C) col_pass_kernel(ColPass a, MomentSpec 
   }
   __syncthreads();
 
-  const int p_begin = MODE == COL_MOMENTS ? 0 : blockIdx.y;
-  const int p_end   = MODE == COL_MOMENTS ? a.nplanes : blockIdx.y + 1;
-  for (int plane = p_begin; plane < p_end; ++plane) {
-    const float2 *src = a.in + w * a.in_win + plane * a.in_plane + col;
-    float2        x[N1];
+  // work items: (plane) for the moments mode (the CTA owns its strip across planes), otherwise
+  // (plane) for a fixed strip with the grid's y dimension striding over planes
+  const int p_begin  = MODE == COL_MOMENTS ? 0 : blockIdx.y;
+  const int p_end    = a.nplanes;
+  const int p_stride = MODE == COL_MOMENTS ? 1 : gridDim.y;
+  float2    nxt[N1];
+  {
+    const float2 *src = a.in + w * a.in_win + (int64_t)p_begin * a.in_plane + col;
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1)
-      x[n1] = valid ? __ldg(src + (int64_t)(n2 + 32 * n1) * a.in_row) : make_float2(0.f, 0.f);
+      nxt[n1] = (valid && p_begin < p_end) ? __ldg(src + (int64_t)(n2 + 32 * n1) * a.in_row)
+                                           : make_float2(0.f, 0.f);
+  }
+  for (int plane = p_begin; plane < p_end; plane += p_stride) {
+    float2 x[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1)
+      x[n1] = nxt[n1];
+    if (plane + p_stride < p_end) {
+      const float2 *src = a.in + w * a.in_win + (int64_t)(plane + p_stride) * a.in_plane + col;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1)
+        nxt[n1] = valid ? __ldg(src + (int64_t)(n2 + 32 * n1) * a.in_row) : make_float2(0.f, 0.f);
+    }
     four_step_a<N1, INV>(x, n2, tw, xb);
     __syncthreads();
 
@@ -330,6 +361,10 @@ int launch_col_fast(const ColPass &a, int mode, const MomentSpec &m, int nwin, c
   constexpr int C = N1 <= 32 ? 8 : 4;
   const size_t  base = 2 * N * sizeof(float) + C * XBuf<N1>::kSize * sizeof(float2);
   const int     strips = (a.W + C - 1) / C;
+  // CTAs along planes: enough for ~2 CTAs per SM overall, each striding over the rest
+  const int64_t want       = std::max<int64_t>(1, (2LL * sm_count() + (int64_t)strips * nwin - 1) /
+                                                    ((int64_t)strips * nwin));
+  const int     plane_grid = (int)std::min<int64_t>(a.nplanes, want);
   switch (mode) {
 #define HF_COL_CASE(MODE, EXTRA, PLANES)                                                           \
   case MODE: {                                                                                     \
@@ -340,8 +375,8 @@ int launch_col_fast(const ColPass &a, int mode, const MomentSpec &m, int nwin, c
     note_launch();                                                                                 \
     return launch_status("col_pass_kernel");                                                       \
   }
-    HF_COL_CASE(COL_COMPLEX, 0, a.nplanes)
-    HF_COL_CASE(COL_MAGNITUDE, 0, a.nplanes)
+    HF_COL_CASE(COL_COMPLEX, 0, plane_grid)
+    HF_COL_CASE(COL_MAGNITUDE, 0, plane_grid)
     HF_COL_CASE(COL_MOMENTS, (size_t)3 * N * C * sizeof(float), 1)
 #undef HF_COL_CASE
   case COL_TF_SANDWICH:
@@ -350,7 +385,7 @@ int launch_col_fast(const ColPass &a, int mode, const MomentSpec &m, int nwin, c
       HF_CUDA(cudaFuncSetAttribute(col_pass_kernel<N1, C, INV, COL_TF_SANDWICH>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       col_pass_kernel<N1, C, INV, COL_TF_SANDWICH>
-          <<<dim3(strips, a.nplanes, nwin), 32 * C, smem, s>>>(a, m);
+          <<<dim3(strips, plane_grid, nwin), 32 * C, smem, s>>>(a, m);
       note_launch();
       return launch_status("col_pass_kernel");
     }

@@ -219,10 +219,7 @@ int launch_cov_tiled(const FrameRing &ring, int64_t P, int nwin, void *ws, doubl
   cov_tiled_kernel<FMT, T><<<dim3(ctas, nwin), Gm::THR, smem, s>>>(a);
   note_launch();
   HF_TRY(launch_status("cov_tiled_kernel"));
-  cov_finalize_kernel<<<dim3((T * T + 255) / 256, nwin), 256, 0, s>>>(
-      a.partial, a.sums, a.nblk, ctas, T, P, (double)a.shift, gram);
-  note_launch();
-  return launch_status("cov_finalize_kernel");
+  return launch_cov_finalize(a.partial, a.sums, a.nblk, ctas, T, P, (double)a.shift, gram, nwin, s);
 }
 
 template <int FMT>
@@ -272,9 +269,15 @@ __device__ __forceinline__ int sym_idx(int i, int j, int np) {
 
 // Parallel cyclic Jacobi (round-robin pairing, np/2 disjoint rotations per step).  The matrix is
 // kept as a packed upper triangle and the rotation accumulator transposed (Vt[p][:] = V[:, p]),
-// both in shared memory: 194 KB at n = 128.
-__global__ void __launch_bounds__(512) jacobi_kernel(const double *a_in, double *evecs,
-                                                     double *evals, int *info, int n) {
+// both in shared memory (194 KB at n = 128).  Every thread owns a fixed set of 2x2 blocks (k, l)
+// and accumulator entries for the whole solve, so a step is: rotations of the np/2 pairs,
+// barrier, block and accumulator updates, barrier.
+constexpr int kJacobiThreads = 1024;
+constexpr int kJacobiMaxBlk  = 3;  // 2x2 blocks per thread: ceil(65*64/2 / 1024)
+constexpr int kJacobiMaxV    = 8;  // accumulator entries per thread: 64*128 / 1024
+
+__global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(const double *a_in, double *evecs,
+                                                                double *evals, int *info, int n) {
   extern __shared__ __align__(16) double dsm[];
   const int np   = n + (n & 1);
   const int half = np / 2;
@@ -299,6 +302,25 @@ __global__ void __launch_bounds__(512) jacobi_kernel(const double *a_in, double 
       A[sym_idx(i, j, np)] = v;
     }
   }
+  // this thread's fixed work items
+  const int nblocks = half * (half + 1) / 2;
+  int       bk[kJacobiMaxBlk], bl[kJacobiMaxBlk], nb = 0;
+  for (int e = tid; e < nblocks && nb < kJacobiMaxBlk; e += nt) {
+    int k = 0, rem = e;
+    while (rem >= half - k) {
+      rem -= half - k;
+      ++k;
+    }
+    bk[nb] = k;
+    bl[nb] = k + rem;
+    ++nb;
+  }
+  int vk[kJacobiMaxV], vj[kJacobiMaxV], nv = 0;
+  for (int f = tid; f < half * np && nv < kJacobiMaxV; f += nt) {
+    vk[nv] = f / np;
+    vj[nv] = f % np;
+    ++nv;
+  }
   __syncthreads();
 
   const int max_sweeps = 40;
@@ -322,7 +344,7 @@ __global__ void __launch_bounds__(512) jacobi_kernel(const double *a_in, double 
             t = 0.5 / theta;
           else
             t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-          c = 1.0 / sqrt(t * t + 1.0);
+          c = rsqrt(t * t + 1.0);
           s = t * c;
           flag[0] = 1;
         }
@@ -332,48 +354,45 @@ __global__ void __launch_bounds__(512) jacobi_kernel(const double *a_in, double 
         pq[2 * tid + 1] = q;
       }
       __syncthreads();
-      // two-sided update of the 2x2 blocks (k <= l) and of the accumulator rows
-      const int nblocks = half * (half + 1) / 2;
-      for (int e = tid; e < nblocks + half * np; e += nt) {
-        if (e < nblocks) {
-          int k = 0, rem = e;
-          while (rem >= half - k) {
-            rem -= half - k;
-            ++k;
-          }
-          const int    l  = k + rem;
-          const double ck = cs[2 * k], sk = cs[2 * k + 1], cl = cs[2 * l], sl = cs[2 * l + 1];
-          if (sk == 0.0 && sl == 0.0)
-            continue;
-          const int pk = pq[2 * k], qk = pq[2 * k + 1], pl = pq[2 * l], ql = pq[2 * l + 1];
-          const int i00 = sym_idx(pk, pl, np), i01 = sym_idx(pk, ql, np);
-          const int i10 = sym_idx(qk, pl, np), i11 = sym_idx(qk, ql, np);
-          const double b00 = A[i00], b01 = A[i01], b10 = A[i10], b11 = A[i11];
-          // M = B J_l ;  B' = J_k^T M   with J = [[c, s], [-s, c]]
-          const double m00 = cl * b00 - sl * b01, m01 = sl * b00 + cl * b01;
-          const double m10 = cl * b10 - sl * b11, m11 = sl * b10 + cl * b11;
-          const double n00 = ck * m00 - sk * m10, n01 = ck * m01 - sk * m11;
-          const double n10 = sk * m00 + ck * m10, n11 = sk * m01 + ck * m11;
-          if (k == l) { // diagonal block: i01 == i10 is the annihilated entry
-            A[i00] = n00;
-            A[i11] = n11;
-            A[i01] = 0.0;
-          } else {
-            A[i00] = n00;
-            A[i01] = n01;
-            A[i10] = n10;
-            A[i11] = n11;
-          }
+#pragma unroll
+      for (int b = 0; b < kJacobiMaxBlk; ++b) {
+        if (b >= nb)
+          break;
+        const int    k = bk[b], l = bl[b];
+        const double ck = cs[2 * k], sk = cs[2 * k + 1], cl = cs[2 * l], sl = cs[2 * l + 1];
+        if (sk == 0.0 && sl == 0.0)
+          continue;
+        const int pk = pq[2 * k], qk = pq[2 * k + 1], pl = pq[2 * l], ql = pq[2 * l + 1];
+        const int i00 = sym_idx(pk, pl, np), i01 = sym_idx(pk, ql, np);
+        const int i10 = sym_idx(qk, pl, np), i11 = sym_idx(qk, ql, np);
+        const double b00 = A[i00], b01 = A[i01], b10 = A[i10], b11 = A[i11];
+        // M = B J_l ;  B' = J_k^T M   with J = [[c, s], [-s, c]]
+        const double m00 = cl * b00 - sl * b01, m01 = sl * b00 + cl * b01;
+        const double m10 = cl * b10 - sl * b11, m11 = sl * b10 + cl * b11;
+        const double n00 = ck * m00 - sk * m10, n01 = ck * m01 - sk * m11;
+        const double n10 = sk * m00 + ck * m10, n11 = sk * m01 + ck * m11;
+        if (k == l) { // diagonal block: i01 == i10 is the annihilated entry
+          A[i00] = n00;
+          A[i11] = n11;
+          A[i01] = 0.0;
         } else {
-          const int    f = e - nblocks;
-          const int    k = f / np, j = f % np;
-          const double c = cs[2 * k], s = cs[2 * k + 1];
-          if (s != 0.0) {
-            const int    p = pq[2 * k], q = pq[2 * k + 1];
-            const double vp = Vt[p * np + j], vq = Vt[q * np + j];
-            Vt[p * np + j] = c * vp - s * vq;
-            Vt[q * np + j] = s * vp + c * vq;
-          }
+          A[i00] = n00;
+          A[i01] = n01;
+          A[i10] = n10;
+          A[i11] = n11;
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < kJacobiMaxV; ++v) {
+        if (v >= nv)
+          break;
+        const int    k = vk[v], j = vj[v];
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        if (s != 0.0) {
+          const int    p = pq[2 * k], q = pq[2 * k + 1];
+          const double vp = Vt[p * np + j], vq = Vt[q * np + j];
+          Vt[p * np + j] = c * vp - s * vq;
+          Vt[q * np + j] = s * vp + c * vq;
         }
       }
       __syncthreads();
@@ -471,6 +490,14 @@ __global__ void pca_project_kernel(const float *in, int T, int64_t P, const doub
 
 } // namespace
 
+int launch_cov_finalize(const float *partial, const double *sums, int nblk, int nsum, int T, int64_t P,
+                        double shift, double *gram, int nwin, cudaStream_t s) {
+  cov_finalize_kernel<<<dim3((T * T + 255) / 256, nwin), 256, 0, s>>>(partial, sums, nblk, nsum, T, P, shift,
+                                                                      gram);
+  note_launch();
+  return launch_status("cov_finalize_kernel");
+}
+
 size_t cov_workspace_bytes(int T, int64_t P, int nwin) {
   const int ctas = cov_ctas_per_window(P, nwin);
   const int G    = T == 32 ? 4 : (T == 64 ? 2 : 1);
@@ -496,7 +523,7 @@ int launch_jacobi(const double *a, double *evecs, double *evals, int *info, int 
   const size_t smem = (size_t)(np * (np + 1) / 2) * 8 + (size_t)np * np * 8 + (size_t)np * 8 +
                       (size_t)np * 4 + 16;
   HF_CUDA(cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  jacobi_kernel<<<(unsigned)batch, 512, smem, s>>>(a, evecs, evals, info, n);
+  jacobi_kernel<<<(unsigned)batch, kJacobiThreads, smem, s>>>(a, evecs, evals, info, n);
   note_launch();
   return launch_status("jacobi_kernel");
 }

@@ -19,6 +19,16 @@ struct CovArgs {
 };
 
 size_t cov_workspace_bytes(int T, int64_t P, int nwin);
+// Deterministic float64 reduction of block partials; undoes the sample shift exactly.
+int launch_cov_finalize(const float *partial, const double *sums, int nblk, int nsum, int T, int64_t P,
+                        double shift, double *gram, int nwin, cudaStream_t s);
+
+// Tensor-core (tcgen05, f16 operands, f32 accumulation) Gram matrix for 8/12/16-bit samples and
+// T in {64, 128}; `status` receives a nonzero code if a bounded mbarrier wait expires.
+bool   cov_tc_supported(int fmt, int T, int64_t P, int64_t frame_bytes);
+size_t cov_tc_workspace_bytes(int T, int64_t P, int nwin);
+int    launch_covariance_tc(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, void *ws,
+                            double *gram, int *status, cudaStream_t s);
 // Full Gram computation: block partials -> deterministic float64 reduction -> gram[nwin][T][T].
 int launch_covariance(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, void *ws,
                       double *gram, cudaStream_t s);

@@ -1,0 +1,420 @@
+// Tensor-core (tcgen05) Gram matrix of a window's frames — the chosen form's covariance.
+//
+// G' = (X - 2048)^T (X - 2048) with X = [T][P] 12-bit samples: (x - 2048) is exact in f16, the
+// products are exact in the f32 accumulator, and the shift is undone in float64 by the shared
+// finalize kernel (k_pca.cu) from exact integer frame sums.  Per CTA: a ring of 4 shared-memory
+// stages of 128 pixels x T frames in the canonical K-major 128-byte-swizzled layout (rows = frames,
+// K = pixels).  All threads unpack the next stage while the tensor core consumes the previous ones;
+// one thread issues M = N = T, K = 16 MMAs (A and B are the same tile) into a TMEM accumulator and
+// commits each stage to its mbarrier, which gates the stage's reuse.
+#include <cuda_fp16.h>
+
+#include "k_pca.cuh"
+#include "tc_common.cuh"
+
+namespace hf {
+
+namespace {
+
+constexpr int kTcPX     = 128; // pixels per stage (two K-subtiles of 64)
+constexpr int kTcStages = 4;
+
+template <int FMT> struct TcBpp;
+template <> struct TcBpp<HF_MONO12P> { static constexpr int num = 3, den = 2, words = 3; };
+template <> struct TcBpp<HF_U16> { static constexpr int num = 2, den = 1, words = 4; };
+template <> struct TcBpp<HF_U8> { static constexpr int num = 1, den = 1, words = 2; };
+
+template <int FMT> __device__ __forceinline__ void unpack_group(const uint32_t *w, uint32_t (&v)[8]) {
+  if constexpr (FMT == HF_MONO12P) {
+    unpack8(w[0], w[1], w[2], v);
+  } else if constexpr (FMT == HF_U16) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      v[2 * i]     = w[i] & 0xFFFFu;
+      v[2 * i + 1] = w[i] >> 16;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        v[4 * i + j] = (w[i] >> (8 * j)) & 0xFFu;
+  }
+}
+
+template <int FMT, int T>
+__global__ void __launch_bounds__(128) cov_tc_kernel(CovArgs a, int *status) {
+  constexpr int SUB   = T * 128;       // bytes of one 64-pixel K-subtile (T rows x 128 B)
+  constexpr int STAGE = 2 * SUB;       // 128 pixels
+  constexpr int NCOL  = T == 64 ? 64 : 128;
+  constexpr int TPT   = T * 16 / 128;  // (frame, 8-pixel group) items per thread per stage
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte alignment of the swizzle atoms
+  uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t *mbar  = reinterpret_cast<uint64_t *>(smem + kTcStages * STAGE);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + kTcStages);
+  unsigned long long *ssum = reinterpret_cast<unsigned long long *>(tslot + 2);
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int w   = blockIdx.y;
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s)
+      tc::mbar_init(&mbar[s], 1);
+    tc::mbar_fence_init();
+  }
+  for (int t = tid; t < T; t += blockDim.x)
+    ssum[t] = 0ull;
+  if (warp == 0)
+    tc::tmem_alloc(tslot, NCOL);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *tslot;
+  constexpr uint32_t idesc = tc::idesc_f16(T, T, false, false);
+
+  // this thread's fixed (frame, group) items: t = tid/16 + 8k, g = tid % 16
+  const int g = tid & 15;
+  uint32_t  isum[TPT];
+#pragma unroll
+  for (int k = 0; k < TPT; ++k)
+    isum[k] = 0u;
+
+  const int64_t ntiles = (a.P + kTcPX - 1) / kTcPX;
+  int           nj     = 0;
+  bool          ok     = true;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++nj) {
+    const int s = nj % kTcStages;
+    bool      w_ok = true;
+    if (nj >= kTcStages)
+      w_ok = tc::mbar_wait_bounded(&mbar[s], (uint32_t)((nj / kTcStages) - 1) & 1u, status, 1);
+    ok = __syncthreads_and(w_ok) != 0; // uniform: every thread leaves together on a timeout
+    if (!ok)
+      break;
+    uint8_t      *st = smem + s * STAGE;
+    const int64_t p  = tile * kTcPX + g * 8;
+    const bool    valid = p < a.P;
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      const int t = (tid >> 4) + 8 * k;
+      uint32_t  v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (valid) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(a.ring.frame(w, t) +
+                                                                 p * TcBpp<FMT>::num / TcBpp<FMT>::den);
+        uint32_t wv[TcBpp<FMT>::words];
+#pragma unroll
+        for (int i = 0; i < TcBpp<FMT>::words; ++i)
+          wv[i] = __ldg(src + i);
+        unpack_group<FMT>(wv, v);
+      }
+      __half2 h[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        isum[k] += valid ? v[2 * i] + v[2 * i + 1] : 0u;
+        const float x0 = valid ? (float)v[2 * i] - a.shift : 0.f;
+        const float x1 = valid ? (float)v[2 * i + 1] - a.shift : 0.f;
+        h[i] = __floats2half2_rn(x0, x1);
+      }
+      const int sub = g >> 3, c = g & 7;
+      uint4    *dst = reinterpret_cast<uint4 *>(st + sub * SUB + t * 128 + ((c ^ (t & 7)) << 4));
+      *dst = *reinterpret_cast<const uint4 *>(h);
+    }
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int sub = 0; sub < 2; ++sub)
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+          const uint64_t d = tc::sw128_desc(tc::smem_u32(st + sub * SUB + ks * 32), 16, 1024);
+          tc::mma_f16(tbase, d, d, idesc, (nj > 0 || sub > 0 || ks > 0) ? 1u : 0u);
+        }
+      tc::mma_commit(&mbar[s]);
+    }
+  }
+  // drain: the last commit covers every MMA issued before it
+  if (nj > 0 && ok) {
+    const int last = nj - 1;
+    ok = tc::mbar_wait_bounded(&mbar[last % kTcStages], (uint32_t)(last / kTcStages) & 1u, status, 2);
+  }
+  ok = __syncthreads_and(ok) != 0;
+  tc::fence_after_sync();
+#pragma unroll
+  for (int k = 0; k < TPT; ++k)
+    atomicAdd(&ssum[(tid >> 4) + 8 * k], (unsigned long long)isum[k]);
+
+  const int64_t pidx = ((int64_t)w * a.nblk + blockIdx.x) * T * T;
+  if constexpr (T == 64) {
+    // M = 64 accumulator: row m sits in TMEM lane 32*(m/16) + m%16 (the lower half of each
+    // 32-lane subpartition), columns 0..63 hold N = 0..63
+    uint32_t r0[32], r1[32];
+    tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16), r0);
+    tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + 32, r1);
+    tc::tmem_wait_ld();
+    const int i = tid & 31;
+    if (i < 16) {
+      const int m = 16 * warp + i;
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        a.partial[pidx + m * T + c]      = (nj > 0 && ok) ? __uint_as_float(r0[c]) : 0.f;
+        a.partial[pidx + m * T + 32 + c] = (nj > 0 && ok) ? __uint_as_float(r1[c]) : 0.f;
+      }
+    }
+  } else {
+    const int m = 32 * warp + (tid & 31);
+#pragma unroll
+    for (int cb = 0; cb < 4; ++cb) {
+      uint32_t r[32];
+      tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + 32 * cb, r);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int c = 0; c < 32; ++c)
+        a.partial[pidx + m * T + 32 * cb + c] = (nj > 0 && ok) ? __uint_as_float(r[c]) : 0.f;
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  for (int t = tid; t < T; t += blockDim.x)
+    a.sums[((int64_t)w * gridDim.x + blockIdx.x) * T + t] = (double)ssum[t];
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tbase, NCOL);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Exact integer variant for samples of at most 12 bits: x - shift = 64 h + l with h in [-32, 31],
+// l in [0, 63] (both int8).  The stage holds R = 2T K-major rows [h of every frame; l of every
+// frame]; one kind::i8 MMA per 32-pixel K-step and 128-row M-block yields D = [H; L][H; L]^T in
+// int32, and G' = 4096 HH + 64 (HL + LH) + LL is folded into a per-window int64 accumulator with
+// integer atomics (exact, so the result does not depend on their order).
+// ------------------------------------------------------------------------------------------------
+template <int FMT, int T>
+__global__ void __launch_bounds__(128) cov_tc_i8_kernel(FrameRing ring, int64_t P, float shift,
+                                                      unsigned long long *acc, unsigned long long *sums,
+                                                      int *status) {
+  constexpr int R     = 2 * T;           // operand rows
+  constexpr int STAGE = R * 128;         // 128 pixels (int8 K) per row
+  constexpr int NMB   = R / 128;         // 128-row M-blocks
+  constexpr int NCOL  = NMB * R;         // TMEM columns (int32)
+  constexpr int TPT   = T * 16 / 128;    // (frame, 8-pixel group) items per thread
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t *mbar  = reinterpret_cast<uint64_t *>(smem + kTcStages * STAGE);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + kTcStages);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int w   = blockIdx.y;
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s)
+      tc::mbar_init(&mbar[s], 1);
+    tc::mbar_fence_init();
+  }
+  if (warp == 0)
+    tc::tmem_alloc(tslot, NCOL);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *tslot;
+  constexpr uint32_t idesc = tc::idesc_i8(128, R, false, false);
+
+  const int g = tid & 15;
+  uint32_t  isum[TPT];
+#pragma unroll
+  for (int k = 0; k < TPT; ++k)
+    isum[k] = 0u;
+  const int ishift = (int)shift;
+
+  const int64_t ntiles = (P + kTcPX - 1) / kTcPX;
+  int           nj     = 0;
+  bool          ok     = true;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++nj) {
+    const int s = nj % kTcStages;
+    bool      w_ok = true;
+    if (nj >= kTcStages)
+      w_ok = tc::mbar_wait_bounded(&mbar[s], (uint32_t)((nj / kTcStages) - 1) & 1u, status, 3);
+    ok = __syncthreads_and(w_ok) != 0;
+    if (!ok)
+      break;
+    uint8_t      *st    = smem + s * STAGE;
+    const int64_t p     = tile * kTcPX + g * 8;
+    const bool    valid = p < P;
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      const int t = (tid >> 4) + 8 * k;
+      uint32_t  v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (valid) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(ring.frame(w, t) +
+                                                                 p * TcBpp<FMT>::num / TcBpp<FMT>::den);
+        uint32_t wv[TcBpp<FMT>::words];
+#pragma unroll
+        for (int i = 0; i < TcBpp<FMT>::words; ++i)
+          wv[i] = __ldg(src + i);
+        unpack_group<FMT>(wv, v);
+      }
+      uint32_t hw[2] = {0, 0}, lw[2] = {0, 0};
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        isum[k] += v[i];
+        const int d = valid ? (int)v[i] - ishift : 0;      // in [-2048, 2047]
+        const int h = d >> 6;                              // floor division: [-32, 31]
+        const int l = d & 63;                              // [0, 63]
+        hw[i >> 2] |= (uint32_t)(h & 0xFF) << (8 * (i & 3));
+        lw[i >> 2] |= (uint32_t)l << (8 * (i & 3));
+      }
+      const int c = g >> 1, half = g & 1;
+      *reinterpret_cast<uint2 *>(st + t * 128 + ((c ^ (t & 7)) << 4) + half * 8) = make_uint2(hw[0], hw[1]);
+      const int tl = T + t;
+      *reinterpret_cast<uint2 *>(st + tl * 128 + ((c ^ (tl & 7)) << 4) + half * 8) = make_uint2(lw[0], lw[1]);
+    }
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const uint64_t bdesc = tc::sw128_desc(tc::smem_u32(st + ks * 32), 16, 1024);
+#pragma unroll
+        for (int mb = 0; mb < NMB; ++mb) {
+          const uint64_t adesc = tc::sw128_desc(tc::smem_u32(st + mb * 128 * 128 + ks * 32), 16, 1024);
+          tc::mma_i8(tbase + mb * R, adesc, bdesc, idesc, (nj > 0 || ks > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(&mbar[s]);
+    }
+  }
+  if (nj > 0 && ok) {
+    const int last = nj - 1;
+    ok = tc::mbar_wait_bounded(&mbar[last % kTcStages], (uint32_t)(last / kTcStages) & 1u, status, 4);
+  }
+  ok = __syncthreads_and(ok) != 0;
+  tc::fence_after_sync();
+#pragma unroll
+  for (int k = 0; k < TPT; ++k)
+    atomicAdd(&sums[(int64_t)w * T + (tid >> 4) + 8 * k], (unsigned long long)isum[k]);
+  if (nj > 0 && ok) {
+    unsigned long long *aw = acc + (int64_t)w * T * T;
+#pragma unroll
+    for (int mb = 0; mb < NMB; ++mb) {
+      const int row = mb * 128 + 32 * warp + (tid & 31); // operand row held by this thread
+      const bool is_h = row < T;
+      const int  a    = is_h ? row : row - T;
+      // this row's contribution to G'[a][b]: h-row -> 4096 HH + 64 HL, l-row -> 64 LH + LL
+      const long long wa = is_h ? 4096 : 64, wb = is_h ? 64 : 1;
+#pragma unroll
+      for (int cb = 0; cb < T / 32; ++cb) {
+        uint32_t r0[32], r1[32];
+        tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + mb * R + 32 * cb, r0);
+        tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + mb * R + T + 32 * cb, r1);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const long long v = wa * (long long)(int)r0[c] + wb * (long long)(int)r1[c];
+          atomicAdd(&aw[a * T + 32 * cb + c], (unsigned long long)v);
+        }
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tbase, NCOL);
+  }
+}
+
+// int64 accumulator -> float64 Gram with the shift undone exactly.
+__global__ void cov_i8_finalize_kernel(const unsigned long long *acc, const unsigned long long *sums, int T,
+                                       int64_t P, long long shift, double *gram) {
+  const int w = blockIdx.y;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= T * T)
+    return;
+  const int       i = e / T, j = e % T;
+  const long long g = (long long)acc[(int64_t)w * T * T + e] +
+                      shift * (long long)(sums[(int64_t)w * T + i] + sums[(int64_t)w * T + j]) -
+                      shift * shift * (long long)P;
+  gram[(int64_t)w * T * T + e] = (double)g;
+}
+
+template <int FMT, int T>
+int launch_tc(const FrameRing &ring, int64_t P, int nwin, void *ws, double *gram, int *status,
+              cudaStream_t s) {
+  const size_t smem = 1024 + (size_t)kTcStages * 2 * T * 128 + kTcStages * 8 + 8 + T * 8;
+  const int64_t ntiles = (P + kTcPX - 1) / kTcPX;
+  int ctas = (int)std::max<int64_t>(1, std::min<int64_t>((3LL * sm_count() + nwin - 1) / nwin, ntiles));
+  CovArgs a;
+  a.ring    = ring;
+  a.T       = T;
+  a.P       = P;
+  a.shift   = FMT == HF_U8 ? 128.f : 2048.f;
+  a.nblk    = ctas;
+  a.partial = reinterpret_cast<float *>(ws);
+  a.sums    = reinterpret_cast<double *>(reinterpret_cast<uint8_t *>(ws) +
+                                      (size_t)nwin * ctas * T * T * sizeof(float));
+  HF_CUDA(cudaFuncSetAttribute(cov_tc_kernel<FMT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cov_tc_kernel<FMT, T><<<dim3(ctas, nwin), 128, smem, s>>>(a, status);
+  note_launch();
+  HF_TRY(launch_status("cov_tc_kernel"));
+  return launch_cov_finalize(a.partial, a.sums, a.nblk, ctas, T, P, (double)a.shift, gram, nwin, s);
+}
+
+template <int FMT, int T>
+int launch_tc_i8(const FrameRing &ring, int64_t P, int nwin, void *ws, double *gram, int *status,
+                 cudaStream_t s) {
+  constexpr int R    = 2 * T;
+  const size_t  smem = 1024 + (size_t)kTcStages * R * 128 + kTcStages * 8 + 8;
+  const int64_t ntiles = (P + kTcPX - 1) / kTcPX;
+  // at most ~256K pixels per CTA keeps every int32 accumulator entry below 63*63*256K < 2^31
+  const int64_t min_ctas = (P + (1 << 18) - 1) >> 18;
+  const int     per_sm   = T == 64 ? 3 : 1;
+  int ctas = (int)std::max<int64_t>(min_ctas, std::min<int64_t>(((int64_t)per_sm * sm_count() + nwin - 1) / nwin, ntiles));
+  auto *acc  = reinterpret_cast<unsigned long long *>(ws);
+  auto *sums = acc + (size_t)nwin * T * T;
+  HF_CUDA(cudaMemsetAsync(acc, 0, ((size_t)nwin * T * T + (size_t)nwin * T) * sizeof(unsigned long long), s));
+  HF_CUDA(cudaFuncSetAttribute(cov_tc_i8_kernel<FMT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cov_tc_i8_kernel<FMT, T><<<dim3(ctas, nwin), 128, smem, s>>>(ring, P, FMT == HF_U8 ? 128.f : 2048.f, acc, sums,
+                                                               status);
+  note_launch();
+  HF_TRY(launch_status("cov_tc_i8_kernel"));
+  cov_i8_finalize_kernel<<<dim3((T * T + 255) / 256, nwin), 256, 0, s>>>(acc, sums, T, P,
+                                                                        FMT == HF_U8 ? 128 : 2048, gram);
+  note_launch();
+  return launch_status("cov_i8_finalize_kernel");
+}
+
+} // namespace
+
+size_t cov_tc_workspace_bytes(int T, int64_t P, int nwin) {
+  const int64_t ntiles = (P + kTcPX - 1) / kTcPX;
+  const int64_t ctas   = std::max<int64_t>(1, std::min<int64_t>((3LL * sm_count() + nwin - 1) / nwin, ntiles));
+  const size_t f16 = (size_t)(nwin * ctas) * T * T * sizeof(float) + (size_t)(nwin * ctas) * T * sizeof(double) + 256;
+  const size_t i8  = ((size_t)nwin * T * T + (size_t)nwin * T) * sizeof(unsigned long long) + 256;
+  return std::max(f16, i8);
+}
+
+bool cov_tc_supported(int fmt, int T, int64_t P, int64_t frame_bytes) {
+  return (fmt == HF_MONO12P || fmt == HF_U16 || fmt == HF_U8) && (T == 64 || T == 128) && P % 8 == 0 &&
+         frame_bytes % 4 == 0;
+}
+
+int launch_covariance_tc(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, void *ws,
+                         double *gram, int *status, cudaStream_t s) {
+  HF_CHECK_ARG(cov_tc_supported(fmt, T, P, ring.frame_bytes), "tensor-core covariance: unsupported shape");
+  // samples of at most 12 bits: exact int8 split; 16-bit samples: f16 operands
+  if (fmt == HF_MONO12P)
+    return T == 64 ? launch_tc_i8<HF_MONO12P, 64>(ring, P, nwin, ws, gram, status, s)
+                   : launch_tc_i8<HF_MONO12P, 128>(ring, P, nwin, ws, gram, status, s);
+  if (fmt == HF_U8)
+    return T == 64 ? launch_tc_i8<HF_U8, 64>(ring, P, nwin, ws, gram, status, s)
+                   : launch_tc_i8<HF_U8, 128>(ring, P, nwin, ws, gram, status, s);
+  if (T == 64) {
+    if (fmt == HF_MONO12P) return launch_tc<HF_MONO12P, 64>(ring, P, nwin, ws, gram, status, s);
+    if (fmt == HF_U16) return launch_tc<HF_U16, 64>(ring, P, nwin, ws, gram, status, s);
+    return launch_tc<HF_U8, 64>(ring, P, nwin, ws, gram, status, s);
+  }
+  if (fmt == HF_MONO12P) return launch_tc<HF_MONO12P, 128>(ring, P, nwin, ws, gram, status, s);
+  if (fmt == HF_U16) return launch_tc<HF_U16, 128>(ring, P, nwin, ws, gram, status, s);
+  return launch_tc<HF_U8, 128>(ring, P, nwin, ws, gram, status, s);
+}
+
+} // namespace hf

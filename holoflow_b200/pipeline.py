@@ -138,6 +138,11 @@ class Pipeline:
         check(lib().hf_pipeline_inspect(self._plan, w, _ptr(gram), _ptr(wm), _stream()))
         return gram, wm
 
+    def status(self, reset: bool = True) -> int:
+        st = C.c_int()
+        check(lib().hf_plan_status(self._plan, C.byref(st), int(reset)))
+        return st.value
+
     def timing(self, enable: bool) -> None:
         check(lib().hf_plan_timing(self._plan, int(enable)))
 

@@ -203,6 +203,10 @@ int hf_pipeline_exec(hf_plan *plan, const void *ring, int64_t ring_frames, int64
 int hf_plan_timing(hf_plan *plan, int enable);
 int hf_plan_stage_times(hf_plan *plan, float *ms, const char **names, int *nstages, int *nexec);
 
+/* Device status word of the plan (synchronises the device): 0, or the code of the first bounded
+ * device-side wait (tensor-core pipeline mbarriers) that expired; `reset` clears it. */
+int hf_plan_status(hf_plan *plan, int *status, int reset);
+
 /* Debug/inspection: after hf_pipeline_exec, copy window `w`'s T x T Gram matrix (float64) and
  * its filter+DFT matrix W (complex64 [T][Nz]) to device buffers (either may be NULL). */
 int hf_pipeline_inspect(hf_plan *plan, int w, double *gram, void *wmat, hf_stream_t s);

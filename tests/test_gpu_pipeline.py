@@ -102,3 +102,25 @@ def test_pipeline_rejects_bad_desc(cuda):
     with pytest.raises(hf.HfError) as e:
         pl.Pipeline(pl.PipelineConfig(height=64, width=64, frames=32, hop=8, z_begin=10, z_end=5))
     assert e.value.code == hf.HF_ERR_INVALID
+
+
+@pytest.mark.parametrize("T,H,W", [(64, 256, 256), (128, 128, 128), (64, 1024, 1024)])
+def test_chosen_form_tensor_core_gram(cuda, T, H, W):
+    """The chosen form's tcgen05 Gram matrix equals the exact integer Gram of the 12-bit frames."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    frames = S.Interferograms(S.config1(T, height=H, width=W)).frames(0, T)
+    ring = torch.from_numpy(O.pack12(frames.reshape(-1))).to(cuda)
+    cfg = pl.PipelineConfig(height=H, width=W, frames=T, hop=16, z_begin=4, z_end=min(32, T // 2),
+                            fs=67e3, z=0.25, clutter_rank=4, form=hf.HF_FORM_CHOSEN)
+    p = pl.Pipeline(cfg)
+    p.run(ring, T, 0, 1)
+    gram, _ = p.inspect(0)
+    assert p.status() == 0
+    X = frames.reshape(T, -1).astype(np.float64)
+    exact = X @ X.T
+    g = gram.cpu().numpy()
+    # 12-bit samples: exact int8 split on the tensor core, so the Gram matrix is exact
+    assert np.array_equal(g, exact)
+    assert np.array_equal(g, g.T)
