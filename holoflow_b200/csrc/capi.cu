@@ -10,6 +10,7 @@
 #include "k_fft2d.cuh"
 #include "k_misc.cuh"
 #include "k_pca.cuh"
+#include "k_tc_band.cuh"
 
 namespace hf {
 
@@ -98,6 +99,7 @@ struct hf_plan {
   int       *status = nullptr; // device status word: nonzero when a bounded device wait expired
   void      *cov_ws = nullptr;
   bool       cov_tc = false;   // tensor-core Gram matrix (chosen form)
+  bool       rows_tc = false;  // tensor-core band DFT fused with lens + row FFT (chosen form)
   size_t     bytes = 0;
   // optional per-stage CUDA-event timing (hf_plan_timing / hf_plan_stage_times)
   static constexpr int kSets = 128, kMarks = HF_MAX_STAGES + 1;
@@ -260,6 +262,8 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       break;
     if ((rc = cuda_status(cudaMemsetAsync(p->status, 0, sizeof(int), stream), "status reset")))
       break;
+    p->rows_tc = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
+                 band_rows_tc_supported(d.input_dtype, d.frames, d.width, p->nz, p->frame_bytes);
     rc = plan_tables(p, stream);
   } while (0);
   if (rc != HF_OK) {
@@ -317,12 +321,16 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
                (int64_t)d.hop, p->frame_bytes};
   const int T = d.frames;
   int       mk = 0;
+  // the tensor-core passes read 16-byte runs of the ring: fall back to the plain kernels otherwise
+  const bool aligned16 = (reinterpret_cast<uintptr_t>(ring) & 15) == 0;
+  const bool cov_tc    = p->cov_tc && aligned16;
+  const bool rows_tc   = p->rows_tc && aligned16;
   mark(p, s, mk++, nullptr);
 
   // 1. SVD clutter filter: Gram -> FP64 Jacobi -> W = (I - V V^T) D_band
   BandArgs ba{};
   if (d.clutter_rank > 0) {
-    if (p->cov_tc)
+    if (cov_tc)
       HF_TRY(launch_covariance_tc(fr, d.input_dtype, T, p->P, nwin, p->cov_ws, p->gram, p->status, s));
     else
       HF_TRY(launch_covariance(fr, d.input_dtype, T, p->P, nwin, p->cov_ws, p->gram, s));
@@ -335,6 +343,44 @@ int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t 
   } else {
     ba.wmat        = p->wmat_plain;
     ba.wmat_stride = 0;
+  }
+  if (rows_tc) {
+    // chosen form: tensor-core band DFT + lens + row FFT in one pass, then columns + moments
+    BandRowsArgs br{};
+    br.ring        = fr;
+    br.T           = T;
+    br.H           = d.height;
+    br.W           = d.width;
+    br.nz          = p->nz;
+    br.wmat        = ba.wmat;
+    br.wmat_stride = ba.wmat_stride;
+    br.lens        = p->lens;
+    br.out         = p->band;
+    br.out_win     = (int64_t)p->nz * p->P;
+    br.out_plane   = p->P;
+    br.out_row     = d.width;
+    br.nwin        = nwin;
+    br.shift       = 2048.f;
+    br.status      = p->status;
+    HF_CUDA(cudaPeekAtLastError());
+    HF_TRY(launch_band_rows_tc(br, d.input_dtype, s));
+    mark(p, s, mk++, "band_dft_rows");
+    ColPass cp{};
+    cp.in        = p->band;
+    cp.in_win    = br.out_win;
+    cp.in_plane  = p->P;
+    cp.in_row    = d.width;
+    cp.H         = d.height;
+    cp.W         = d.width;
+    cp.nplanes   = p->nz;
+    cp.out       = out;
+    cp.out_win   = (int64_t)p->nmom * p->OH * p->OW;
+    cp.out_plane = (int64_t)p->OH * p->OW;
+    cp.out_row   = p->OW;
+    cp.out_col   = 1;
+    HF_TRY(launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s));
+    mark(p, s, mk++, "fft_cols_moments");
+    return finish_exec(p);
   }
   // 2. band DFT (+ lens for Fresnel) -> band planes [nwin][nz][H][W]
   ba.ring      = fr;

@@ -204,4 +204,26 @@ __device__ __forceinline__ void four_step_rev_b(float2 *x, int kb, const float2 
   dft_reg<N1, INV>(x);
 }
 
+// In-place variants of the forward four-step for a buffer of exactly N = 32*N1 complex values:
+// the exchange uses index k1*32 + (n2 ^ k1) (an XOR swizzle instead of padding), so the same
+// buffer that held the natural-order input can hold the exchange without bank conflicts.
+template <int N1, bool INV>
+__device__ __forceinline__ void four_step_a_sw(float2 *x, int n2, const SmemTwiddles &tw, float2 *xb) {
+  dft_reg<N1, INV>(x);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    float2 v = x[k1];
+    if (k1 != 0)
+      v = cmul(v, tw.get<INV>((n2 * k1) % (N1 * 32)));
+    xb[k1 * 32 + (n2 ^ k1)] = v;
+  }
+}
+template <int N1, bool INV>
+__device__ __forceinline__ void four_step_b_sw(float2 *y, int k1, const float2 *xb) {
+#pragma unroll
+  for (int n2 = 0; n2 < 32; ++n2)
+    y[n2] = xb[k1 * 32 + (n2 ^ k1)];
+  dft_reg<32, INV>(y);
+}
+
 } // namespace hf

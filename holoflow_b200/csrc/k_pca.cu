@@ -302,6 +302,19 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(const double *a_
       A[sym_idx(i, j, np)] = v;
     }
   }
+  // absolute rotation threshold: entries below 2^-52 of the trace (the matrix is a Gram matrix,
+  // so the trace bounds its norm) are at the rounding level of the largest eigenvalues and cannot
+  // be reduced further by two-sided rotations
+  __syncthreads(); // the cooperative load of A above must be complete
+  if (tid == 0) {
+    double tr = 0.0;
+    for (int i = 0; i < n; ++i)
+      tr += fabs(A[sym_idx(i, i, np)]);
+    cs[0] = tr * 2.220446049250313e-16;
+  }
+  __syncthreads();
+  const double tol_abs = cs[0];
+  __syncthreads();
   // this thread's fixed work items
   const int nblocks = half * (half + 1) / 2;
   int       bk[kJacobiMaxBlk], bl[kJacobiMaxBlk], nb = 0;
@@ -337,14 +350,13 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(const double *a_
         const double apq = A[sym_idx(p, q, np)];
         double       c = 1.0, s = 0.0;
         const bool   pad = (p >= n) || (q >= n);
-        if (!pad && apq != 0.0 && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
-          const double theta = (aqq - app) / (2.0 * apq);
-          double       t;
-          if (fabs(theta) > 1e150)
-            t = 0.5 / theta;
-          else
-            t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-          c = rsqrt(t * t + 1.0);
+        if (!pad && fabs(apq) > tol_abs && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
+          // t = tan(phi) of the annihilating rotation, the smaller root of t^2 + 2 theta t - 1 = 0
+          // with theta = d / (2 apq), d = aqq - app, written with one square root and one division
+          const double d  = aqq - app;
+          const double a2 = 2.0 * apq;
+          const double t  = (d >= 0.0 ? a2 : -a2) / (fabs(d) + sqrt(fma(d, d, a2 * a2)));
+          c = rsqrt(fma(t, t, 1.0));
           s = t * c;
           flag[0] = 1;
         }

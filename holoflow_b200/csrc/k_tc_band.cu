@@ -1,0 +1,322 @@
+// Chosen form, fused pass 1: temporal band DFT (with the SVD clutter filter folded into W) on the
+// tensor cores, lens multiply and the row FFT of every band plane, one image row at a time.
+//
+// Per image row r of window w (W pixels = W/128 M-tiles):
+//   S[p][k] = sum_t (x_t[p] - 2048) W16[t][k] + 2048 sum_t W16[t][k]     (W16 = f16(W))
+// is a [W x 64] x [64 x 2nz] product: A = the row's samples, f16, MN-major (pixels contiguous per
+// frame, as they arrive), B = W16 as real/imaginary columns, K-major; tcgen05.mma M = 128, N = 64,
+// K = 16, f32 accumulators in TMEM (tile j -> columns 64j .. 64j+63, all 512 columns for W = 1024).
+// The epilogue moves 8 bins at a time from TMEM into shared memory (adding the DC correction and
+// multiplying by the Fresnel lens), runs each bin's length-W row FFT in place (four-step, XOR-
+// swizzled exchange) and stores the row of that band plane.
+//
+// Warp roles (384 threads, one CTA per SM, persistent over rows):
+//   warps 0-3  : load + unpack the next row into the A operand, rebuild B, and (thread 0) issue the
+//                MMAs once the epilogue has released TMEM;
+//   warps 4-11 : epilogue (each warp owns the TMEM lane quarter warp % 4).
+// mbarriers: `full` (MMAs of a row complete: TMEM readable, A/B reusable) and `free` (the 8
+// epilogue warps finished reading TMEM).  Every wait is bounded; an expired wait sets the status
+// word and an abort flag that turns the remaining waits into no-ops, so the kernel always exits.
+#include <cuda_fp16.h>
+
+#include "fft_core.cuh"
+#include "k_tc_band.cuh"
+#include "tc_common.cuh"
+
+namespace hf {
+
+namespace {
+
+constexpr int kLoaders   = 128; // warps 0-3
+constexpr int kEpilogue  = 256; // warps 4-11
+constexpr int kBandTcThr = kLoaders + kEpilogue;
+constexpr int kTileBytes = 16384; // [K = 64][M = 128] f16 in two 64-pixel MN atoms of 8 K atoms
+
+__device__ __forceinline__ bool wait_or_abort(uint64_t *mbar, uint32_t parity, volatile int *abort, int *status,
+                                              int code) {
+  for (uint32_t i = 0; i < tc::kWaitLimit; ++i) {
+    if (tc::mbar_try_wait(mbar, parity))
+      return true;
+    if ((i & 1023u) == 1023u && *abort)
+      return false;
+  }
+  if (status)
+    atomicCAS(status, 0, code);
+  *abort = 1;
+  return false;
+}
+
+__device__ __forceinline__ void named_bar(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(mbar)) : "memory");
+}
+
+template <int FMT> struct GroupLoad; // 32 consecutive samples of one frame
+template <> struct GroupLoad<HF_MONO12P> {
+  static constexpr int kBytes = 48;
+  __device__ static void load(const uint8_t *src, uint32_t (&v)[32]) {
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+    const uint4  a = __ldg(s), b = __ldg(s + 1), c = __ldg(s + 2);
+    const uint32_t w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint32_t p[8];
+      unpack8(w[3 * q], w[3 * q + 1], w[3 * q + 2], p);
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        v[8 * q + i] = p[i];
+    }
+  }
+};
+template <> struct GroupLoad<HF_U16> {
+  static constexpr int kBytes = 64;
+  __device__ static void load(const uint8_t *src, uint32_t (&v)[32]) {
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint4    a    = __ldg(s + q);
+      const uint32_t w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        v[8 * q + 2 * i]     = w[i] & 0xFFFFu;
+        v[8 * q + 2 * i + 1] = w[i] >> 16;
+      }
+    }
+  }
+};
+
+template <int FMT, int N1>
+__global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArgs a) {
+  constexpr int W      = N1 * 32;
+  constexpr int NTILE  = W / 128;
+  constexpr int NCOL   = NTILE * 64 < 32 ? 32 : NTILE * 64;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t *sA   = smem;                                  // NTILE x 16 KB
+  uint8_t *sB   = sA + NTILE * kTileBytes;               // 64 rows x 128 B
+  float2  *gbuf = reinterpret_cast<float2 *>(sB + 8192); // 8 bins x W
+  float   *twc  = reinterpret_cast<float *>(gbuf + 8 * W);
+  float   *colsum = twc + 2 * W;                          // [2][64], indexed by row parity
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(colsum + 128); // [0] full, [1] free
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+  int      *abort_flag = reinterpret_cast<int *>(tslot + 1);
+  SmemTwiddles tw{twc, twc + W, W};
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[1], kEpilogue / 32);
+    *abort_flag = 0;
+    tc::mbar_fence_init();
+  }
+  tw.fill(tid, blockDim.x);
+  if (warp == 0)
+    tc::tmem_alloc(tslot, NCOL);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *tslot;
+  volatile int  *abortv = abort_flag;
+  constexpr uint32_t idesc = tc::idesc_f16(128, 64, true, false);
+  const int64_t nrows = (int64_t)a.nwin * a.H;
+
+  if (tid < kLoaders) {
+    // ------------------------------------------------------------------ loader / MMA warps
+    int k = 0;
+    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x, ++k) {
+      const int w = (int)(row / a.H), r = (int)(row % a.H);
+      if (k > 0) // MMAs of the previous row done: A and B may be overwritten
+        wait_or_abort(&mbar[0], (uint32_t)((k - 1) & 1), abortv, a.status, 11);
+      // B (K-major, 128-byte swizzle): row n = 2*bin + {re, im}, K = frame t
+      const float2 *wm = a.wmat + (int64_t)w * a.wmat_stride;
+      for (int e = tid; e < 64 * 8; e += kLoaders) {
+        const int n = e >> 3, c = e & 7; // one 16-byte chunk = 8 frames
+        __half hv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int t = 8 * c + i;
+          float     v = 0.f;
+          if ((n >> 1) < a.nz) {
+            const float2 z = __ldg(wm + (int64_t)t * a.nz + (n >> 1));
+            v              = (n & 1) ? z.y : z.x;
+          }
+          hv[i] = __float2half_rn(v);
+        }
+        *reinterpret_cast<uint4 *>(sB + n * 128 + ((c ^ (n & 7)) << 4)) = *reinterpret_cast<const uint4 *>(hv);
+      }
+      // A: tile j = pixels [128 j, 128 j + 128) of row r; element (m, t) at
+      //    (m/64)*8192 + (t/8)*1024 + (t%8)*128 + ((m%64/8) ^ (t%8))*16 + (m%8)*2.
+      //    Loads of two tiles are issued before any of them is unpacked.
+      for (int j0 = 0; j0 < NTILE; j0 += 2) {
+        uint32_t v[4][32];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = j0 + (u >> 1), item = tid + (u & 1) * kLoaders;
+          const int t = item >> 2, grp = item & 3;
+          const int64_t px0 = (int64_t)r * W + 128 * j + 32 * grp;
+          if (j < NTILE)
+            GroupLoad<FMT>::load(a.ring.frame(w, t) + px0 * GroupLoad<FMT>::kBytes / 32, v[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = j0 + (u >> 1), item = tid + (u & 1) * kLoaders;
+          const int t = item >> 2, grp = item & 3;
+          if (j >= NTILE)
+            continue;
+          uint8_t *tile = sA + j * kTileBytes;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int m0 = 32 * grp + 8 * q;
+            __half2 h[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              h[i] = __floats2half2_rn((float)v[u][8 * q + 2 * i] - a.shift, (float)v[u][8 * q + 2 * i + 1] - a.shift);
+            const int chunk = (m0 & 63) >> 3;
+            uint8_t  *dst   = tile + (m0 >> 6) * 8192 + (t >> 3) * 1024 + (t & 7) * 128 + ((chunk ^ (t & 7)) << 4);
+            *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(h);
+          }
+        }
+      }
+      named_bar(1, kLoaders); // B complete
+      if (tid < 64) {         // DC correction of the shifted samples: shift * sum_t W16[t][n]
+        float sacc = 0.f;
+        for (int t = 0; t < 64; ++t) {
+          const int    c  = t >> 3;
+          const __half hv = *reinterpret_cast<const __half *>(sB + tid * 128 + ((c ^ (tid & 7)) << 4) + (t & 7) * 2);
+          sacc += __half2float(hv);
+        }
+        colsum[(k & 1) * 64 + tid] = a.shift * sacc;
+      }
+      tc::fence_proxy_async_smem();
+      named_bar(1, kLoaders);
+      if (tid == 0) {
+        if (k > 0) // the epilogue has read the previous row out of TMEM
+          wait_or_abort(&mbar[1], (uint32_t)((k - 1) & 1), abortv, a.status, 12);
+        tc::fence_after_sync();
+        if (!*abortv) {
+#pragma unroll
+          for (int j = 0; j < NTILE; ++j)
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+              const uint64_t ad = tc::sw128_desc(tc::smem_u32(sA + j * kTileBytes + ks * 2048), 8192, 1024);
+              const uint64_t bd = tc::sw128_desc(tc::smem_u32(sB + ks * 32), 16, 1024);
+              tc::mma_f16(tbase + 64 * j, ad, bd, idesc, ks > 0 ? 1u : 0u);
+            }
+        }
+        tc::mma_commit(&mbar[0]);
+      }
+    }
+  } else {
+    // ------------------------------------------------------------------ epilogue warps
+    const int e = warp - 4;          // 0..7
+    const int q = warp & 3;          // TMEM lane quarter
+    const int h = e >> 2;            // which half of the tiles this warp gathers
+    constexpr int TPH = (NTILE + 1) / 2;
+    int k = 0;
+    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x, ++k) {
+      const int w = (int)(row / a.H), r = (int)(row % a.H);
+      wait_or_abort(&mbar[0], (uint32_t)(k & 1), abortv, a.status, 13);
+      tc::fence_after_sync();
+      float2 L[TPH];
+#pragma unroll
+      for (int jj = 0; jj < TPH; ++jj) {
+        const int j = h * TPH + jj;
+        const int p = 128 * j + 32 * q + lane;
+        L[jj] = (a.lens != nullptr && j < NTILE) ? __ldg(a.lens + (int64_t)r * W + p) : make_float2(1.f, 0.f);
+      }
+      const int ngrp = (a.nz + 7) / 8;
+      for (int gi = 0; gi < ngrp; ++gi) {
+#pragma unroll
+        for (int jj = 0; jj < TPH; ++jj) {
+          const int j = h * TPH + jj;
+          if (j < NTILE) {
+            uint32_t v[16];
+            const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + 64 * j + 16 * gi;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                           "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                         : "r"(ta));
+            tc::tmem_wait_ld();
+            const int p = 128 * j + 32 * q + lane;
+#pragma unroll
+            const float *cs = colsum + (k & 1) * 64 + 16 * gi;
+            for (int b = 0; b < 8; ++b) {
+              const float2 s = make_float2(__uint_as_float(v[2 * b]) + cs[2 * b],
+                                           __uint_as_float(v[2 * b + 1]) + cs[2 * b + 1]);
+              gbuf[b * W + p] = cmul(s, L[jj]);
+            }
+          }
+        }
+        if (gi == ngrp - 1) { // TMEM fully read for this row: release it to the MMA issuer
+          tc::fence_before_sync();
+          __syncwarp();
+          if (lane == 0)
+            mbar_arrive(&mbar[1]);
+        }
+        named_bar(2, kEpilogue);
+        const int bin = 8 * gi + e;
+        if (bin < a.nz) {
+          float2 *buf = gbuf + e * W;
+          float2  x[N1];
+#pragma unroll
+          for (int n1 = 0; n1 < N1; ++n1)
+            x[n1] = buf[lane + 32 * n1];
+          __syncwarp();
+          four_step_a_sw<N1, false>(x, lane, tw, buf);
+          __syncwarp();
+          float2 *orow = a.out + (int64_t)w * a.out_win + (int64_t)bin * a.out_plane + (int64_t)r * a.out_row;
+          for (int k1 = lane; k1 < N1; k1 += 32) {
+            float2 y[32];
+            four_step_b_sw<N1, false>(y, k1, buf);
+#pragma unroll
+            for (int k2 = 0; k2 < 32; ++k2)
+              orow[k1 + N1 * k2] = y[k2];
+          }
+        }
+        named_bar(2, kEpilogue);
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tbase, NCOL);
+  }
+}
+
+template <int FMT, int N1> int launch_n1(const BandRowsArgs &a, cudaStream_t s) {
+  constexpr int W     = N1 * 32;
+  constexpr int NTILE = W / 128;
+  const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 8192 + (size_t)8 * W * 8 + (size_t)2 * W * 4 + 128 * 4 +
+                      16 + 8;
+  HF_CUDA(cudaFuncSetAttribute(band_rows_tc_kernel<FMT, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t nrows = (int64_t)a.nwin * a.H;
+  const int     grid  = (int)std::min<int64_t>(nrows, sm_count());
+  band_rows_tc_kernel<FMT, N1><<<grid, kBandTcThr, smem, s>>>(a);
+  note_launch();
+  return launch_status("band_rows_tc_kernel");
+}
+
+} // namespace
+
+bool band_rows_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes) {
+  return (fmt == HF_MONO12P || fmt == HF_U16) && T == 64 && (W == 256 || W == 512 || W == 1024) && nz >= 1 &&
+         nz <= 32 && frame_bytes % 16 == 0;
+}
+
+int launch_band_rows_tc(const BandRowsArgs &a, int fmt, cudaStream_t s) {
+  HF_CHECK_ARG(band_rows_tc_supported(fmt, a.T, a.W, a.nz, a.ring.frame_bytes), "band rows (tensor core): unsupported shape");
+  HF_CHECK_ARG(((uintptr_t)a.ring.base & 15) == 0, "band rows (tensor core): ring must be 16-byte aligned");
+  switch (a.W) {
+  case 256: return fmt == HF_MONO12P ? launch_n1<HF_MONO12P, 8>(a, s) : launch_n1<HF_U16, 8>(a, s);
+  case 512: return fmt == HF_MONO12P ? launch_n1<HF_MONO12P, 16>(a, s) : launch_n1<HF_U16, 16>(a, s);
+  default: return fmt == HF_MONO12P ? launch_n1<HF_MONO12P, 32>(a, s) : launch_n1<HF_U16, 32>(a, s);
+  }
+}
+
+} // namespace hf

@@ -1,0 +1,26 @@
+// Launch interface of the tensor-core fused band DFT + lens + row FFT pass (k_tc_band.cu).
+#pragma once
+
+#include "frames.cuh"
+
+namespace hf {
+
+struct BandRowsArgs {
+  FrameRing     ring;        // window frames (packed 12-bit or uint16)
+  int           T;           // frames per window (64)
+  int           H, W;        // frame geometry (W in {256, 512, 1024})
+  int           nz;          // band bins (<= 32)
+  const float2 *wmat;        // [nwin][T][nz] filter+DFT matrices (float32)
+  int64_t       wmat_stride; // complex elements between windows (0 = shared)
+  const float2 *lens;        // [H][W] or nullptr
+  float2       *out;         // row-transformed band planes [nwin][nz][H][W]
+  int64_t       out_win, out_plane, out_row;
+  int           nwin;
+  float         shift;       // sample offset removed before the f16 conversion (2048)
+  int          *status;      // device status word (bounded waits)
+};
+
+bool band_rows_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes);
+int  launch_band_rows_tc(const BandRowsArgs &a, int fmt, cudaStream_t s);
+
+} // namespace hf

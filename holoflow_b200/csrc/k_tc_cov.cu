@@ -197,7 +197,6 @@ __global__ void __launch_bounds__(128) cov_tc_i8_kernel(FrameRing ring, int64_t 
   constexpr int STAGE = R * 128;         // 128 pixels (int8 K) per row
   constexpr int NMB   = R / 128;         // 128-row M-blocks
   constexpr int NCOL  = NMB * R;         // TMEM columns (int32)
-  constexpr int TPT   = T * 16 / 128;    // (frame, 8-pixel group) items per thread
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t *mbar  = reinterpret_cast<uint64_t *>(smem + kTcStages * STAGE);
@@ -217,54 +216,97 @@ __global__ void __launch_bounds__(128) cov_tc_i8_kernel(FrameRing ring, int64_t 
   const uint32_t tbase = *tslot;
   constexpr uint32_t idesc = tc::idesc_i8(128, R, false, false);
 
-  const int g = tid & 15;
-  uint32_t  isum[TPT];
+  // items: (frame t, 32-pixel group grp) with t = (tid >> 2) + 32 * k, grp = tid & 3; each item is
+  // one 16-byte-aligned run of packed bytes (48 B for 12-bit, 32 B for 8-bit samples)
+  constexpr int IPT = T * 4 / 128; // items per thread per stage
+  const int grp = tid & 3;
+  uint32_t  isum[IPT];
 #pragma unroll
-  for (int k = 0; k < TPT; ++k)
+  for (int k = 0; k < IPT; ++k)
     isum[k] = 0u;
   const int ishift = (int)shift;
+  constexpr int GW = FMT == HF_MONO12P ? 12 : 8; // words per item
+
+  auto load_items = [&](int64_t tile, uint32_t (&raw)[IPT][GW]) {
+    const int64_t p = tile * kTcPX + grp * 32;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      const int t = (tid >> 2) + 32 * k;
+      if (tile >= 0 && p < P) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(ring.frame(w, t) + p * TcBpp<FMT>::num / TcBpp<FMT>::den);
+#pragma unroll
+        for (int i = 0; i < GW / 4; ++i) {
+          const uint4 v = __ldg(src + i);
+          raw[k][4 * i] = v.x, raw[k][4 * i + 1] = v.y, raw[k][4 * i + 2] = v.z, raw[k][4 * i + 3] = v.w;
+        }
+      }
+    }
+  };
 
   const int64_t ntiles = (P + kTcPX - 1) / kTcPX;
   int           nj     = 0;
   bool          ok     = true;
+  uint32_t      nxt[IPT][GW];
+  load_items(blockIdx.x < ntiles ? (int64_t)blockIdx.x : -1, nxt);
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++nj) {
     const int s = nj % kTcStages;
-    bool      w_ok = true;
+    uint32_t  cur[IPT][GW];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k)
+#pragma unroll
+      for (int i = 0; i < GW; ++i)
+        cur[k][i] = nxt[k][i];
+    const bool valid = tile * kTcPX + grp * 32 < P;
+    if (tile + gridDim.x < ntiles) // prefetch the next tile's samples while this one is staged
+      load_items(tile + gridDim.x, nxt);
+    bool w_ok = true;
     if (nj >= kTcStages)
       w_ok = tc::mbar_wait_bounded(&mbar[s], (uint32_t)((nj / kTcStages) - 1) & 1u, status, 3);
     ok = __syncthreads_and(w_ok) != 0;
     if (!ok)
       break;
-    uint8_t      *st    = smem + s * STAGE;
-    const int64_t p     = tile * kTcPX + g * 8;
-    const bool    valid = p < P;
+    uint8_t *st = smem + s * STAGE;
 #pragma unroll
-    for (int k = 0; k < TPT; ++k) {
-      const int t = (tid >> 4) + 8 * k;
-      uint32_t  v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (valid) {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(ring.frame(w, t) +
-                                                                 p * TcBpp<FMT>::num / TcBpp<FMT>::den);
-        uint32_t wv[TcBpp<FMT>::words];
+    for (int k = 0; k < IPT; ++k) {
+      const int t = (tid >> 2) + 32 * k;
+      uint32_t  v[32];
 #pragma unroll
-        for (int i = 0; i < TcBpp<FMT>::words; ++i)
-          wv[i] = __ldg(src + i);
-        unpack_group<FMT>(wv, v);
+      for (int q = 0; q < 4; ++q) {
+        uint32_t p8[8];
+        if constexpr (FMT == HF_MONO12P) {
+          unpack8(cur[k][3 * q], cur[k][3 * q + 1], cur[k][3 * q + 2], p8);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              p8[4 * i + j] = (cur[k][2 * q + i] >> (8 * j)) & 0xFFu;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          v[8 * q + i] = valid ? p8[i] : 0u;
       }
-      uint32_t hw[2] = {0, 0}, lw[2] = {0, 0};
+      uint32_t hw[8], lw[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
+      for (int i = 0; i < 8; ++i)
+        hw[i] = lw[i] = 0u;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
         isum[k] += v[i];
-        const int d = valid ? (int)v[i] - ishift : 0;      // in [-2048, 2047]
-        const int h = d >> 6;                              // floor division: [-32, 31]
-        const int l = d & 63;                              // [0, 63]
-        hw[i >> 2] |= (uint32_t)(h & 0xFF) << (8 * (i & 3));
-        lw[i >> 2] |= (uint32_t)l << (8 * (i & 3));
+        const int d = valid ? (int)v[i] - ishift : 0; // in [-2048, 2047]
+        hw[i >> 2] |= (uint32_t)((d >> 6) & 0xFF) << (8 * (i & 3)); // floor(d / 64): [-32, 31]
+        lw[i >> 2] |= (uint32_t)(d & 63) << (8 * (i & 3));           // [0, 63]
       }
-      const int c = g >> 1, half = g & 1;
-      *reinterpret_cast<uint2 *>(st + t * 128 + ((c ^ (t & 7)) << 4) + half * 8) = make_uint2(hw[0], hw[1]);
+      // 32 pixels = two 16-byte chunks of a 128-byte row, chunk index 2*grp + {0, 1}
       const int tl = T + t;
-      *reinterpret_cast<uint2 *>(st + tl * 128 + ((c ^ (tl & 7)) << 4) + half * 8) = make_uint2(lw[0], lw[1]);
+#pragma unroll
+      for (int hc = 0; hc < 2; ++hc) {
+        const int c = 2 * grp + hc;
+        *reinterpret_cast<uint4 *>(st + t * 128 + ((c ^ (t & 7)) << 4)) =
+            make_uint4(hw[4 * hc], hw[4 * hc + 1], hw[4 * hc + 2], hw[4 * hc + 3]);
+        *reinterpret_cast<uint4 *>(st + tl * 128 + ((c ^ (tl & 7)) << 4)) =
+            make_uint4(lw[4 * hc], lw[4 * hc + 1], lw[4 * hc + 2], lw[4 * hc + 3]);
+      }
     }
     tc::fence_proxy_async_smem();
     __syncthreads();
@@ -289,8 +331,8 @@ __global__ void __launch_bounds__(128) cov_tc_i8_kernel(FrameRing ring, int64_t 
   ok = __syncthreads_and(ok) != 0;
   tc::fence_after_sync();
 #pragma unroll
-  for (int k = 0; k < TPT; ++k)
-    atomicAdd(&sums[(int64_t)w * T + (tid >> 4) + 8 * k], (unsigned long long)isum[k]);
+  for (int k = 0; k < IPT; ++k)
+    atomicAdd(&sums[(int64_t)w * T + (tid >> 2) + 32 * k], (unsigned long long)isum[k]);
   if (nj > 0 && ok) {
     unsigned long long *aw = acc + (int64_t)w * T * T;
 #pragma unroll
@@ -393,8 +435,9 @@ size_t cov_tc_workspace_bytes(int T, int64_t P, int nwin) {
 }
 
 bool cov_tc_supported(int fmt, int T, int64_t P, int64_t frame_bytes) {
-  return (fmt == HF_MONO12P || fmt == HF_U16 || fmt == HF_U8) && (T == 64 || T == 128) && P % 8 == 0 &&
-         frame_bytes % 4 == 0;
+  if (fmt == HF_MONO12P || fmt == HF_U8) // 16-byte loads of 32-pixel runs
+    return (T == 64 || T == 128) && P % 32 == 0 && frame_bytes % 16 == 0;
+  return fmt == HF_U16 && (T == 64 || T == 128) && P % 8 == 0 && frame_bytes % 4 == 0;
 }
 
 int launch_covariance_tc(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, void *ws,

@@ -124,3 +124,28 @@ def test_chosen_form_tensor_core_gram(cuda, T, H, W):
     # 12-bit samples: exact int8 split on the tensor core, so the Gram matrix is exact
     assert np.array_equal(g, exact)
     assert np.array_equal(g, g.T)
+
+
+@pytest.mark.parametrize("H,W,nwin", [(256, 256, 3), (512, 512, 2), (1024, 1024, 2)])
+def test_chosen_form_fresnel_vs_oracle(cuda, H, W, nwin):
+    """Chosen form (int8 tensor-core Gram, f16 tensor-core band DFT fused with lens + row FFT):
+    M0/M1/M2 within the 1e-3 relative-L2 target of the float64 oracle, and the device status word
+    stays clear."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    z0, z1 = O.band_bins(4e3, 33e3, 67e3, 64)
+    n = 64 + 16 * (nwin - 1)
+    frames = S.Interferograms(S.config1(n, height=H, width=W)).frames(0, n)
+    ring = torch.from_numpy(O.pack12(frames.reshape(-1))).to(cuda)
+    cfg = pl.PipelineConfig(height=H, width=W, frames=64, hop=16, z_begin=z0, z_end=z1, fs=67e3, z=0.25,
+                            clutter_rank=4, form=hf.HF_FORM_CHOSEN, max_batch=nwin)
+    p = pl.Pipeline(cfg)
+    got = p.run(ring, n, 0, nwin).cpu().numpy()
+    assert p.status() == 0
+    ocfg = O.PathConfig(H, W, 64, 16, z0, z1, fs=67e3, z=0.25, clutter_rank=4)
+    for w in range(nwin):
+        exp = O.reconstruct_window(frames[16 * w:16 * w + 64], ocfg)
+        for m in range(3):
+            err = O.rel_l2(got[w, m], exp[m])
+            assert err < 1e-3, (w, m, err)
