@@ -209,9 +209,20 @@ def main():
     out = torch.empty((B, *pipe.out_shape), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream()
 
+    # device-resident input: every frame of the warm-up and timed steps is in the camera stream's
+    # ring before timing starts (the stream overlaps the next batch's eigen phase with this one)
+    nsteps = args.warmup + args.steps
+    total_frames = (T - HOP) + nsteps * B * HOP
+    cam_dev = pl.CameraStream(pipe, total_frames)
+    reps = (total_frames + 63) // 64
+    src = torch.cat([packed] * reps)[:total_frames].contiguous()
+    cam_dev.push(src, total_frames)
+    del src
+    torch.cuda.synchronize()
+
     def step(s):
-        first = (s * B * HOP) % RING_FRAMES
-        pipe.run(ring, RING_FRAMES, first, B, out)
+        n = cam_dev.process(B, out)
+        assert n == B
 
     for s in range(args.warmup):
         step(s)
@@ -231,8 +242,9 @@ def main():
         torch.cuda.synchronize()
     launches = lib.hf_launch_count()
     ms = e0.elapsed_time(e1)
-    stages = pipe.stage_times()
+    stages = {k: v for k, v in pipe.stage_times().items() if v[0] > 0}
     pipe.timing(False)
+    cam_dev.close()
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -245,7 +257,7 @@ def main():
     dom = max(stages, key=lambda k: stages[k][0]) if stages else None
     roof = None
     if dom:
-        per_launch_ms = stages[dom][0] / max(stages[dom][1], 1)
+        per_launch_ms = stages[dom][0] / max(args.steps, 1)
         bytes_launch = algo.get(dom, 0.0) * B
         achieved = bytes_launch / (per_launch_ms / 1000.0) / 1e9
         tr = traffic_table().get(dom)
@@ -253,7 +265,8 @@ def main():
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": (tr * B) if tr else None,
                 "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": round(per_launch_ms, 4),
-                "stages_ms_per_step": {k: round(v[0] / max(v[1], 1), 4) for k, v in stages.items()}}
+                "stages_ms_per_step": {k: round(v[0] / max(args.steps, 1), 4) for k, v in stages.items()},
+                "stage_note": "eigen_filter of the next batch runs on a side stream, overlapped"}
 
     # end to end through the camera-stream API: pinned host frames in, host moments out
     e2e = None

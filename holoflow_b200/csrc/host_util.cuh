@@ -1,0 +1,55 @@
+// Host-side helpers shared by the C ABI translation units: device allocation bookkeeping and
+// parameter conversions.
+#pragma once
+
+#include <cmath>
+#include <string>
+
+#include "k_fft2d.cuh"
+
+namespace hf {
+
+template <typename T> inline int dev_alloc(T **p, size_t count, size_t &total) {
+  *p = nullptr;
+  if (count == 0)
+    return HF_OK;
+  const size_t bytes = count * sizeof(T);
+  cudaError_t  e     = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    (void)cudaGetLastError();
+    return fail(HF_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  total += bytes;
+  return HF_OK;
+}
+
+template <typename T> inline void dev_free(T *&p) {
+  if (p)
+    cudaFree(p);
+  p = nullptr;
+}
+
+inline float norm_scale(int norm, int n) {
+  if (norm == HF_NORM_FORWARD)
+    return (float)(1.0 / (double)n);
+  if (norm == HF_NORM_ORTHO)
+    return (float)(1.0 / std::sqrt((double)n));
+  return 1.0f;
+}
+
+inline bool real_fmt(int f) { return f == HF_U8 || f == HF_U16 || f == HF_F32 || f == HF_MONO12P; }
+
+// f_k = start + k*df evaluated in double and cast (arange.cu:62-75); f_k^2 in float32
+// (graph_builder.cc:624-627).
+inline void fill_weights(MomentSpec &m, int T, int z0, int nz, double fs) {
+  const double df = fs / (double)T;
+  const double f0 = z0 * df;
+  for (int k = 0; k < kMaxBands; ++k) {
+    const float f = k < nz ? (float)(f0 + df * (double)k) : 0.f;
+    m.w1[k]       = f;
+    m.w2[k]       = f * f;
+  }
+}
+
+} // namespace hf

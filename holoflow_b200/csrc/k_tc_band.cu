@@ -296,7 +296,8 @@ template <int FMT, int N1> int launch_n1(const BandRowsArgs &a, cudaStream_t s) 
                       16 + 8;
   HF_CUDA(cudaFuncSetAttribute(band_rows_tc_kernel<FMT, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t nrows = (int64_t)a.nwin * a.H;
-  const int     grid  = (int)std::min<int64_t>(nrows, sm_count());
+  const int     cap   = a.max_ctas > 0 ? std::min(a.max_ctas, sm_count()) : sm_count();
+  const int     grid  = (int)std::min<int64_t>(nrows, cap);
   band_rows_tc_kernel<FMT, N1><<<grid, kBandTcThr, smem, s>>>(a);
   note_launch();
   return launch_status("band_rows_tc_kernel");

@@ -18,6 +18,7 @@ struct BandRowsArgs {
   int           nwin;
   float         shift;       // sample offset removed before the f16 conversion (2048)
   int          *status;      // device status word (bounded waits)
+  int           max_ctas;    // persistent grid size cap (SMs left to concurrent work otherwise)
 };
 
 bool band_rows_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes);

@@ -1,0 +1,646 @@
+// The fused per-window reconstruction (hf_plan / hf_pipeline_exec) and camera streams
+// (hf_stream_*): the composition of the stage kernels that replaces the reference graph
+// GraphBuilder wires for one window (graph_builder.cc:245-305 time-frequency analysis, 522-566
+// propagation, 604-631 moments), plus the device-resident frame ring that replaces BatchQueue
+// (batch_queue.cc:92-174).
+//
+// A window goes through three phases:
+//   covariance  Gram matrix of the window's frames               (bandwidth-bound, whole GPU)
+//   eigen       FP64 Jacobi + filter/DFT matrix W                (latency-bound, one CTA/window)
+//   propagate   band DFT (+ lens) -> row FFT -> column FFT + |.| + moments
+// hf_pipeline_exec runs them in order on the caller's stream.  A camera stream with frames of
+// the next batch already in its ring overlaps the next batch's eigen phase (on a side stream)
+// with the current batch's propagation; the per-window W matrices are the stream's device state.
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "host_util.cuh"
+#include "k_band.cuh"
+#include "k_fft2d.cuh"
+#include "k_misc.cuh"
+#include "k_pca.cuh"
+#include "k_tc_band.cuh"
+
+using namespace hf;
+
+namespace {
+
+// ---- per-stage CUDA-event timing ------------------------------------------------------------
+enum Stage {
+  ST_COV = 0,
+  ST_EIGEN,
+  ST_BAND,
+  ST_ROWS,
+  ST_BAND_ROWS,
+  ST_COLS_MOM,
+  ST_COLS_TF,
+  ST_ROWS_MOM,
+  ST_COUNT
+};
+const char *kStageName[ST_COUNT] = {"covariance", "eigen_filter", "band_dft", "fft_rows",
+                                    "band_dft_rows", "fft_cols_moments", "fft_cols_tf", "fft_rows_moments"};
+static_assert(ST_COUNT <= HF_MAX_STAGES, "stage table");
+
+struct StageTimer {
+  static constexpr int kRec = 2048;
+  bool        on = false;
+  int         n = 0, nexec = 0;
+  cudaEvent_t b[kRec] = {}, e[kRec] = {};
+  int         stage[kRec] = {};
+  int begin(cudaStream_t s, int st) {
+    if (!on || n >= kRec)
+      return -1;
+    cudaEventRecord(b[n], s);
+    stage[n] = st;
+    return n++;
+  }
+  void end(cudaStream_t s, int rec) {
+    if (rec >= 0)
+      cudaEventRecord(e[rec], s);
+  }
+  void destroy() {
+    for (int i = 0; i < kRec; ++i) {
+      if (b[i])
+        cudaEventDestroy(b[i]);
+      if (e[i])
+        cudaEventDestroy(e[i]);
+      b[i] = e[i] = nullptr;
+    }
+  }
+};
+
+// Buffers of one batch's filter state (Gram -> eigenvectors -> W).
+struct FilterSet {
+  double *gram = nullptr, *evecs = nullptr, *evals = nullptr;
+  int    *info = nullptr;
+  float2 *wmat = nullptr;
+};
+
+} // namespace
+
+struct hf_plan {
+  hf_desc    d{};
+  int        P = 0, nz = 0, nmom = 0, OH = 0, OW = 0;
+  bool       fast = false;
+  int64_t    frame_bytes = 0;
+  MomentSpec mom{};
+  float2    *lens = nullptr, *tf = nullptr, *band = nullptr, *band2 = nullptr;
+  float2    *wmat_plain = nullptr;
+  FilterSet  set[2];          // [0] for hf_pipeline_exec and stream batches, [1] stream lookahead
+  int       *status = nullptr; // device status word: nonzero when a bounded device wait expired
+  void      *cov_ws = nullptr;
+  bool       cov_tc = false;   // tensor-core Gram matrix (chosen form)
+  bool       rows_tc = false;  // tensor-core band DFT fused with lens + row FFT (chosen form)
+  size_t     bytes = 0;
+  StageTimer timer;
+};
+
+static void plan_free(hf_plan *p) {
+  dev_free(p->lens);
+  dev_free(p->tf);
+  dev_free(p->band);
+  dev_free(p->band2);
+  dev_free(p->wmat_plain);
+  for (auto &fs : p->set) {
+    dev_free(fs.gram);
+    dev_free(fs.evecs);
+    dev_free(fs.evals);
+    dev_free(fs.info);
+    dev_free(fs.wmat);
+  }
+  dev_free(p->status);
+  if (p->cov_ws)
+    cudaFree(p->cov_ws);
+  p->cov_ws = nullptr;
+  p->timer.destroy();
+}
+
+static int plan_tables(hf_plan *p, cudaStream_t s) {
+  const hf_desc &d = p->d;
+  if (d.propagation == HF_PROP_FRESNEL)
+    HF_TRY(launch_fresnel_lens(p->lens, d.width, d.height, d.lambda, d.z, d.pitch, s));
+  if (d.propagation == HF_PROP_ANGULAR_SPECTRUM) {
+    AsFilter f{d.r_inner, d.r_outer, d.s_inner, d.s_outer};
+    HF_TRY(launch_as_tf(p->tf, p->OW, p->OH, d.lambda, d.z, d.pitch, d.as_filter, f, s));
+  }
+  return HF_OK;
+}
+
+static FrameRing ring_of(const hf_plan *p, const void *ring, int64_t ring_frames, int64_t first) {
+  return FrameRing{reinterpret_cast<const uint8_t *>(ring), ring_frames, first % ring_frames, (int64_t)p->d.hop,
+                   p->frame_bytes};
+}
+
+// ---- phases ----------------------------------------------------------------------------------
+static int phase_cov(hf_plan *p, const FrameRing &fr, int nwin, double *gram, cudaStream_t s) {
+  const hf_desc &d  = p->d;
+  const bool     tc = p->cov_tc && (reinterpret_cast<uintptr_t>(fr.base) & 15) == 0;
+  const int      rec = p->timer.begin(s, ST_COV);
+  if (tc)
+    HF_TRY(launch_covariance_tc(fr, d.input_dtype, d.frames, p->P, nwin, p->cov_ws, gram, p->status, s));
+  else
+    HF_TRY(launch_covariance(fr, d.input_dtype, d.frames, p->P, nwin, p->cov_ws, gram, s));
+  p->timer.end(s, rec);
+  return HF_OK;
+}
+
+static int phase_eigen(hf_plan *p, const FilterSet &fs, int nwin, cudaStream_t s) {
+  const hf_desc &d   = p->d;
+  const int      rec = p->timer.begin(s, ST_EIGEN);
+  HF_TRY(launch_jacobi(fs.gram, fs.evecs, fs.evals, fs.info, d.frames, nwin, s));
+  HF_TRY(launch_band_matrix(fs.evecs, nwin, d.frames, d.clutter_rank, d.z_begin, d.z_end, fs.wmat, s));
+  p->timer.end(s, rec);
+  return HF_OK;
+}
+
+// Band DFT with W (per window, or shared when wstride == 0), propagation and moments.
+// `reserve_sms` SMs are left to concurrently running work by the persistent tensor-core pass.
+static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const float2 *wmat, int64_t wstride,
+                           float *out, cudaStream_t s, int reserve_sms) {
+  const hf_desc &d      = p->d;
+  const int64_t  win_px = (int64_t)p->nz * p->P;
+  const int64_t  oplane = (int64_t)p->OH * p->OW;
+  const int64_t  owin   = (int64_t)p->nmom * oplane;
+  const bool     rows_tc = p->rows_tc && (reinterpret_cast<uintptr_t>(fr.base) & 15) == 0;
+
+  if (rows_tc) { // chosen form: tensor-core band DFT + lens + row FFT, then columns + moments
+    BandRowsArgs br{};
+    br.ring = fr, br.T = d.frames, br.H = d.height, br.W = d.width, br.nz = p->nz;
+    br.wmat = wmat, br.wmat_stride = wstride, br.lens = p->lens, br.out = p->band;
+    br.out_win = win_px, br.out_plane = p->P, br.out_row = d.width, br.nwin = nwin, br.shift = 2048.f;
+    br.status = p->status, br.max_ctas = std::max(1, sm_count() - reserve_sms);
+    int rec = p->timer.begin(s, ST_BAND_ROWS);
+    HF_TRY(launch_band_rows_tc(br, d.input_dtype, s));
+    p->timer.end(s, rec);
+    ColPass cp{};
+    cp.in = p->band, cp.in_win = win_px, cp.in_plane = p->P, cp.in_row = d.width;
+    cp.H = d.height, cp.W = d.width, cp.nplanes = p->nz;
+    cp.out = out, cp.out_win = owin, cp.out_plane = oplane, cp.out_row = p->OW, cp.out_col = 1;
+    rec = p->timer.begin(s, ST_COLS_MOM);
+    HF_TRY(launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s));
+    p->timer.end(s, rec);
+    return HF_OK;
+  }
+
+  BandArgs ba{};
+  ba.ring = fr, ba.T = d.frames, ba.P = p->P, ba.H = d.height, ba.W = d.width, ba.nz = p->nz;
+  ba.wmat = wmat, ba.wmat_stride = wstride, ba.z0 = d.z_begin;
+  ba.lens = d.propagation == HF_PROP_FRESNEL ? p->lens : nullptr;
+  ba.out = p->band, ba.OH = d.height, ba.OW = d.width, ba.oy = 0, ba.ox = 0;
+  ba.out_plane = p->P, ba.out_win = win_px, ba.scale = 1.0f;
+  int rec = p->timer.begin(s, ST_BAND);
+  HF_TRY(launch_band_dft(ba, d.input_dtype, nwin, s));
+  p->timer.end(s, rec);
+
+  if (d.propagation == HF_PROP_NONE) {
+    MomentWeights mw;
+    memcpy(mw.w1, p->mom.w1, sizeof(mw.w1));
+    memcpy(mw.w2, p->mom.w2, sizeof(mw.w2));
+    rec = p->timer.begin(s, ST_COLS_MOM);
+    for (int w = 0; w < nwin; ++w)
+      HF_TRY(launch_band_moments(p->band + w * win_px, HF_CF32, p->nz, p->P, mw, d.moment_mask, out + w * owin, s));
+    p->timer.end(s, rec);
+    return HF_OK;
+  }
+
+  if (d.propagation == HF_PROP_FRESNEL) {
+    RowPass rp{};
+    rp.in = p->band, rp.in_real = 0, rp.in_win = win_px, rp.in_plane = p->P, rp.in_row = d.width, rp.in_col = 1;
+    rp.IH = d.height, rp.IW = d.width, rp.H = d.height, rp.N = d.width, rp.nplanes = p->nz, rp.inverse = 0;
+    rp.out = p->fast ? p->band : p->band2, rp.out_win = win_px, rp.out_plane = p->P, rp.out_row = d.width;
+    rec = p->timer.begin(s, ST_ROWS);
+    HF_TRY(launch_row_pass(rp, nwin, s));
+    p->timer.end(s, rec);
+    ColPass cp{};
+    cp.in = rp.out, cp.in_win = win_px, cp.in_plane = p->P, cp.in_row = d.width;
+    cp.H = d.height, cp.W = d.width, cp.nplanes = p->nz, cp.inverse = 0;
+    rec = p->timer.begin(s, ST_COLS_MOM);
+    if (p->fast) {
+      cp.out = out, cp.out_win = owin, cp.out_plane = oplane, cp.out_row = p->OW, cp.out_col = 1;
+      HF_TRY(launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s));
+    } else { // general sizes: complex column DFT back into `band`, then the moment reduction
+      HF_CHECK_ARG(!d.fftshift, "fftshift needs four-step frame sizes");
+      cp.out = p->band, cp.out_win = win_px, cp.out_plane = p->P, cp.out_row = d.width, cp.out_col = 1;
+      HF_TRY(launch_col_pass(cp, COL_COMPLEX, nullptr, nwin, s));
+      MomentWeights mw;
+      memcpy(mw.w1, p->mom.w1, sizeof(mw.w1));
+      memcpy(mw.w2, p->mom.w2, sizeof(mw.w2));
+      for (int w = 0; w < nwin; ++w)
+        HF_TRY(launch_band_moments(p->band + w * win_px, HF_CF32, p->nz, p->P, mw, d.moment_mask, out + w * owin, s));
+    }
+    p->timer.end(s, rec);
+    return HF_OK;
+  }
+
+  // angular spectrum: rows forward (with placement) -> columns fwd x TF inv -> rows inverse + moments
+  RowPass rp{};
+  rp.in = p->band, rp.in_real = 0, rp.in_win = win_px, rp.in_plane = p->P, rp.in_row = d.width, rp.in_col = 1;
+  rp.IH = d.height, rp.IW = d.width, rp.oy = (p->OH - d.height) / 2, rp.ox = (p->OW - d.width) / 2;
+  rp.H = p->OH, rp.N = p->OW, rp.nplanes = p->nz, rp.inverse = 0;
+  rp.out = p->band2, rp.out_win = (int64_t)p->nz * oplane, rp.out_plane = oplane, rp.out_row = p->OW;
+  rec = p->timer.begin(s, ST_ROWS);
+  HF_TRY(launch_row_pass(rp, nwin, s));
+  p->timer.end(s, rec);
+  ColPass cp{};
+  cp.in = p->band2, cp.in_win = rp.out_win, cp.in_plane = oplane, cp.in_row = p->OW;
+  cp.H = p->OH, cp.W = p->OW, cp.nplanes = p->nz;
+  cp.out = p->band2, cp.out_win = rp.out_win, cp.out_plane = oplane, cp.out_row = p->OW, cp.out_col = 1;
+  cp.tf = p->tf, cp.inverse = 0;
+  rec = p->timer.begin(s, ST_COLS_TF);
+  HF_TRY(launch_col_pass(cp, COL_TF_SANDWICH, nullptr, nwin, s));
+  p->timer.end(s, rec);
+  ColPass rm = cp;
+  rm.out = out, rm.out_win = owin, rm.out_plane = oplane, rm.out_row = p->OW, rm.inverse = 1;
+  rec = p->timer.begin(s, ST_ROWS_MOM);
+  HF_TRY(launch_row_moments(rm, p->mom, nwin, s));
+  p->timer.end(s, rec);
+  return HF_OK;
+}
+
+extern "C" {
+
+int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
+  clear_error();
+  HF_CHECK_ARG(desc != nullptr && out != nullptr, "hf_plan_create: null argument");
+  *out = nullptr;
+  const hf_desc &d = *desc;
+  HF_CHECK_ARG(d.height > 0 && d.width > 0, "plan: frame size must be positive");
+  HF_CHECK_ARG(d.frames >= 2 && d.frames <= 128, "plan: frames per window must be in [2, 128]");
+  HF_CHECK_ARG(d.hop >= 1, "plan: hop must be >= 1");
+  HF_CHECK_ARG(d.z_begin >= 0 && d.z_end > d.z_begin && d.z_end <= d.frames,
+               "plan: band must satisfy 0 <= z_begin < z_end <= frames");
+  HF_CHECK_ARG(d.z_end - d.z_begin <= kMaxBands, "plan: at most 64 band bins");
+  HF_CHECK_ARG(d.input_dtype == HF_MONO12P || d.input_dtype == HF_U16 || d.input_dtype == HF_U8 ||
+                   d.input_dtype == HF_F32,
+               "plan: input dtype must be MONO12P, U16, U8 or F32");
+  HF_CHECK_ARG(d.input_dtype != HF_MONO12P || ((int64_t)d.height * d.width) % 2 == 0,
+               "plan: 12-bit packed frames need an even pixel count");
+  HF_CHECK_ARG(d.propagation >= HF_PROP_NONE && d.propagation <= HF_PROP_ANGULAR_SPECTRUM,
+               "plan: unknown propagation");
+  HF_CHECK_ARG(d.clutter_rank >= 0 && d.clutter_rank < d.frames, "plan: clutter rank must be < frames");
+  HF_CHECK_ARG((d.moment_mask & 7) != 0 && (d.moment_mask & ~7) == 0, "plan: bad moment mask");
+  HF_CHECK_ARG(d.max_batch >= 1, "plan: max_batch must be >= 1");
+  HF_CHECK_ARG(d.form == HF_FORM_PLAIN || d.form == HF_FORM_CHOSEN, "plan: unknown form");
+  if (d.propagation != HF_PROP_NONE)
+    HF_CHECK_ARG(d.lambda > 0.f && d.pitch > 0.f, "plan: wavelength and pitch must be positive");
+  const bool padded = d.propagation == HF_PROP_ANGULAR_SPECTRUM && (d.pad_w > 0 || d.pad_h > 0);
+  if (padded)
+    HF_CHECK_ARG(d.pad_w >= d.width && d.pad_h >= d.height && (d.pad_w - d.width) % 2 == 0 &&
+                     (d.pad_h - d.height) % 2 == 0,
+                 "plan: padding must be >= the frame and leave even margins");
+  const int OH = padded ? d.pad_h : d.height, OW = padded ? d.pad_w : d.width;
+  if (d.propagation == HF_PROP_ANGULAR_SPECTRUM && !(fft_fast_length(OH) && fft_fast_length(OW) && OH <= 1024))
+    return fail(HF_ERR_UNSUPPORTED, "plan: angular spectrum pipeline needs padded sizes in {64..1536} (rows <= 1024)");
+
+  hf_plan *p = new (std::nothrow) hf_plan();
+  if (!p)
+    return fail(HF_ERR_NOMEM, "plan: host allocation failed");
+  p->d           = d;
+  p->P           = d.height * d.width;
+  p->nz          = d.z_end - d.z_begin;
+  p->nmom        = __builtin_popcount(d.moment_mask);
+  p->OH          = OH;
+  p->OW          = OW;
+  p->frame_bytes = frame_bytes_of(d.input_dtype, p->P);
+  p->fast        = fft_fast_length(OH) && fft_fast_length(OW);
+  p->mom.nz       = p->nz;
+  p->mom.mask     = d.moment_mask;
+  p->mom.fftshift = d.fftshift;
+  p->mom.inv_nz   = 1.0f / (float)p->nz;
+  fill_weights(p->mom, d.frames, d.z_begin, p->nz, d.fs > 0.f ? d.fs : 37e3);
+
+  const int64_t B  = d.max_batch;
+  const int     T  = d.frames;
+  int           rc = HF_OK;
+  do {
+    const int64_t plane = (int64_t)p->P, oplane = (int64_t)OH * OW;
+    if ((rc = dev_alloc(&p->band, (size_t)(B * p->nz * plane), p->bytes)))
+      break;
+    const bool need_band2 = d.propagation == HF_PROP_ANGULAR_SPECTRUM || (d.propagation == HF_PROP_FRESNEL && !p->fast);
+    if (need_band2 && (rc = dev_alloc(&p->band2, (size_t)(B * p->nz * oplane), p->bytes)))
+      break;
+    if (d.propagation == HF_PROP_FRESNEL && (rc = dev_alloc(&p->lens, (size_t)plane, p->bytes)))
+      break;
+    if (d.propagation == HF_PROP_ANGULAR_SPECTRUM && (rc = dev_alloc(&p->tf, (size_t)oplane, p->bytes)))
+      break;
+    if (d.clutter_rank > 0) {
+      for (auto &fs : p->set)
+        if ((rc = dev_alloc(&fs.gram, (size_t)(B * T * T), p->bytes)) ||
+            (rc = dev_alloc(&fs.evecs, (size_t)(B * T * T), p->bytes)) ||
+            (rc = dev_alloc(&fs.evals, (size_t)(B * T), p->bytes)) || (rc = dev_alloc(&fs.info, (size_t)B, p->bytes)) ||
+            (rc = dev_alloc(&fs.wmat, (size_t)(B * T * p->nz), p->bytes)))
+          break;
+      if (rc)
+        break;
+      p->cov_tc = d.form == HF_FORM_CHOSEN && cov_tc_supported(d.input_dtype, T, p->P, p->frame_bytes);
+      size_t wsb = cov_workspace_bytes(T, p->P, (int)B) + cov_workspace_bytes(T, p->P, 1);
+      if (p->cov_tc)
+        wsb = std::max(wsb, cov_tc_workspace_bytes(T, p->P, (int)B) + cov_tc_workspace_bytes(T, p->P, 1));
+      uint8_t *ws = nullptr;
+      if ((rc = dev_alloc(&ws, wsb, p->bytes)))
+        break;
+      p->cov_ws = ws;
+    } else {
+      if ((rc = dev_alloc(&p->wmat_plain, (size_t)T * p->nz, p->bytes)))
+        break;
+      if ((rc = launch_band_matrix(nullptr, 1, T, 0, d.z_begin, d.z_end, p->wmat_plain, stream)))
+        break;
+    }
+    if ((rc = dev_alloc(&p->status, 1, p->bytes)))
+      break;
+    if ((rc = cuda_status(cudaMemsetAsync(p->status, 0, sizeof(int), stream), "status reset")))
+      break;
+    p->rows_tc = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
+                 band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
+    rc = plan_tables(p, stream);
+  } while (0);
+  if (rc != HF_OK) {
+    plan_free(p);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return HF_OK;
+}
+
+int hf_plan_destroy(hf_plan *p) {
+  if (!p)
+    return HF_OK;
+  cudaDeviceSynchronize();
+  plan_free(p);
+  delete p;
+  return HF_OK;
+}
+
+int hf_plan_set_z(hf_plan *p, float z, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr, "hf_plan_set_z: null plan");
+  p->d.z = z;
+  return plan_tables(p, s);
+}
+
+int hf_plan_output_shape(const hf_plan *p, int32_t *oh, int32_t *ow, int32_t *nm) {
+  HF_CHECK_ARG(p != nullptr, "hf_plan_output_shape: null plan");
+  if (oh)
+    *oh = p->OH;
+  if (ow)
+    *ow = p->OW;
+  if (nm)
+    *nm = p->nmom;
+  return HF_OK;
+}
+
+int hf_plan_device_bytes(const hf_plan *p, size_t *bytes) {
+  HF_CHECK_ARG(p != nullptr && bytes != nullptr, "hf_plan_device_bytes: null argument");
+  *bytes = p->bytes;
+  return HF_OK;
+}
+
+int hf_pipeline_exec(hf_plan *p, const void *ring, int64_t ring_frames, int64_t first_frame, int nwin, float *out,
+                     hf_stream_t stream) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr && ring != nullptr && out != nullptr, "hf_pipeline_exec: null argument");
+  HF_CHECK_ARG(nwin >= 1 && nwin <= p->d.max_batch, "hf_pipeline_exec: nwin must be in [1, max_batch]");
+  HF_CHECK_ARG(ring_frames >= p->d.frames && first_frame >= 0, "hf_pipeline_exec: the ring must hold at least one window");
+  const FrameRing fr = ring_of(p, ring, ring_frames, first_frame);
+  if (p->d.clutter_rank > 0) {
+    HF_TRY(phase_cov(p, fr, nwin, p->set[0].gram, stream));
+    HF_TRY(phase_eigen(p, p->set[0], nwin, stream));
+    HF_TRY(phase_propagate(p, fr, nwin, p->set[0].wmat, (int64_t)p->d.frames * p->nz, out, stream, 0));
+  } else {
+    HF_TRY(phase_propagate(p, fr, nwin, p->wmat_plain, 0, out, stream, 0));
+  }
+  if (p->timer.on)
+    ++p->timer.nexec;
+  return HF_OK;
+}
+
+int hf_plan_timing(hf_plan *p, int enable) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr, "hf_plan_timing: null plan");
+  if (enable)
+    for (int i = 0; i < StageTimer::kRec; ++i) {
+      if (!p->timer.b[i])
+        HF_CUDA(cudaEventCreate(&p->timer.b[i]));
+      if (!p->timer.e[i])
+        HF_CUDA(cudaEventCreate(&p->timer.e[i]));
+    }
+  p->timer.on    = enable != 0;
+  p->timer.n     = 0;
+  p->timer.nexec = 0;
+  return HF_OK;
+}
+
+int hf_plan_stage_times(hf_plan *p, float *ms, const char **names, int *nstages, int *nexec) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr && ms != nullptr && nstages != nullptr, "hf_plan_stage_times: null argument");
+  for (int k = 0; k < HF_MAX_STAGES; ++k)
+    ms[k] = 0.f;
+  for (int i = 0; i < p->timer.n; ++i) {
+    float       t = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&t, p->timer.b[i], p->timer.e[i]);
+    if (e == cudaErrorNotReady)
+      return fail(HF_ERR_STATE, "hf_plan_stage_times: synchronise the stream first");
+    HF_CUDA(e);
+    ms[p->timer.stage[i]] += t;
+  }
+  if (names)
+    for (int k = 0; k < ST_COUNT; ++k)
+      names[k] = kStageName[k];
+  *nstages = ST_COUNT;
+  if (nexec)
+    *nexec = p->timer.nexec;
+  return HF_OK;
+}
+
+int hf_plan_status(hf_plan *p, int *status, int reset) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr && status != nullptr, "hf_plan_status: null argument");
+  HF_CUDA(cudaDeviceSynchronize());
+  HF_CUDA(cudaMemcpy(status, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (reset)
+    HF_CUDA(cudaMemset(p->status, 0, sizeof(int)));
+  return HF_OK;
+}
+
+int hf_pipeline_inspect(hf_plan *p, int w, double *gram, void *wmat, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr && w >= 0 && w < p->d.max_batch, "hf_pipeline_inspect: bad window");
+  const int T = p->d.frames;
+  if (gram) {
+    HF_CHECK_ARG(p->set[0].gram != nullptr, "hf_pipeline_inspect: plan has no clutter filter");
+    HF_CUDA(cudaMemcpyAsync(gram, p->set[0].gram + (int64_t)w * T * T, sizeof(double) * T * T,
+                            cudaMemcpyDeviceToDevice, s));
+  }
+  if (wmat) {
+    const float2 *src = p->set[0].wmat ? p->set[0].wmat + (int64_t)w * T * p->nz : p->wmat_plain;
+    HF_CUDA(cudaMemcpyAsync(wmat, src, sizeof(float2) * T * p->nz, cudaMemcpyDeviceToDevice, s));
+  }
+  return HF_OK;
+}
+
+} // extern "C"
+
+// ================================================================================================
+// Camera stream: device-resident frame ring + window cursor + lookahead filter state
+// ================================================================================================
+struct hf_stream {
+  hf_plan     *plan        = nullptr;
+  uint8_t     *ring        = nullptr;
+  int64_t      ring_frames = 0;
+  int64_t      pushed      = 0;       // frames appended since creation
+  int64_t      next_win    = 0;       // index of the next window to reconstruct
+  float       *dev_out     = nullptr; // staging for host outputs [max_batch][nmom][OH][OW]
+  size_t       bytes       = 0;
+  cudaStream_t side        = nullptr; // eigen phase of the lookahead batch
+  cudaEvent_t  ev_cov      = nullptr; // lookahead Gram matrices written (main stream)
+  cudaEvent_t  ev_ready    = nullptr; // lookahead W matrices written (side stream)
+  bool         look_valid  = false;   // set[look_set] holds W for windows [look_base, +look_n)
+  int64_t      look_base   = 0;
+  int          look_n      = 0;
+  int          look_set    = 1;
+};
+
+extern "C" {
+
+int hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **out) {
+  clear_error();
+  HF_CHECK_ARG(plan != nullptr && out != nullptr, "hf_stream_create: null argument");
+  *out = nullptr;
+  const int64_t need = plan->d.frames + (int64_t)(plan->d.max_batch - 1) * plan->d.hop;
+  HF_CHECK_ARG(ring_frames >= need, "hf_stream_create: ring must hold max_batch overlapping windows");
+  auto *st = new (std::nothrow) hf_stream();
+  if (!st)
+    return fail(HF_ERR_NOMEM, "hf_stream_create: host allocation failed");
+  st->plan        = plan;
+  st->ring_frames = ring_frames;
+  int rc = dev_alloc(&st->ring, (size_t)(ring_frames * plan->frame_bytes), st->bytes);
+  if (rc == HF_OK)
+    rc = dev_alloc(&st->dev_out, (size_t)plan->d.max_batch * plan->nmom * plan->OH * plan->OW, st->bytes);
+  if (rc == HF_OK)
+    rc = cuda_status(cudaStreamCreateWithFlags(&st->side, cudaStreamNonBlocking), "side stream");
+  if (rc == HF_OK)
+    rc = cuda_status(cudaEventCreateWithFlags(&st->ev_cov, cudaEventDisableTiming), "stream event");
+  if (rc == HF_OK)
+    rc = cuda_status(cudaEventCreateWithFlags(&st->ev_ready, cudaEventDisableTiming), "stream event");
+  if (rc != HF_OK) {
+    hf_stream_destroy(st);
+    return rc;
+  }
+  *out = st;
+  return HF_OK;
+}
+
+int hf_stream_destroy(hf_stream *st) {
+  if (!st)
+    return HF_OK;
+  cudaDeviceSynchronize();
+  dev_free(st->ring);
+  dev_free(st->dev_out);
+  if (st->side)
+    cudaStreamDestroy(st->side);
+  if (st->ev_cov)
+    cudaEventDestroy(st->ev_cov);
+  if (st->ev_ready)
+    cudaEventDestroy(st->ev_ready);
+  delete st;
+  return HF_OK;
+}
+
+int64_t hf_stream_ready(const hf_stream *st) {
+  if (!st)
+    return 0;
+  const hf_desc &d = st->plan->d;
+  if (st->pushed < d.frames)
+    return 0;
+  const int64_t complete = (st->pushed - d.frames) / d.hop + 1;
+  return complete - st->next_win;
+}
+
+int hf_stream_push(hf_stream *st, const void *frames, int64_t nframes, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(st != nullptr && (frames != nullptr || nframes == 0) && nframes >= 0, "hf_stream_push: bad argument");
+  const hf_desc &d = st->plan->d;
+  // frames still needed: those of the next window to process and of a prepared lookahead batch
+  const int64_t keep0 = st->next_win * d.hop;
+  HF_CHECK_ARG(st->pushed + nframes - keep0 <= st->ring_frames,
+               "hf_stream_push: ring overrun (process ready windows first)");
+  const int64_t fb   = st->plan->frame_bytes;
+  const auto   *src  = reinterpret_cast<const uint8_t *>(frames);
+  int64_t       done = 0;
+  while (done < nframes) {
+    const int64_t slot = (st->pushed + done) % st->ring_frames;
+    const int64_t n    = std::min(nframes - done, st->ring_frames - slot);
+    HF_CUDA(cudaMemcpyAsync(st->ring + slot * fb, src + done * fb, (size_t)(n * fb), cudaMemcpyDefault, s));
+    done += n;
+  }
+  st->pushed += nframes;
+  return HF_OK;
+}
+
+int hf_stream_process(hf_stream *st, int max_windows, float *out, int out_is_host, int *nwin, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(st != nullptr && out != nullptr, "hf_stream_process: null argument");
+  hf_plan       *p     = st->plan;
+  const hf_desc &d     = p->d;
+  const int64_t  ready = hf_stream_ready(st);
+  const int n = (int)std::min<int64_t>({ready, (int64_t)max_windows, (int64_t)d.max_batch});
+  if (nwin)
+    *nwin = n;
+  if (n <= 0)
+    return HF_OK;
+  const int64_t base = st->next_win;
+  auto win_ring = [&](int64_t w0) { return ring_of(p, st->ring, st->ring_frames, (w0 * d.hop) % st->ring_frames); };
+  const int64_t wstride = (int64_t)d.frames * p->nz;
+  float        *dst     = out_is_host ? st->dev_out : out;
+
+  if (d.clutter_rank == 0) {
+    HF_TRY(phase_propagate(p, win_ring(base), n, p->wmat_plain, 0, dst, s, 0));
+  } else {
+    // 1. W for this batch: prepared by the previous call's lookahead, or computed now
+    int cur;
+    if (st->look_valid && st->look_base == base && st->look_n == n) {
+      cur = st->look_set;
+      HF_CUDA(cudaStreamWaitEvent(s, st->ev_ready, 0));
+    } else {
+      // a stale lookahead (different window range) still owns look_set: let it finish, use the
+      // other set, and recompute this batch's filter here
+      if (st->look_valid)
+        HF_CUDA(cudaStreamWaitEvent(s, st->ev_ready, 0));
+      cur = st->look_valid ? st->look_set ^ 1 : 0;
+      HF_TRY(phase_cov(p, win_ring(base), n, p->set[cur].gram, s));
+      HF_TRY(phase_eigen(p, p->set[cur], n, s));
+    }
+    st->look_valid = false;
+    // 2. lookahead: Gram matrices of the next batch now (whole GPU), its eigen phase on the side
+    //    stream concurrently with this batch's propagation
+    const int n2 = (int)std::min<int64_t>(ready - n, (int64_t)d.max_batch);
+    int       reserve = 0;
+    if (n2 > 0) {
+      const int nxt = cur ^ 1;
+      HF_TRY(phase_cov(p, win_ring(base + n), n2, p->set[nxt].gram, s));
+      HF_CUDA(cudaEventRecord(st->ev_cov, s));
+      HF_CUDA(cudaStreamWaitEvent(st->side, st->ev_cov, 0));
+      HF_TRY(phase_eigen(p, p->set[nxt], n2, st->side));
+      HF_CUDA(cudaEventRecord(st->ev_ready, st->side));
+      st->look_valid = true;
+      st->look_base  = base + n;
+      st->look_n     = n2;
+      st->look_set   = nxt;
+      reserve        = n2; // one SM per lookahead Jacobi
+    }
+    // 3. this batch's propagation
+    HF_TRY(phase_propagate(p, win_ring(base), n, p->set[cur].wmat, wstride, dst, s, reserve));
+  }
+  if (out_is_host) {
+    const size_t bytes = (size_t)n * p->nmom * p->OH * p->OW * sizeof(float);
+    HF_CUDA(cudaMemcpyAsync(out, st->dev_out, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  st->next_win += n;
+  if (p->timer.on)
+    ++p->timer.nexec;
+  return HF_OK;
+}
+
+} // extern "C"

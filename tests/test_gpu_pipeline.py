@@ -149,3 +149,41 @@ def test_chosen_form_fresnel_vs_oracle(cuda, H, W, nwin):
         for m in range(3):
             err = O.rel_l2(got[w, m], exp[m])
             assert err < 1e-3, (w, m, err)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_camera_stream_lookahead_matches_exec(cuda, form):
+    """Windows reconstructed through a camera stream (pushes from host memory, batches of varying
+    size, the next batch's filter prepared ahead on a side stream) equal hf_pipeline_exec of each
+    window alone: bit for bit in the chosen form (exact integer Gram matrices); within 1e-5 in the
+    plain form, whose FP32 covariance splits its partial sums by a grid sized from the batch."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    H = W = 256
+    nwin = 9
+    n = 64 + 16 * (nwin - 1)
+    frames = S.Interferograms(S.config1(n, height=H, width=W)).frames(0, n)
+    packed = O.pack12(frames.reshape(-1)).reshape(n, -1)
+    cfg = pl.PipelineConfig(height=H, width=W, frames=64, hop=16, z_begin=4, z_end=32, fs=67e3, z=0.25,
+                            clutter_rank=4, form=form, max_batch=3)
+    ref = pl.Pipeline(cfg)
+    ring = torch.from_numpy(packed.reshape(-1).copy()).to(cuda)
+    expect = [ref.run(ring, n, 16 * w, 1).cpu().numpy()[0] for w in range(nwin)]
+    p = pl.Pipeline(cfg)
+    cam = pl.CameraStream(p, n)
+    host = torch.from_numpy(packed.copy()).pin_memory()
+    cam.push(host, n)
+    out = torch.empty((3, *p.out_shape), dtype=torch.float32, pin_memory=True)
+    got = []
+    for mw in (2, 2, 1, 3, 3):      # matching and mismatching lookahead batches
+        k = cam.process(mw, out)
+        torch.cuda.synchronize()
+        got += [out[i].numpy().copy() for i in range(k)]
+    assert len(got) == nwin and cam.ready() == 0
+    for w in range(nwin):
+        if form == 1:
+            assert np.array_equal(got[w], expect[w]), w
+        else:
+            assert O.rel_l2(got[w], expect[w]) < 1e-5, w
+    assert p.status() == 0
