@@ -120,6 +120,17 @@ int hf_covariance(const void *in, int in_dtype, int64_t batch, int T, int64_t P,
   return launch_covariance(fr, in_dtype, T, P, (int)batch, ws, gram, s);
 }
 
+int hf_covariance_noalloc(const void *in, int in_dtype, int64_t batch, int T, int64_t P, double *gram,
+                          hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(in != nullptr && gram != nullptr, "hf_covariance_noalloc: null pointer");
+  HF_CHECK_ARG(batch >= 1 && batch <= 65535 && T >= 1 && P >= 1, "hf_covariance_noalloc: bad extents");
+  HF_CHECK_ARG(real_fmt(in_dtype), "hf_covariance_noalloc: unsupported dtype");
+  HF_CHECK_ARG(in_dtype != HF_MONO12P || P % 2 == 0, "hf_covariance_noalloc: packed frames need even P");
+  FrameRing fr{reinterpret_cast<const uint8_t *>(in), batch * T, 0, T, frame_bytes_of(in_dtype, P)};
+  return launch_covariance_fixed_scratch(fr, in_dtype, T, P, (int)batch, gram, s);
+}
+
 int hf_eigh_jacobi_f64(const double *a, double *evecs, double *evals, int *info, int n,
                        int64_t batch, hf_stream_t s) {
   clear_error();

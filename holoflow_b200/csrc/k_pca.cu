@@ -6,7 +6,10 @@
 // (pca_heev.cc:35-133) and the projection X V[:, begin:end].  Here the Gram matrix is
 // accumulated in FP32 over pixel tiles on shifted samples (x - 2048 is exact for 12-bit data)
 // and reduced in FP64 with the shift undone exactly; the eigensolver is FP64 throughout.
+#include <algorithm>
 #include <cfloat>
+#include <mutex>
+#include <string>
 
 #include "k_pca.cuh"
 
@@ -197,14 +200,16 @@ int cov_ctas_per_window(int64_t P, int nwin) {
   return ctas;
 }
 
+// `max_ctas` > 0 caps the CTAs per window (and so the workspace) below the default split.
 template <int FMT, int T>
 int launch_cov_tiled(const FrameRing &ring, int64_t P, int nwin, void *ws, double *gram,
-                     cudaStream_t s) {
+                     cudaStream_t s, int max_ctas = 0) {
   using Gm = CovGeom<T>;
   constexpr int RB   = kCovPT * Bpp<FMT>::num / Bpp<FMT>::den;
   constexpr int RW   = RB / 4 + 1;
   const size_t  smem = (size_t)T * RW * 4 + (size_t)kCovPT * Gm::XS * 4 + T * 8;
-  const int     ctas = cov_ctas_per_window(P, nwin);
+  const int     ctas = max_ctas > 0 ? std::min(max_ctas, cov_ctas_per_window(P, nwin))
+                                    : cov_ctas_per_window(P, nwin);
   CovArgs       a;
   a.ring    = ring;
   a.T       = T;
@@ -562,6 +567,89 @@ int launch_pca_project(const float *in, int64_t batch, int T, int64_t P, const d
       in, T, P, evecs, begin, ncomp, out);
   note_launch();
   return launch_status("pca_project_kernel");
+}
+
+// ------------------------------------------------------------------------------------------------
+// Gram matrices with a fixed, library-owned workspace (hf_covariance_noalloc).
+//
+// The workspace is a file-scope device array, so the module loader reserves it once per device
+// and the call itself never allocates.  Its device address is looked up once per device (with
+// that device current) and cached.  The tiled kernel writes every partial and per-frame sum the
+// reduction reads before it is read, so nothing in the array has to start at zero.  Every call
+// on a device uses the same array: calls whose work overlaps in time race on it.
+// ------------------------------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_cov_scratch[HF_COVARIANCE_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxScratchDevices = 64;
+std::mutex    g_scratch_mu;
+void         *g_scratch_ptr[kMaxScratchDevices] = {};
+
+int scratch_address(void **ptr) {
+  int dev = 0;
+  HF_CUDA(cudaGetDevice(&dev));
+  HF_CHECK_ARG(dev >= 0 && dev < kMaxScratchDevices, "hf_covariance_noalloc: device ordinal above 63");
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (g_scratch_ptr[dev] == nullptr) {
+    void             *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_cov_scratch);
+    if (e != cudaSuccess)
+      return cuda_status(e, "hf_covariance_noalloc: cudaGetSymbolAddress of the fixed workspace");
+    g_scratch_ptr[dev] = p;
+  }
+  *ptr = g_scratch_ptr[dev];
+  return HF_OK;
+}
+
+// CTAs per window that fit the fixed workspace (0 when even one does not).
+template <int T> int fitting_ctas(int nwin) {
+  using Gm                 = CovGeom<T>;
+  const size_t per_cta     = (size_t)Gm::G * T * T * sizeof(float) + (size_t)T * sizeof(double);
+  const size_t usable      = HF_COVARIANCE_NOALLOC_SCRATCH_BYTES - 256;
+  const size_t fit         = usable / ((size_t)nwin * per_cta);
+  return (int)std::min<size_t>(fit, (size_t)1 << 20);
+}
+
+template <int FMT, int T>
+int cov_fixed_tiled(const FrameRing &ring, int64_t P, int nwin, void *ws, double *gram, cudaStream_t s) {
+  const int fit = fitting_ctas<T>(nwin);
+  if (fit < 1)
+    return fail(HF_ERR_INVALID,
+                "hf_covariance_noalloc: batch " + std::to_string(nwin) + " at T = " + std::to_string(T) +
+                    " needs more than the fixed " +
+                    std::to_string(HF_COVARIANCE_NOALLOC_SCRATCH_BYTES >> 20) +
+                    " MiB workspace; split the batch or use hf_covariance with a workspace");
+  return launch_cov_tiled<FMT, T>(ring, P, nwin, ws, gram, s, fit);
+}
+
+template <int FMT>
+int cov_fixed_fmt(const FrameRing &ring, int T, int64_t P, int nwin, double *gram, cudaStream_t s) {
+  const bool tiled = (P % 8 == 0) && (ring.frame_bytes % 4 == 0) && (T == 32 || T == 64 || T == 128);
+  if (!tiled) { // the direct kernel needs no workspace
+    cov_generic_kernel<FMT><<<dim3((T * T + 127) / 128, nwin), 128, 0, s>>>(ring, T, P, gram);
+    note_launch();
+    return launch_status("cov_generic_kernel");
+  }
+  void *ws = nullptr;
+  HF_TRY(scratch_address(&ws));
+  if (T == 32)
+    return cov_fixed_tiled<FMT, 32>(ring, P, nwin, ws, gram, s);
+  if (T == 64)
+    return cov_fixed_tiled<FMT, 64>(ring, P, nwin, ws, gram, s);
+  return cov_fixed_tiled<FMT, 128>(ring, P, nwin, ws, gram, s);
+}
+} // namespace
+
+int launch_covariance_fixed_scratch(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, double *gram,
+                                    cudaStream_t s) {
+  HF_CHECK_ARG(T > 0 && P > 0 && nwin > 0, "covariance: empty problem");
+  switch (fmt) {
+  case HF_MONO12P: return cov_fixed_fmt<HF_MONO12P>(ring, T, P, nwin, gram, s);
+  case HF_U16: return cov_fixed_fmt<HF_U16>(ring, T, P, nwin, gram, s);
+  case HF_U8: return cov_fixed_fmt<HF_U8>(ring, T, P, nwin, gram, s);
+  case HF_F32: return cov_fixed_fmt<HF_F32>(ring, T, P, nwin, gram, s);
+  default: return fail(HF_ERR_INVALID, "covariance: unsupported input dtype");
+  }
 }
 
 } // namespace hf

@@ -32,6 +32,10 @@ int    launch_covariance_tc(const FrameRing &ring, int fmt, int T, int64_t P, in
 // Full Gram computation: block partials -> deterministic float64 reduction -> gram[nwin][T][T].
 int launch_covariance(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, void *ws,
                       double *gram, cudaStream_t s);
+// The same computation on the library's fixed device workspace (no allocation; see
+// hf_covariance_noalloc for the limits).
+int launch_covariance_fixed_scratch(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, double *gram,
+                                    cudaStream_t s);
 
 // FP64 cyclic Jacobi, one CTA per matrix (n <= 128).  Eigenvalues ascending, eigenvector j in
 // column j of evecs (row-major).

@@ -53,6 +53,14 @@ def covariance(frames: torch.Tensor, dtype: int, batch: int, T: int, P: int) -> 
     return gram
 
 
+def covariance_noalloc(frames: torch.Tensor, dtype: int, batch: int, T: int, P: int,
+                       gram: torch.Tensor) -> torch.Tensor:
+    """Gram matrices into the caller's `gram` [batch][T][T] float64 using the library's fixed
+    device workspace: the call allocates nothing (hf_covariance_noalloc)."""
+    check(lib().hf_covariance_noalloc(_ptr(frames), dtype, batch, T, P, _ptr(gram), _stream()))
+    return gram
+
+
 def eigh_jacobi(a: torch.Tensor):
     batch, n, _ = a.shape
     evecs = torch.empty_like(a)

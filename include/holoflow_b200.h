@@ -95,6 +95,26 @@ size_t hf_covariance_workspace_bytes(int T, int64_t P);
 int    hf_covariance(const void *in, int in_dtype, int64_t batch, int T, int64_t P, double *gram,
                      void *ws, hf_stream_t s);
 
+/* hf_covariance_noalloc: hf_covariance without a caller workspace and without any allocation.
+ * It has no counterpart in the reference (PcaTask gets its buffers from the task's allocator).
+ * It is for callers that hold device pointers to frames and the Gram output but cannot allocate
+ * device memory when they call: a camera callback or real-time acquisition thread, where
+ * cudaMalloc's implicit device synchronisation would stall the stream, or a host program that
+ * has no device allocator of its own to make a workspace with.
+ * The workspace is a fixed HF_COVARIANCE_NOALLOC_SCRATCH_BYTES array inside the library, one per
+ * device, reserved when the library's device code is loaded.  Nothing in it has to start at zero.
+ *  - The first call on a device (made with that device current) looks up the array's address
+ *    and caches it; make that first call before any stream capture on that device.
+ *  - A batch whose partial sums cannot fit (batch x one CTA's partials, T*T*4*G + T*8 bytes with
+ *    G = 4, 2, 1 for T = 32, 64, 128) is rejected with HF_ERR_INVALID; larger problems are split
+ *    over fewer CTAs so that they fit, which can change the float32 rounding of the partials.
+ *  - Calls on one device share the array: calls whose work can overlap in time (different
+ *    streams without ordering, or different host threads) race; serialise them on one stream.
+ * Arguments, results and errors are otherwise those of hf_covariance. */
+#define HF_COVARIANCE_NOALLOC_SCRATCH_BYTES (16u << 20)
+int    hf_covariance_noalloc(const void *in, int in_dtype, int64_t batch, int T, int64_t P, double *gram,
+                             hf_stream_t s);
+
 /* Symmetric eigendecomposition (PcaHeevSolver::launch, pca_heev.cc:101-121) by FP64 cyclic
  * Jacobi, one CTA per matrix, n <= 128.  a: [batch][n][n] row-major symmetric; on return
  * evecs[b] holds eigenvector j in COLUMN j (row-major [n][n]), evals[b] ascending.  info[b] = 0 on
