@@ -89,6 +89,7 @@ _PROTOS = {
     "hf_stream_push": (C.c_int, [_vp, _vp, _i64, _vp]),
     "hf_stream_ready": (_i64, [_vp]),
     "hf_stream_process": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.POINTER(C.c_int), _vp]),
+    "hf_stream_output_wait": (C.c_int, [_vp, _vp, C.c_int]),
     "hf_plan_stage_times": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
 }

@@ -491,7 +491,7 @@ struct hf_stream {
   int64_t      ring_frames = 0;
   int64_t      pushed      = 0;       // frames appended since creation
   int64_t      next_win    = 0;       // index of the next window to reconstruct
-  float       *dev_out     = nullptr; // staging for host outputs [max_batch][nmom][OH][OW]
+  float       *stage[2]    = {};      // staging for host outputs, 2 x [max_batch][nmom][OH][OW]
   size_t       bytes       = 0;
   cudaStream_t side        = nullptr; // eigen phase of the lookahead batch
   cudaEvent_t  ev_cov      = nullptr; // lookahead Gram matrices written (main stream)
@@ -500,7 +500,58 @@ struct hf_stream {
   int64_t      look_base   = 0;
   int          look_n      = 0;
   int          look_set    = 1;
+
+  // Ordering between pushes and processes issued on different CUDA streams: the absolute frame
+  // range each recent push wrote and each recent process read, with an event recorded after it.
+  static constexpr int kHist = 8;
+  struct Rec {
+    int64_t     lo = 0, hi = -1;
+    cudaEvent_t ev = nullptr;
+  };
+  Rec     push_rec[kHist];
+  Rec     proc_rec[kHist];
+  int64_t npush = 0, nproc = 0;
+
+  // Asynchronous host output (out_is_host == 2): the copy of stage[k] runs on `d2h`.
+  cudaStream_t d2h            = nullptr;
+  cudaEvent_t  ev_out[2]      = {}; // stage[k] written by the compute stream
+  cudaEvent_t  ev_d2h[2]      = {}; // stage[k] copied to the host
+  bool         d2h_pending[2] = {};
+  int          stage_k        = 0;
+  int          last_k         = -1;
 };
+
+namespace {
+// Makes `s` wait until every push that wrote frames up to absolute index `need_hi` has landed.
+// Pushes of one camera stream are issued in order on one CUDA stream, so the oldest recorded push
+// that reaches `need_hi` covers all earlier ones.
+int wait_for_pushes(hf_stream *st, int64_t need_hi, cudaStream_t s) {
+  const int64_t first = std::max<int64_t>(0, st->npush - hf_stream::kHist);
+  for (int64_t i = first; i < st->npush; ++i) {
+    const hf_stream::Rec &r = st->push_rec[i % hf_stream::kHist];
+    if (r.hi >= need_hi)
+      return cuda_status(cudaStreamWaitEvent(s, r.ev, 0), "hf_stream_process: wait for pushed frames");
+  }
+  return fail(HF_ERR_STATE, "hf_stream_process: frames of the batch were never pushed");
+}
+
+// Makes `s` wait until no recorded process still reads a frame in [dlo, dhi] (the frames a push is
+// about to overwrite).  Processes are issued in order on one CUDA stream, so waiting for the most
+// recent one that started at or below dhi covers all earlier ones; if every recorded process
+// starts above dhi but older ones were dropped from the record, the oldest recorded one covers them.
+int wait_for_readers(hf_stream *st, int64_t dhi, cudaStream_t s) {
+  const int64_t first = std::max<int64_t>(0, st->nproc - hf_stream::kHist);
+  for (int64_t i = st->nproc - 1; i >= first; --i) {
+    const hf_stream::Rec &r = st->proc_rec[i % hf_stream::kHist];
+    if (r.lo <= dhi)
+      return cuda_status(cudaStreamWaitEvent(s, r.ev, 0), "hf_stream_push: wait for readers");
+  }
+  if (first > 0)
+    return cuda_status(cudaStreamWaitEvent(s, st->proc_rec[first % hf_stream::kHist].ev, 0),
+                       "hf_stream_push: wait for readers");
+  return HF_OK;
+}
+} // namespace
 
 extern "C" {
 
@@ -515,15 +566,23 @@ int hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **out) {
     return fail(HF_ERR_NOMEM, "hf_stream_create: host allocation failed");
   st->plan        = plan;
   st->ring_frames = ring_frames;
+  const size_t out_elems = (size_t)plan->d.max_batch * plan->nmom * plan->OH * plan->OW;
   int rc = dev_alloc(&st->ring, (size_t)(ring_frames * plan->frame_bytes), st->bytes);
-  if (rc == HF_OK)
-    rc = dev_alloc(&st->dev_out, (size_t)plan->d.max_batch * plan->nmom * plan->OH * plan->OW, st->bytes);
+  for (int k = 0; k < 2 && rc == HF_OK; ++k)
+    rc = dev_alloc(&st->stage[k], out_elems, st->bytes);
   if (rc == HF_OK)
     rc = cuda_status(cudaStreamCreateWithFlags(&st->side, cudaStreamNonBlocking), "side stream");
   if (rc == HF_OK)
-    rc = cuda_status(cudaEventCreateWithFlags(&st->ev_cov, cudaEventDisableTiming), "stream event");
-  if (rc == HF_OK)
-    rc = cuda_status(cudaEventCreateWithFlags(&st->ev_ready, cudaEventDisableTiming), "stream event");
+    rc = cuda_status(cudaStreamCreateWithFlags(&st->d2h, cudaStreamNonBlocking), "output copy stream");
+  cudaEvent_t *evs[] = {&st->ev_cov, &st->ev_ready, &st->ev_out[0], &st->ev_out[1], &st->ev_d2h[0], &st->ev_d2h[1]};
+  for (cudaEvent_t *e : evs)
+    if (rc == HF_OK)
+      rc = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "stream event");
+  for (int i = 0; i < hf_stream::kHist && rc == HF_OK; ++i) {
+    rc = cuda_status(cudaEventCreateWithFlags(&st->push_rec[i].ev, cudaEventDisableTiming), "stream event");
+    if (rc == HF_OK)
+      rc = cuda_status(cudaEventCreateWithFlags(&st->proc_rec[i].ev, cudaEventDisableTiming), "stream event");
+  }
   if (rc != HF_OK) {
     hf_stream_destroy(st);
     return rc;
@@ -537,13 +596,20 @@ int hf_stream_destroy(hf_stream *st) {
     return HF_OK;
   cudaDeviceSynchronize();
   dev_free(st->ring);
-  dev_free(st->dev_out);
-  if (st->side)
-    cudaStreamDestroy(st->side);
-  if (st->ev_cov)
-    cudaEventDestroy(st->ev_cov);
-  if (st->ev_ready)
-    cudaEventDestroy(st->ev_ready);
+  for (float *&b : st->stage)
+    dev_free(b);
+  for (cudaStream_t q : {st->side, st->d2h})
+    if (q)
+      cudaStreamDestroy(q);
+  for (cudaEvent_t e : {st->ev_cov, st->ev_ready, st->ev_out[0], st->ev_out[1], st->ev_d2h[0], st->ev_d2h[1]})
+    if (e)
+      cudaEventDestroy(e);
+  for (int i = 0; i < hf_stream::kHist; ++i) {
+    if (st->push_rec[i].ev)
+      cudaEventDestroy(st->push_rec[i].ev);
+    if (st->proc_rec[i].ev)
+      cudaEventDestroy(st->proc_rec[i].ev);
+  }
   delete st;
   return HF_OK;
 }
@@ -566,6 +632,12 @@ int hf_stream_push(hf_stream *st, const void *frames, int64_t nframes, hf_stream
   const int64_t keep0 = st->next_win * d.hop;
   HF_CHECK_ARG(st->pushed + nframes - keep0 <= st->ring_frames,
                "hf_stream_push: ring overrun (process ready windows first)");
+  if (nframes == 0)
+    return HF_OK;
+  // the slots about to be written held frames [pushed - R, pushed + n - R): wait for their readers
+  const int64_t dhi = st->pushed + nframes - st->ring_frames - 1;
+  if (dhi >= 0)
+    HF_TRY(wait_for_readers(st, dhi, s));
   const int64_t fb   = st->plan->frame_bytes;
   const auto   *src  = reinterpret_cast<const uint8_t *>(frames);
   int64_t       done = 0;
@@ -575,6 +647,11 @@ int hf_stream_push(hf_stream *st, const void *frames, int64_t nframes, hf_stream
     HF_CUDA(cudaMemcpyAsync(st->ring + slot * fb, src + done * fb, (size_t)(n * fb), cudaMemcpyDefault, s));
     done += n;
   }
+  hf_stream::Rec &r = st->push_rec[st->npush % hf_stream::kHist];
+  r.lo = st->pushed;
+  r.hi = st->pushed + nframes - 1;
+  HF_CUDA(cudaEventRecord(r.ev, s));
+  ++st->npush;
   st->pushed += nframes;
   return HF_OK;
 }
@@ -582,6 +659,7 @@ int hf_stream_push(hf_stream *st, const void *frames, int64_t nframes, hf_stream
 int hf_stream_process(hf_stream *st, int max_windows, float *out, int out_is_host, int *nwin, hf_stream_t s) {
   clear_error();
   HF_CHECK_ARG(st != nullptr && out != nullptr, "hf_stream_process: null argument");
+  HF_CHECK_ARG(out_is_host >= 0 && out_is_host <= 2, "hf_stream_process: out_is_host must be 0, 1 or 2");
   hf_plan       *p     = st->plan;
   const hf_desc &d     = p->d;
   const int64_t  ready = hf_stream_ready(st);
@@ -593,7 +671,23 @@ int hf_stream_process(hf_stream *st, int max_windows, float *out, int out_is_hos
   const int64_t base = st->next_win;
   auto win_ring = [&](int64_t w0) { return ring_of(p, st->ring, st->ring_frames, (w0 * d.hop) % st->ring_frames); };
   const int64_t wstride = (int64_t)d.frames * p->nz;
-  float        *dst     = out_is_host ? st->dev_out : out;
+  // windows of the lookahead batch (their Gram matrices are computed by this call)
+  const int n2 = d.clutter_rank == 0 ? 0 : (int)std::min<int64_t>(ready - n, (int64_t)d.max_batch);
+
+  // frames read by this call: windows [base, base + n + n2); wait for the pushes that bring them
+  const int64_t read_lo = base * d.hop;
+  const int64_t read_hi = (base + n + n2 - 1) * d.hop + d.frames - 1;
+  HF_TRY(wait_for_pushes(st, read_hi, s));
+
+  float *dst = out;
+  int    k   = -1;
+  if (out_is_host) { // stage the images; the staging buffer's previous copy must have finished
+    k           = st->stage_k;
+    st->stage_k = k ^ 1;
+    if (st->d2h_pending[k])
+      HF_CUDA(cudaStreamWaitEvent(s, st->ev_d2h[k], 0));
+    dst = st->stage[k];
+  }
 
   if (d.clutter_rank == 0) {
     HF_TRY(phase_propagate(p, win_ring(base), n, p->wmat_plain, 0, dst, s, 0));
@@ -615,8 +709,7 @@ int hf_stream_process(hf_stream *st, int max_windows, float *out, int out_is_hos
     st->look_valid = false;
     // 2. lookahead: Gram matrices of the next batch now (whole GPU), its eigen phase on the side
     //    stream concurrently with this batch's propagation
-    const int n2 = (int)std::min<int64_t>(ready - n, (int64_t)d.max_batch);
-    int       reserve = 0;
+    int reserve = 0;
     if (n2 > 0) {
       const int nxt = cur ^ 1;
       HF_TRY(phase_cov(p, win_ring(base + n), n2, p->set[nxt].gram, s));
@@ -633,13 +726,40 @@ int hf_stream_process(hf_stream *st, int max_windows, float *out, int out_is_hos
     // 3. this batch's propagation
     HF_TRY(phase_propagate(p, win_ring(base), n, p->set[cur].wmat, wstride, dst, s, reserve));
   }
-  if (out_is_host) {
-    const size_t bytes = (size_t)n * p->nmom * p->OH * p->OW * sizeof(float);
-    HF_CUDA(cudaMemcpyAsync(out, st->dev_out, bytes, cudaMemcpyDeviceToHost, s));
+  // every frame read by this call has been consumed once `s` passes this point
+  hf_stream::Rec &r = st->proc_rec[st->nproc % hf_stream::kHist];
+  r.lo = read_lo;
+  r.hi = read_hi;
+  HF_CUDA(cudaEventRecord(r.ev, s));
+  ++st->nproc;
+
+  const size_t bytes = (size_t)n * p->nmom * p->OH * p->OW * sizeof(float);
+  if (out_is_host == 1) { // copy in stream order: the images are on the host once `s` passes here
+    HF_CUDA(cudaMemcpyAsync(out, st->stage[k], bytes, cudaMemcpyDeviceToHost, s));
+    st->d2h_pending[k] = false;
+  } else if (out_is_host == 2) { // copy on the stream's own copy engine queue, overlapping later work
+    HF_CUDA(cudaEventRecord(st->ev_out[k], s));
+    HF_CUDA(cudaStreamWaitEvent(st->d2h, st->ev_out[k], 0));
+    HF_CUDA(cudaMemcpyAsync(out, st->stage[k], bytes, cudaMemcpyDeviceToHost, st->d2h));
+    HF_CUDA(cudaEventRecord(st->ev_d2h[k], st->d2h));
+    st->d2h_pending[k] = true;
+    st->last_k         = k;
   }
   st->next_win += n;
   if (p->timer.on)
     ++p->timer.nexec;
+  return HF_OK;
+}
+
+int hf_stream_output_wait(hf_stream *st, hf_stream_t s, int host_block) {
+  clear_error();
+  HF_CHECK_ARG(st != nullptr, "hf_stream_output_wait: null stream");
+  if (st->last_k < 0 || !st->d2h_pending[st->last_k])
+    return HF_OK;
+  if (host_block)
+    HF_CUDA(cudaEventSynchronize(st->ev_d2h[st->last_k]));
+  else
+    HF_CUDA(cudaStreamWaitEvent(s, st->ev_d2h[st->last_k], 0));
   return HF_OK;
 }
 

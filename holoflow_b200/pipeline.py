@@ -240,11 +240,18 @@ class CameraStream:
     def ready(self) -> int:
         return lib().hf_stream_ready(self._s)
 
-    def process(self, max_windows: int, out: torch.Tensor, stream=None) -> int:
+    def process(self, max_windows: int, out: torch.Tensor, stream=None, async_copy: bool = False) -> int:
+        """Reconstructs up to `max_windows` ready windows into `out` (device, or pinned host).
+        With a host `out` and async_copy, the D2H copy overlaps later work: call output_wait()
+        before reading `out`."""
         n = C.c_int()
-        check(lib().hf_stream_process(self._s, max_windows, _ptr(out), int(not out.is_cuda), C.byref(n),
-                                      _stream(stream)))
+        mode = 0 if out.is_cuda else (2 if async_copy else 1)
+        check(lib().hf_stream_process(self._s, max_windows, _ptr(out), mode, C.byref(n), _stream(stream)))
         return n.value
+
+    def output_wait(self, stream=None, host_block: bool = False) -> None:
+        """Waits for the latest asynchronous output copy (on the host, or by making `stream` wait)."""
+        check(lib().hf_stream_output_wait(self._s, _stream(stream), int(host_block)))
 
     def close(self):
         if self._s:

@@ -236,8 +236,20 @@ int hf_pipeline_inspect(hf_plan *plan, int w, double *gram, void *wmat, hf_strea
  * A stream owns a device ring of `ring_frames` frames of the plan's input format and a window
  * cursor.  hf_stream_push appends frames (host or device memory; copies are enqueued on `s`;
  * HF_ERR_INVALID if it would overwrite frames of a window not yet processed).  hf_stream_process
- * reconstructs up to min(max_windows, max_batch) ready windows in one hf_pipeline_exec; `out` is
- * device memory, or pinned host memory when out_is_host (a D2H copy is enqueued on `s`). */
+ * reconstructs up to min(max_windows, max_batch) ready windows in one hf_pipeline_exec, and
+ * computes the Gram matrices of the next ready batch so that its eigen phase overlaps this
+ * batch's propagation on a side stream.
+ * Pushes may be issued on a different CUDA stream than processes (to overlap the H2D copy of
+ * later frames with the reconstruction of earlier ones): a process waits for the pushes that
+ * brought its frames, and a push waits for the processes still reading the slots it overwrites.
+ * All pushes of one camera stream must use one CUDA stream, and all processes one CUDA stream.
+ * out_is_host: 0 = `out` is device memory; 1 = pinned host memory, copied in order on `s` (the
+ * images are on the host when `s` reaches that point); 2 = pinned host memory, copied on the
+ * camera stream's own copy stream so that the copy overlaps later work on `s` -- the images are
+ * on the host once hf_stream_output_wait has returned with host_block = 1, or once a stream made
+ * to wait by hf_stream_output_wait(st, s2, 0) reaches that point.  Two consecutive mode-2 calls
+ * use two staging buffers, so the host buffer of a call must stay untouched until its copy is
+ * known to be complete. */
 typedef struct hf_stream hf_stream;
 int     hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **stream);
 int     hf_stream_destroy(hf_stream *stream);
@@ -245,6 +257,9 @@ int     hf_stream_push(hf_stream *stream, const void *frames, int64_t nframes, h
 int64_t hf_stream_ready(const hf_stream *stream);
 int     hf_stream_process(hf_stream *stream, int max_windows, float *out, int out_is_host, int *nwin,
                           hf_stream_t s);
+/* Waits for the most recent asynchronous (out_is_host = 2) output copy: on the host when
+ * host_block, else by making `s` wait for it. */
+int     hf_stream_output_wait(hf_stream *stream, hf_stream_t s, int host_block);
 
 #ifdef __cplusplus
 }

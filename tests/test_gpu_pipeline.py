@@ -187,3 +187,49 @@ def test_camera_stream_lookahead_matches_exec(cuda, form):
         else:
             assert O.rel_l2(got[w], expect[w]) < 1e-5, w
     assert p.status() == 0
+
+
+def test_camera_stream_push_stream_and_async_output(cuda):
+    """Pushes on their own CUDA stream, two steps ahead of the reconstruction, with images copied
+    to the host asynchronously into alternating buffers, and a ring just large enough that pushes
+    overwrite slots that recent processes read: every window equals hf_pipeline_exec of it alone."""
+    import torch
+    from holoflow_b200 import pipeline as pl
+    H = W = 256
+    B, hop, T = 2, 16, 64
+    nsteps = 7
+    n = (T - hop) + (nsteps + 2) * B * hop
+    frames = S.Interferograms(S.config1(n, height=H, width=W)).frames(0, n)
+    packed = O.pack12(frames.reshape(-1)).reshape(n, -1)
+    cfg = pl.PipelineConfig(height=H, width=W, frames=T, hop=hop, z_begin=4, z_end=32, fs=67e3, z=0.25,
+                            clutter_rank=4, form=1, max_batch=B)
+    ref = pl.Pipeline(cfg)
+    ring = torch.from_numpy(packed.reshape(-1).copy()).to(cuda)
+    expect = [ref.run(ring, n, hop * w, 1).cpu().numpy()[0] for w in range(nsteps * B)]
+    p = pl.Pipeline(cfg)
+    cam = pl.CameraStream(p, (T - hop) + 4 * B * hop)
+    host = torch.from_numpy(packed.copy()).pin_memory()
+    h2d = torch.cuda.Stream(device=cuda)
+    main = torch.cuda.current_stream()
+    outs = [torch.empty((B, *p.out_shape), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    pos = 0
+
+    def push(k):
+        nonlocal pos
+        cam.push(host[pos:pos + k], k, stream=h2d)
+        pos += k
+
+    push(T - hop)
+    push(B * hop)
+    push(B * hop)
+    got = []
+    for s in range(nsteps):
+        push(B * hop)
+        k = cam.process(B, outs[s % 2], stream=main, async_copy=True)
+        assert k == B
+        cam.output_wait(host_block=True)
+        got += [outs[s % 2][i].numpy().copy() for i in range(B)]
+    torch.cuda.synchronize()
+    for w in range(nsteps * B):
+        assert np.array_equal(got[w], expect[w]), w
+    assert p.status() == 0
