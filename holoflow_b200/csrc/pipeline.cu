@@ -17,10 +17,12 @@
 
 #include "host_util.cuh"
 #include "k_band.cuh"
+#include "k_cols_tma.cuh"
 #include "k_fft2d.cuh"
 #include "k_misc.cuh"
 #include "k_pca.cuh"
 #include "k_tc_band.cuh"
+#include "tma_host.cuh"
 
 using namespace hf;
 
@@ -92,6 +94,8 @@ struct hf_plan {
   void      *cov_ws = nullptr;
   bool       cov_tc = false;   // tensor-core Gram matrix (chosen form)
   bool       rows_tc = false;  // tensor-core band DFT fused with lens + row FFT (chosen form)
+  bool       cols_tma = false; // TMA-fed column FFT + moments over `band` through band_tmap
+  CUtensorMap band_tmap{};
   size_t     bytes = 0;
   StageTimer timer;
 };
@@ -154,6 +158,29 @@ static int phase_eigen(hf_plan *p, const FilterSet &fs, int nwin, cudaStream_t s
   return HF_OK;
 }
 
+// Column FFT + |.| + moments of the band planes in p->band into `out`.
+static int cols_moments(hf_plan *p, int nwin, float *out, cudaStream_t s) {
+  const hf_desc &d      = p->d;
+  const int64_t  win_px = (int64_t)p->nz * p->P;
+  const int64_t  oplane = (int64_t)p->OH * p->OW;
+  const int      rec    = p->timer.begin(s, ST_COLS_MOM);
+  if (p->cols_tma) {
+    ColMomArgs ca{};
+    ca.H = d.height, ca.W = d.width, ca.nz = p->nz, ca.rows_per_win = (int64_t)p->nz * d.height;
+    ca.out = out, ca.out_win = (int64_t)p->nmom * oplane, ca.out_plane = oplane, ca.out_row = p->OW;
+    ca.status = p->status;
+    HF_TRY(launch_col_moments_tma(p->band_tmap, ca, p->mom, nwin, s));
+  } else {
+    ColPass cp{};
+    cp.in = p->band, cp.in_win = win_px, cp.in_plane = p->P, cp.in_row = d.width;
+    cp.H = d.height, cp.W = d.width, cp.nplanes = p->nz, cp.inverse = 0;
+    cp.out = out, cp.out_win = (int64_t)p->nmom * oplane, cp.out_plane = oplane, cp.out_row = p->OW, cp.out_col = 1;
+    HF_TRY(launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s));
+  }
+  p->timer.end(s, rec);
+  return HF_OK;
+}
+
 // Band DFT with W (per window, or shared when wstride == 0), propagation and moments.
 // `reserve_sms` SMs are left to concurrently running work by the persistent tensor-core pass.
 static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const float2 *wmat, int64_t wstride,
@@ -173,14 +200,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     int rec = p->timer.begin(s, ST_BAND_ROWS);
     HF_TRY(launch_band_rows_tc(br, d.input_dtype, s));
     p->timer.end(s, rec);
-    ColPass cp{};
-    cp.in = p->band, cp.in_win = win_px, cp.in_plane = p->P, cp.in_row = d.width;
-    cp.H = d.height, cp.W = d.width, cp.nplanes = p->nz;
-    cp.out = out, cp.out_win = owin, cp.out_plane = oplane, cp.out_row = p->OW, cp.out_col = 1;
-    rec = p->timer.begin(s, ST_COLS_MOM);
-    HF_TRY(launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s));
-    p->timer.end(s, rec);
-    return HF_OK;
+    return cols_moments(p, nwin, out, s);
   }
 
   BandArgs ba{};
@@ -212,14 +232,13 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     rec = p->timer.begin(s, ST_ROWS);
     HF_TRY(launch_row_pass(rp, nwin, s));
     p->timer.end(s, rec);
+    if (p->fast)
+      return cols_moments(p, nwin, out, s);
     ColPass cp{};
     cp.in = rp.out, cp.in_win = win_px, cp.in_plane = p->P, cp.in_row = d.width;
     cp.H = d.height, cp.W = d.width, cp.nplanes = p->nz, cp.inverse = 0;
     rec = p->timer.begin(s, ST_COLS_MOM);
-    if (p->fast) {
-      cp.out = out, cp.out_win = owin, cp.out_plane = oplane, cp.out_row = p->OW, cp.out_col = 1;
-      HF_TRY(launch_col_pass(cp, COL_MOMENTS, &p->mom, nwin, s));
-    } else { // general sizes: complex column DFT back into `band`, then the moment reduction
+    { // general sizes: complex column DFT back into `band`, then the moment reduction
       HF_CHECK_ARG(!d.fftshift, "fftshift needs four-step frame sizes");
       cp.out = p->band, cp.out_win = win_px, cp.out_plane = p->P, cp.out_row = d.width, cp.out_col = 1;
       HF_TRY(launch_col_pass(cp, COL_COMPLEX, nullptr, nwin, s));
@@ -353,6 +372,13 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       break;
     p->rows_tc = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
                  band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
+    if (d.propagation == HF_PROP_FRESNEL && p->fast && col_moments_tma_supported(d.height, d.width)) {
+      const uint64_t rows = (uint64_t)B * p->nz * d.height;
+      if ((rc = make_tmap_2d_f32(&p->band_tmap, p->band, 2 * (uint64_t)d.width, rows, 8 * (uint64_t)d.width, 16,
+                                 (uint32_t)std::min(d.height, 256))))
+        break;
+      p->cols_tma = true;
+    }
     rc = plan_tables(p, stream);
   } while (0);
   if (rc != HF_OK) {

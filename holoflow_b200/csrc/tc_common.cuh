@@ -125,6 +125,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *mbar, uint32_t parity) {
   return ok != 0;
 }
 
+// Arms `mbar` for one arrival plus `bytes` of asynchronous-copy transactions.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+               : "memory");
+}
+
+// ---- TMA (no multicast) --------------------------------------------------------------------------
+// 2D tiled load of the box at element coordinates (x, y) of `tmap` into shared memory; completion
+// is signalled as transaction bytes on `mbar`.  x times the element size must be a multiple of 16.
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *tmap, int x, int y, uint64_t *mbar) {
+  asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+               ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(mbar))
+               : "memory");
+}
+__device__ __forceinline__ void tma_prefetch_desc(const void *tmap) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
+}
+
 // Waits for phase `parity` of `mbar` with an iteration bound; on expiry records `code` in the
 // status word (first writer wins) and returns false instead of hanging.
 constexpr uint32_t kWaitLimit = 1u << 26;
