@@ -39,6 +39,21 @@ template <> __device__ __forceinline__ float2 ctw<32>(int k) { return c_tw32[k &
 template <> __device__ __forceinline__ float2 ctw<48>(int k) { return c_tw48[k % 48]; }
 template <> __device__ __forceinline__ float2 ctw<64>(int k) { return c_tw64[k & 63]; }
 
+// Tangent-form twiddles (m, t) of c_twtN (see gen_twiddles.py): w = m (1 + i t) when the angle is
+// within 45 degrees of the real axis, w = m (t + i) otherwise.
+template <int N> __device__ __forceinline__ float2 ctwt(int k);
+template <> __device__ __forceinline__ float2 ctwt<2>(int) { return make_float2(0.f, 0.f); } // all trivial
+template <> __device__ __forceinline__ float2 ctwt<4>(int k) { return c_twt4[k & 3]; }        // all trivial
+template <> __device__ __forceinline__ float2 ctwt<8>(int k) { return c_twt8[k & 7]; }
+template <> __device__ __forceinline__ float2 ctwt<16>(int k) { return c_twt16[k & 15]; }
+template <> __device__ __forceinline__ float2 ctwt<24>(int k) { return c_twt24[k % 24]; }
+template <> __device__ __forceinline__ float2 ctwt<32>(int k) { return c_twt32[k & 31]; }
+template <> __device__ __forceinline__ float2 ctwt<48>(int k) { return c_twt48[k % 48]; }
+template <> __device__ __forceinline__ float2 ctwt<64>(int k) { return c_twt64[k & 63]; }
+__host__ __device__ constexpr bool tw_near_real(int k, int n) {
+  return 8 * (k % (n / 2)) <= n || 8 * (k % (n / 2)) >= 3 * n;
+}
+
 // b * exp(-+2 pi i k/N) with the trivial angles handled without a multiply.
 template <int N, bool INV> __device__ __forceinline__ float2 twmul_c(float2 b, int k) {
   k %= N;
@@ -54,6 +69,29 @@ template <int N, bool INV> __device__ __forceinline__ float2 twmul_c(float2 b, i
   if (INV)
     w.y = -w.y;
   return cmul(b, w);
+}
+
+// Radix-2 butterfly (a, b) <- (a + w b, a - w b), w = exp(-+2 pi i k/N).  Trivial angles cost
+// adds only; the others six fused multiply-adds through the tangent form of w.
+template <int N, bool INV> __device__ __forceinline__ void bfly(float2 &a, float2 &b, int k) {
+  k %= N;
+  if (k == 0 || 4 * k == N || 2 * k == N || 4 * k == 3 * N) {
+    const float2 wb = twmul_c<N, INV>(b, k);
+    b               = csub(a, wb);
+    a               = cadd(a, wb);
+  } else if (tw_near_real(k, N)) { // w = m (1 + i t); the inverse uses w* = m (1 - i t)
+    const float2 mt = ctwt<N>(k);
+    const float  m = mt.x, t = INV ? -mt.y : mt.y;
+    const float  u = fmaf(-t, b.y, b.x), v = fmaf(t, b.x, b.y);
+    b              = make_float2(fmaf(-m, u, a.x), fmaf(-m, v, a.y));
+    a              = make_float2(fmaf(m, u, a.x), fmaf(m, v, a.y));
+  } else { // w = m (t + i); the inverse uses w* = (-m)(-t + i)
+    const float2 mt = ctwt<N>(k);
+    const float  m = INV ? -mt.x : mt.x, t = INV ? -mt.y : mt.y;
+    const float  u = fmaf(t, b.x, -b.y), v = fmaf(t, b.y, b.x);
+    b              = make_float2(fmaf(-m, u, a.x), fmaf(-m, v, a.y));
+    a              = make_float2(fmaf(m, u, a.x), fmaf(m, v, a.y));
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -77,12 +115,8 @@ template <int N, bool INV> __device__ __forceinline__ void dft_pow2(float2 *x) {
 #pragma unroll
     for (int k = 0; k < h; ++k) {
 #pragma unroll
-      for (int i = 0; i < N; i += m) {
-        const float2 a = x[i + k];
-        const float2 b = twmul_c<N, INV>(x[i + k + h], k * (N / m));
-        x[i + k]       = cadd(a, b);
-        x[i + k + h]   = csub(a, b);
-      }
+      for (int i = 0; i < N; i += m)
+        bfly<N, INV>(x[i + k], x[i + k + h], k * (N / m));
     }
   }
 }
@@ -147,6 +181,25 @@ struct SmemTwiddles {
   template <bool INV> __device__ __forceinline__ float2 get(int m) const {
     const int q = slot(m);
     return make_float2(c[q], INV ? -s[q] : s[q]);
+  }
+};
+
+// Shared-memory table T[k1][n2] = w_N^(k1 n2) (k1 < N1, n2 < 32, so k1 n2 < N): in the forward
+// four-step lane n2 reads T[k1][n2] for compile-time k1 -- one 64-bit load at a constant offset
+// from the lane's base, conflict-free, with no index arithmetic.
+struct TwTable {
+  float2 *t;
+  int     n; // transform length N = 32 * N1 (the table has N entries)
+  __device__ __forceinline__ void fill(int tid, int nthreads) {
+    for (int i = tid; i < n; i += nthreads) {
+      float sv, cv;
+      sincospif(-2.0f * (float)((i >> 5) * (i & 31)) / (float)n, &sv, &cv);
+      t[i] = make_float2(cv, sv);
+    }
+  }
+  template <bool INV> __device__ __forceinline__ float2 get(int k1, int n2) const {
+    const float2 w = t[k1 * 32 + n2];
+    return INV ? make_float2(w.x, -w.y) : w;
   }
 };
 
@@ -216,6 +269,29 @@ __device__ __forceinline__ void four_step_a_sw(float2 *x, int n2, const SmemTwid
     if (k1 != 0)
       v = cmul(v, tw.get<INV>((n2 * k1) % (N1 * 32)));
     xb[k1 * 32 + (n2 ^ k1)] = v;
+  }
+}
+// The same with twiddles from a TwTable.
+template <int N1, bool INV>
+__device__ __forceinline__ void four_step_a_sw(float2 *x, int n2, const TwTable &tw, float2 *xb) {
+  dft_reg<N1, INV>(x);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    float2 v = x[k1];
+    if (k1 != 0)
+      v = cmul(v, tw.get<INV>(k1, n2));
+    xb[k1 * 32 + (n2 ^ k1)] = v;
+  }
+}
+template <int N1, bool INV>
+__device__ __forceinline__ void four_step_a(float2 *x, int n2, const TwTable &tw, float2 *xb) {
+  dft_reg<N1, INV>(x);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    float2 v = x[k1];
+    if (k1 != 0)
+      v = cmul(v, tw.get<INV>(k1, n2));
+    xb[k1 * XBuf<N1>::kRow + n2] = v;
   }
 }
 template <int N1, bool INV>

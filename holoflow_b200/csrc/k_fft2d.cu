@@ -45,14 +45,13 @@ __device__ __forceinline__ void row_load(const RowPass &a, int w, int64_t row, i
   }
 }
 
-// Row pass: one warp per row, grid-stride over the rows of every plane of a window.  The next
-// row's loads are issued before the current row is transformed (register double buffer), so
-// each warp keeps one row of HBM traffic in flight while it computes.
+// Row pass: one warp per row, grid-stride over the rows of every plane of a window.  Each lane
+// loads its 32-stride samples of the row, so a warp load instruction reads 256 contiguous bytes.
 template <int N1, bool INV> __global__ void __launch_bounds__(256) row_pass_kernel(RowPass a) {
   constexpr int N = N1 * 32;
   extern __shared__ __align__(16) float smf[];
-  SmemTwiddles tw{smf, smf + N, N};
-  float2      *xball = reinterpret_cast<float2 *>(smf + 2 * N);
+  TwTable tw{reinterpret_cast<float2 *>(smf), N};
+  float2 *xball = reinterpret_cast<float2 *>(smf + 2 * N);
   tw.fill(threadIdx.x, blockDim.x);
   __syncthreads();
 
@@ -61,17 +60,9 @@ template <int N1, bool INV> __global__ void __launch_bounds__(256) row_pass_kern
   const int w    = blockIdx.y;
   const int64_t nrows  = (int64_t)a.nplanes * a.H;
   const int64_t stride = (int64_t)gridDim.x * nwarps;
-  int64_t row = (int64_t)blockIdx.x * nwarps + warp;
-  float2  nxt[N1];
-  if (row < nrows)
-    row_load<N1>(a, w, row, lane, nxt);
-  for (; row < nrows; row += stride) {
+  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows; row += stride) {
     float2 x[N1];
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1)
-      x[n1] = nxt[n1];
-    if (row + stride < nrows)
-      row_load<N1>(a, w, row + stride, lane, nxt);
+    row_load<N1>(a, w, row, lane, x);
     const int plane = (int)(row / a.H), r = (int)(row % a.H);
     float2   *orow  = a.out + w * a.out_win + plane * a.out_plane + r * a.out_row;
     four_step_a<N1, INV>(x, lane, tw, xb);

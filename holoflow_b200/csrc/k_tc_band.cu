@@ -98,12 +98,13 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
   uint8_t *sA   = smem;                                  // NTILE x 16 KB
   uint8_t *sB   = sA + NTILE * kTileBytes;               // 64 rows x 128 B
   float2  *gbuf = reinterpret_cast<float2 *>(sB + 8192); // 8 bins x W
-  float   *twc  = reinterpret_cast<float *>(gbuf + 8 * W);
-  float   *colsum = twc + 2 * W;                          // [2][64], indexed by row parity
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(colsum + 128); // [0] full, [1] free
+  float2  *twt  = gbuf + 8 * W;                          // [N1][32] twiddles w_W^(k1 n2)
+  float   *colsum = reinterpret_cast<float *>(twt + W);   // [2][64], indexed by window parity
+  int64_t *foff = reinterpret_cast<int64_t *>(colsum + 128); // [64] frame offsets of the window
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(foff + 64); // [0] full, [1] free
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
   int      *abort_flag = reinterpret_cast<int *>(tslot + 1);
-  SmemTwiddles tw{twc, twc + W, W};
+  TwTable   tw{twt, W};
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
@@ -125,13 +126,21 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
 
   if (tid < kLoaders) {
     // ------------------------------------------------------------------ loader / MMA warps
-    int k = 0;
+    int k = 0, cur_w = -1, wpar = 1;
     for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x, ++k) {
       const int w = (int)(row / a.H), r = (int)(row % a.H);
       if (k > 0) // MMAs of the previous row done: A and B may be overwritten
         wait_or_abort(&mbar[0], (uint32_t)((k - 1) & 1), abortv, a.status, 11);
+      const bool new_w = w != cur_w;
+      if (new_w) { // per window: frame offsets, B = W16 and its DC correction
+        cur_w = w;
+        wpar ^= 1;
+        if (tid < 64)
+          foff[tid] = (a.ring.frame(w, tid) - a.ring.base);
+      }
       // B (K-major, 128-byte swizzle): row n = 2*bin + {re, im}, K = frame t
       const float2 *wm = a.wmat + (int64_t)w * a.wmat_stride;
+      if (new_w)
       for (int e = tid; e < 64 * 8; e += kLoaders) {
         const int n = e >> 3, c = e & 7; // one 16-byte chunk = 8 frames
         __half hv[8];
@@ -147,6 +156,8 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
         }
         *reinterpret_cast<uint4 *>(sB + n * 128 + ((c ^ (n & 7)) << 4)) = *reinterpret_cast<const uint4 *>(hv);
       }
+      if (new_w)
+        named_bar(1, kLoaders); // frame offsets visible to every loader
       // A: tile j = pixels [128 j, 128 j + 128) of row r; element (m, t) at
       //    (m/64)*8192 + (t/8)*1024 + (t%8)*128 + ((m%64/8) ^ (t%8))*16 + (m%8)*2.
       //    Loads of two tiles are issued before any of them is unpacked.
@@ -158,7 +169,7 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
           const int t = item >> 2, grp = item & 3;
           const int64_t px0 = (int64_t)r * W + 128 * j + 32 * grp;
           if (j < NTILE)
-            GroupLoad<FMT>::load(a.ring.frame(w, t) + px0 * GroupLoad<FMT>::kBytes / 32, v[u]);
+            GroupLoad<FMT>::load(a.ring.base + foff[t] + px0 * GroupLoad<FMT>::kBytes / 32, v[u]);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -180,15 +191,15 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
           }
         }
       }
-      named_bar(1, kLoaders); // B complete
-      if (tid < 64) {         // DC correction of the shifted samples: shift * sum_t W16[t][n]
+      named_bar(1, kLoaders); // A (and B) complete
+      if (new_w && tid < 64) { // DC correction of the shifted samples: shift * sum_t W16[t][n]
         float sacc = 0.f;
         for (int t = 0; t < 64; ++t) {
           const int    c  = t >> 3;
           const __half hv = *reinterpret_cast<const __half *>(sB + tid * 128 + ((c ^ (tid & 7)) << 4) + (t & 7) * 2);
           sacc += __half2float(hv);
         }
-        colsum[(k & 1) * 64 + tid] = a.shift * sacc;
+        colsum[wpar * 64 + tid] = a.shift * sacc;
       }
       tc::fence_proxy_async_smem();
       named_bar(1, kLoaders);
@@ -215,9 +226,13 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
     const int q = warp & 3;          // TMEM lane quarter
     const int h = e >> 2;            // which half of the tiles this warp gathers
     constexpr int TPH = (NTILE + 1) / 2;
-    int k = 0;
+    int k = 0, cur_w = -1, wpar = 1;
     for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x, ++k) {
       const int w = (int)(row / a.H), r = (int)(row % a.H);
+      if (w != cur_w) {
+        cur_w = w;
+        wpar ^= 1;
+      }
       wait_or_abort(&mbar[0], (uint32_t)(k & 1), abortv, a.status, 13);
       tc::fence_after_sync();
       float2 L[TPH];
@@ -243,7 +258,7 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
             tc::tmem_wait_ld();
             const int p = 128 * j + 32 * q + lane;
 #pragma unroll
-            const float *cs = colsum + (k & 1) * 64 + 16 * gi;
+            const float *cs = colsum + wpar * 64 + 16 * gi;
             for (int b = 0; b < 8; ++b) {
               const float2 s = make_float2(__uint_as_float(v[2 * b]) + cs[2 * b],
                                            __uint_as_float(v[2 * b + 1]) + cs[2 * b + 1]);
@@ -292,8 +307,8 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
 template <int FMT, int N1> int launch_n1(const BandRowsArgs &a, cudaStream_t s) {
   constexpr int W     = N1 * 32;
   constexpr int NTILE = W / 128;
-  const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 8192 + (size_t)8 * W * 8 + (size_t)2 * W * 4 + 128 * 4 +
-                      16 + 8;
+  const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 8192 + (size_t)8 * W * 8 + (size_t)W * 8 + 128 * 4 +
+                      64 * 8 + 16 + 8;
   HF_CUDA(cudaFuncSetAttribute(band_rows_tc_kernel<FMT, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t nrows = (int64_t)a.nwin * a.H;
   const int     cap   = a.max_ctas > 0 ? std::min(a.max_ctas, sm_count()) : sm_count();
