@@ -10,8 +10,9 @@
 //    stages, so the next plane streams in while this one is transformed;
 //  - thread (n2, c) loads its column's samples n2 + 32 n1 from the stage, runs the N1-point DFT in
 //    registers, twiddles by w_N^(n2 k1) from a [N1][32] table (one shared load, no index math)
-//    and writes the exchange back into the same stage at (k1*32 + (n2 ^ k1)) * C + c, which is
-//    conflict-free for both the writes and the transposed reads;
+//    and writes the exchange back into the same stage at k1 * (32 C + 4) + n2 * C + c: the 4-entry
+//    pad per k1 row keeps the transposed reads conflict-free and every address is the thread's
+//    base plus a compile-time offset;
 //  - thread (k1, c) reads Y[0..31][k1], runs the 32-point DFT and accumulates |X| f^j for its 32
 //    output rows k1 + N1 k2 in registers.
 // Waits on the stage barriers are bounded: an expired wait sets the status word and every thread
@@ -46,10 +47,12 @@ __global__ void __launch_bounds__(32 * C, 1)
   constexpr int      NT       = 32 * C;
   constexpr int      kBoxRows = N < 256 ? N : 256;
   constexpr int      kBoxes   = N / kBoxRows;
-  constexpr uint32_t kStage   = (uint32_t)N * C * sizeof(float2);
+  constexpr uint32_t kStage   = (uint32_t)N * C * sizeof(float2); // bytes one plane's boxes bring
+  constexpr int      kXRow    = 32 * C + 4;                      // exchange row (one k1) in float2
+  constexpr int      kSlot    = (N1 * kXRow + 15) / 16 * 16;    // stage slot (128-byte multiple)
   extern __shared__ __align__(128) uint8_t smem[];
-  float2   *stage      = reinterpret_cast<float2 *>(smem);     // [2][N][C]
-  float2   *tw         = stage + 2 * N * C;                    // [N1][32]: w_N^(k1 * n2)
+  float2   *stage      = reinterpret_cast<float2 *>(smem);     // [2][kSlot]
+  float2   *tw         = stage + 2 * kSlot;                    // [N1][32]: w_N^(k1 * n2)
   uint64_t *mbar       = reinterpret_cast<uint64_t *>(tw + N); // [2]
   int      *abort_flag = reinterpret_cast<int *>(mbar + 2);
 
@@ -77,7 +80,7 @@ __global__ void __launch_bounds__(32 * C, 1)
     tc::mbar_arrive_expect_tx(&mbar[s], kStage);
 #pragma unroll
     for (int b = 0; b < kBoxes; ++b)
-      tc::tma_load_2d(stage + (size_t)s * N * C + (size_t)b * kBoxRows * C, &tmap, strip * C * 2,
+      tc::tma_load_2d(stage + (size_t)s * kSlot + (size_t)b * kBoxRows * C, &tmap, strip * C * 2,
                       (int)(row_base + (int64_t)plane * N + b * kBoxRows), &mbar[s]);
   };
   if (tid == 0) {
@@ -94,7 +97,7 @@ __global__ void __launch_bounds__(32 * C, 1)
 
   for (int plane = 0; plane < a.nz; ++plane) {
     const int s  = plane & 1;
-    float2   *st = stage + (size_t)s * N * C;
+    float2   *st = stage + (size_t)s * kSlot;
     const bool ok = wait_stage(&mbar[s], (uint32_t)((plane >> 1) & 1), abortv, a.status);
     float2     x[N1];
 #pragma unroll
@@ -108,14 +111,14 @@ __global__ void __launch_bounds__(32 * C, 1)
       float2 v = x[k];
       if (k != 0)
         v = cmul(v, tw[k * 32 + n2]);
-      st[(k * 32 + (n2 ^ k)) * C + c] = v;
+      st[k * kXRow + n2 * C + c] = v;
     }
     __syncthreads();
     if (k1 < N1) {
       float2 y[32];
 #pragma unroll
       for (int j = 0; j < 32; ++j)
-        y[j] = st[(k1 * 32 + (j ^ k1)) * C + c];
+        y[j] = st[k1 * kXRow + j * C + c];
       dft_reg<32, false>(y);
       const float f1 = m.w1[plane], f2 = m.w2[plane];
 #pragma unroll
@@ -156,7 +159,8 @@ __global__ void __launch_bounds__(32 * C, 1)
 template <int N1> int launch_n1(const CUtensorMap &tmap, const ColMomArgs &a, const MomentSpec &m, int nwin,
                                 cudaStream_t s) {
   constexpr int N    = N1 * 32;
-  const size_t  smem = (size_t)2 * N * kColC * sizeof(float2) + (size_t)N * sizeof(float2) + 32;
+  const size_t  slot = (size_t)(N1 * (32 * kColC + 4) + 15) / 16 * 16;
+  const size_t  smem = 2 * slot * sizeof(float2) + (size_t)N * sizeof(float2) + 32;
   auto          kern = col_moments_tma_kernel<N1, kColC>;
   HF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const dim3 grid((unsigned)((a.W + kColC - 1) / kColC), (unsigned)nwin);

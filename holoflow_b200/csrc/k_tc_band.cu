@@ -97,8 +97,9 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t *sA   = smem;                                  // NTILE x 16 KB
   uint8_t *sB   = sA + NTILE * kTileBytes;               // 64 rows x 128 B
-  float2  *gbuf = reinterpret_cast<float2 *>(sB + 8192); // 8 bins x W
-  float2  *twt  = gbuf + 8 * W;                          // [N1][32] twiddles w_W^(k1 n2)
+  constexpr int RS = XBuf<N1>::kSize > W ? XBuf<N1>::kSize : W; // gbuf row stride (room for the exchange)
+  float2  *gbuf = reinterpret_cast<float2 *>(sB + 8192); // 8 bins x RS
+  float2  *twt  = gbuf + 8 * RS;                         // [N1][32] twiddles w_W^(k1 n2)
   float   *colsum = reinterpret_cast<float *>(twt + W);   // [2][64], indexed by window parity
   int64_t *foff = reinterpret_cast<int64_t *>(colsum + 128); // [64] frame offsets of the window
   uint64_t *mbar = reinterpret_cast<uint64_t *>(foff + 64); // [0] full, [1] free
@@ -222,10 +223,17 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
     }
   } else {
     // ------------------------------------------------------------------ epilogue warps
-    const int e = warp - 4;          // 0..7
-    const int q = warp & 3;          // TMEM lane quarter
-    const int h = e >> 2;            // which half of the tiles this warp gathers
-    constexpr int TPH = (NTILE + 1) / 2;
+    // Two teams of four warps; warp q of a team reads TMEM lane quarter q.  A team takes a group
+    // of 4 bins (8 TMEM columns per tile), reads it for every tile with one wait, writes the bins'
+    // rows (DC-corrected, times the lens) to its half of gbuf and then each of its warps
+    // transforms one bin row.  The teams take alternate groups, starting with the other team on
+    // every other row, so readout and transforms of the two teams overlap and balance out.
+    const int e    = warp - 4;   // 0..7
+    const int q    = warp & 3;   // TMEM lane quarter
+    const int team = e >> 2;
+    float2   *tbuf = gbuf + team * 4 * RS;
+    const int bar  = 2 + team;
+    const int ngrp = (a.nz + 3) / 4;
     int k = 0, cur_w = -1, wpar = 1;
     for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x, ++k) {
       const int w = (int)(row / a.H), r = (int)(row % a.H);
@@ -235,64 +243,60 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
       }
       wait_or_abort(&mbar[0], (uint32_t)(k & 1), abortv, a.status, 13);
       tc::fence_after_sync();
-      float2 L[TPH];
-#pragma unroll
-      for (int jj = 0; jj < TPH; ++jj) {
-        const int j = h * TPH + jj;
-        const int p = 128 * j + 32 * q + lane;
-        L[jj] = (a.lens != nullptr && j < NTILE) ? __ldg(a.lens + (int64_t)r * W + p) : make_float2(1.f, 0.f);
+      const int g0 = (team + k) & 1;
+      if (g0 >= ngrp) { // nothing for this team on this row: TMEM is released at once
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0)
+          mbar_arrive(&mbar[1]);
+        continue;
       }
-      const int ngrp = (a.nz + 7) / 8;
-      for (int gi = 0; gi < ngrp; ++gi) {
+      float2 L[NTILE];
 #pragma unroll
-        for (int jj = 0; jj < TPH; ++jj) {
-          const int j = h * TPH + jj;
-          if (j < NTILE) {
-            uint32_t v[16];
-            const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + 64 * j + 16 * gi;
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-                           "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                         : "r"(ta));
-            tc::tmem_wait_ld();
-            const int p = 128 * j + 32 * q + lane;
+      for (int j = 0; j < NTILE; ++j)
+        L[j] = a.lens != nullptr ? __ldg(a.lens + (int64_t)r * W + 128 * j + 32 * q + lane) : make_float2(1.f, 0.f);
+      const float *cs = colsum + wpar * 64;
+      for (int g = g0; g < ngrp; g += 2) {
+        uint32_t v[NTILE][8];
 #pragma unroll
-            const float *cs = colsum + wpar * 64 + 16 * gi;
-            for (int b = 0; b < 8; ++b) {
-              const float2 s = make_float2(__uint_as_float(v[2 * b]) + cs[2 * b],
-                                           __uint_as_float(v[2 * b + 1]) + cs[2 * b + 1]);
-              gbuf[b * W + p] = cmul(s, L[jj]);
-            }
-          }
-        }
-        if (gi == ngrp - 1) { // TMEM fully read for this row: release it to the MMA issuer
+        for (int j = 0; j < NTILE; ++j)
+          tc::tmem_ld8(tbase + ((uint32_t)(32 * q) << 16) + 64 * j + 8 * g, v[j]);
+        tc::tmem_wait_ld();
+        if (g + 2 >= ngrp) { // this warp's last TMEM read of the row
           tc::fence_before_sync();
           __syncwarp();
           if (lane == 0)
             mbar_arrive(&mbar[1]);
         }
-        named_bar(2, kEpilogue);
-        const int bin = 8 * gi + e;
+#pragma unroll
+        for (int j = 0; j < NTILE; ++j)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const float2 sv = make_float2(__uint_as_float(v[j][2 * b]) + cs[8 * g + 2 * b],
+                                          __uint_as_float(v[j][2 * b + 1]) + cs[8 * g + 2 * b + 1]);
+            tbuf[b * RS + 128 * j + 32 * q + lane] = cmul(sv, L[j]);
+          }
+        named_bar(bar, 128);
+        const int bin = 4 * g + q;
         if (bin < a.nz) {
-          float2 *buf = gbuf + e * W;
+          float2 *buf = tbuf + q * RS;
           float2  x[N1];
 #pragma unroll
           for (int n1 = 0; n1 < N1; ++n1)
             x[n1] = buf[lane + 32 * n1];
-          __syncwarp();
-          four_step_a_sw<N1, false>(x, lane, tw, buf);
+          __syncwarp(); // the row is in registers: its buffer becomes the padded exchange
+          four_step_a<N1, false>(x, lane, tw, buf);
           __syncwarp();
           float2 *orow = a.out + (int64_t)w * a.out_win + (int64_t)bin * a.out_plane + (int64_t)r * a.out_row;
           for (int k1 = lane; k1 < N1; k1 += 32) {
             float2 y[32];
-            four_step_b_sw<N1, false>(y, k1, buf);
+            four_step_b<N1, false>(y, k1, buf);
 #pragma unroll
             for (int k2 = 0; k2 < 32; ++k2)
               orow[k1 + N1 * k2] = y[k2];
           }
         }
-        named_bar(2, kEpilogue);
+        named_bar(bar, 128);
       }
     }
   }
@@ -307,7 +311,8 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
 template <int FMT, int N1> int launch_n1(const BandRowsArgs &a, cudaStream_t s) {
   constexpr int W     = N1 * 32;
   constexpr int NTILE = W / 128;
-  const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 8192 + (size_t)8 * W * 8 + (size_t)W * 8 + 128 * 4 +
+  constexpr int RS    = XBuf<N1>::kSize > W ? XBuf<N1>::kSize : W;
+  const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 8192 + (size_t)8 * RS * 8 + (size_t)W * 8 + 128 * 4 +
                       64 * 8 + 16 + 8;
   HF_CUDA(cudaFuncSetAttribute(band_rows_tc_kernel<FMT, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t nrows = (int64_t)a.nwin * a.H;
