@@ -51,7 +51,9 @@ def main(out: pathlib.Path) -> None:
             else:
                 tvals.append("{%s, %s}" % (fmt(s), fmt(c / s)))
         lines.append("static __constant__ float2 c_twt%d[%d] = {%s};" % (n, n, ", ".join(tvals)))
-    out.write_text("\n".join(lines) + "\n")
+    text = "\n".join(lines) + "\n"
+    if not out.exists() or out.read_text() != text:  # keep the mtime (and the build) when unchanged
+        out.write_text(text)
 
 
 if __name__ == "__main__":
