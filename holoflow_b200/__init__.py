@@ -46,6 +46,12 @@ class HfDesc(C.Structure):
 
 _vp, _i32, _i64, _f32, _sz = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_size_t
 
+
+class HfTDesc(C.Structure):
+    """hf_tdesc: holoflow::core::TDesc across the C ABI (strides in bytes, zero = contiguous)."""
+    _fields_ = [("rank", C.c_int32), ("dtype", C.c_int32), ("mem_loc", C.c_int32), ("reserved", C.c_int32),
+                ("shape", C.c_int64 * 8), ("strides", C.c_int64 * 8), ("offset", C.c_int64)]
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "hf_last_error": (C.c_char_p, []),
@@ -90,6 +96,14 @@ _PROTOS = {
     "hf_stream_ready": (_i64, [_vp]),
     "hf_stream_process": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.POINTER(C.c_int), _vp]),
     "hf_stream_output_wait": (C.c_int, [_vp, _vp, C.c_int]),
+    "hf_node_kinds": (C.c_int, [C.c_char_p, _sz]),
+    "hf_node_infer": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(HfTDesc), C.POINTER(C.c_int),
+                                C.POINTER(HfTDesc), C.c_int]),
+    "hf_node_create": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(HfTDesc), _vp, C.POINTER(_vp)]),
+    "hf_node_update": (C.c_int, [_vp, C.c_char_p, C.c_int, C.POINTER(HfTDesc), _vp]),
+    "hf_node_execute": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_int)]),
+    "hf_node_output_desc": (C.c_int, [_vp, C.c_int, C.POINTER(HfTDesc)]),
+    "hf_node_destroy": (C.c_int, [_vp]),
     "hf_plan_stage_times": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
 }

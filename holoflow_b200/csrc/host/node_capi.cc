@@ -1,0 +1,185 @@
+// C ABI over the node layer: create / update / execute the path's compute nodes by kind string and
+// JSON settings, the way Holoflow's compiler drives ISyncTaskFactory (infer -> create/update ->
+// execute, compiler.cc:436-476, 961-1103) and its tests drive run_sync_factory
+// (sync_task_runner.cc:84-96).  Exceptions become statuses: std::invalid_argument and JSON errors
+// HF_ERR_INVALID, a CUDA failure HF_ERR_CUDA; the message is in hf_last_error().
+#include <cstring>
+
+#include "hf_common.cuh"
+#include "holoflow_b200.h"
+#include "holoflow_b200/nodes.hh"
+
+using namespace hfb;
+
+struct hf_node {
+  std::string                       kind;
+  const core::ISyncTaskFactory     *factory = nullptr;
+  std::unique_ptr<core::ISyncTask>  task;
+  std::vector<core::TDesc>          in_descs, out_descs;
+};
+
+namespace {
+
+core::TDesc to_desc(const hf_tdesc &t) {
+  if (t.rank < 0 || t.rank > HF_TDESC_MAX_RANK)
+    throw std::invalid_argument("hf_tdesc: rank must be in [0, 8]");
+  if (t.dtype < 0 || t.dtype > 3)
+    throw std::invalid_argument("hf_tdesc: dtype must be HF_U8, HF_U16, HF_F32 or HF_CF32");
+  std::vector<size_t> shape(t.shape, t.shape + t.rank), strides;
+  bool                given = false;
+  for (int i = 0; i < t.rank; ++i)
+    given |= t.strides[i] != 0;
+  if (given)
+    strides.assign(t.strides, t.strides + t.rank);
+  return core::TDesc(std::move(shape), static_cast<core::DType>(t.dtype),
+                     t.mem_loc ? core::MemLoc::Device : core::MemLoc::Host, std::move(strides), (size_t)t.offset);
+}
+
+hf_tdesc from_desc(const core::TDesc &d) {
+  hf_tdesc t{};
+  t.rank    = (int32_t)d.rank();
+  t.dtype   = (int32_t)d.dtype;
+  t.mem_loc = d.mem_loc == core::MemLoc::Device ? 1 : 0;
+  for (size_t i = 0; i < d.rank() && i < HF_TDESC_MAX_RANK; ++i) {
+    t.shape[i]   = (int64_t)d.shape[i];
+    t.strides[i] = (int64_t)d.strides[i];
+  }
+  t.offset = (int64_t)d.offset;
+  return t;
+}
+
+std::vector<core::TDesc> to_descs(int n, const hf_tdesc *in) {
+  if (n < 0 || (n > 0 && in == nullptr))
+    throw std::invalid_argument("input descriptors: bad count or null pointer");
+  std::vector<core::TDesc> v;
+  for (int i = 0; i < n; ++i)
+    v.push_back(to_desc(in[i]));
+  return v;
+}
+
+nlohmann::json parse(const char *json) {
+  return json && *json ? nlohmann::json::parse(json) : nlohmann::json::object();
+}
+
+template <class F> int guarded(F &&f) {
+  hf::clear_error();
+  try {
+    return f();
+  } catch (const core::CudaError &e) {
+    return hf::fail(HF_ERR_CUDA, e.what());
+  } catch (const std::invalid_argument &e) {
+    return hf::fail(HF_ERR_INVALID, e.what());
+  } catch (const std::out_of_range &e) {
+    return hf::fail(HF_ERR_INVALID, e.what());
+  } catch (const nlohmann::json::exception &e) {
+    return hf::fail(HF_ERR_INVALID, std::string("settings: ") + e.what());
+  } catch (const std::exception &e) {
+    return hf::fail(HF_ERR_STATE, e.what());
+  }
+}
+
+} // namespace
+
+extern "C" {
+
+int hf_node_kinds(char *buf, size_t cap) {
+  return guarded([&]() -> int {
+    std::string s;
+    for (const auto &k : nodes::default_registry().kinds())
+      s += (s.empty() ? "" : ",") + k;
+    HF_CHECK_ARG(buf != nullptr && cap > s.size(), "hf_node_kinds: buffer too small");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return HF_OK;
+  });
+}
+
+int hf_node_infer(const char *kind, const char *json, int n_in, const hf_tdesc *in, int *n_out, hf_tdesc *out,
+                  int out_cap) {
+  return guarded([&]() -> int {
+    HF_CHECK_ARG(kind != nullptr && n_out != nullptr, "hf_node_infer: null argument");
+    const auto &f     = nodes::default_registry().get_sync(kind);
+    const auto  descs = to_descs(n_in, in);
+    const auto  r     = f.infer(descs, parse(json));
+    *n_out            = (int)r.output_descs.size();
+    HF_CHECK_ARG(out != nullptr && out_cap >= *n_out, "hf_node_infer: output descriptor array too small");
+    for (int i = 0; i < *n_out; ++i)
+      out[i] = from_desc(r.output_descs[i]);
+    return HF_OK;
+  });
+}
+
+int hf_node_create(const char *kind, const char *json, int n_in, const hf_tdesc *in, hf_stream_t s, hf_node **node) {
+  return guarded([&]() -> int {
+    HF_CHECK_ARG(kind != nullptr && node != nullptr, "hf_node_create: null argument");
+    *node        = nullptr;
+    auto n       = std::make_unique<hf_node>();
+    n->kind      = kind;
+    n->factory   = &nodes::default_registry().get_sync(kind);
+    n->in_descs  = to_descs(n_in, in);
+    const auto j = parse(json);
+    n->out_descs = n->factory->infer(n->in_descs, j).output_descs;
+    n->task      = n->factory->create(n->in_descs, j, core::SyncCreateCtx{reinterpret_cast<cudaStream_t>(s)});
+    *node        = n.release();
+    return HF_OK;
+  });
+}
+
+int hf_node_update(hf_node *node, const char *json, int n_in, const hf_tdesc *in, hf_stream_t s) {
+  return guarded([&]() -> int {
+    HF_CHECK_ARG(node != nullptr && node->task != nullptr, "hf_node_update: node was not created");
+    const auto descs = to_descs(n_in, in);
+    const auto j     = parse(json);
+    auto       out   = node->factory->infer(descs, j).output_descs;
+    node->task       = node->factory->update(std::move(node->task), descs, j,
+                                             core::SyncCreateCtx{reinterpret_cast<cudaStream_t>(s)});
+    node->in_descs   = descs;
+    node->out_descs  = std::move(out);
+    return HF_OK;
+  });
+}
+
+int hf_node_execute(hf_node *node, void *const *inputs, void *const *outputs, int *op_result) {
+  return guarded([&]() -> int {
+    HF_CHECK_ARG(node != nullptr && node->task != nullptr, "hf_node_execute: node was not created");
+    HF_CHECK_ARG((node->in_descs.empty() || inputs != nullptr) && (node->out_descs.empty() || outputs != nullptr),
+                 "hf_node_execute: null tensor array");
+    std::vector<core::Storage> st(node->in_descs.size() + node->out_descs.size());
+    std::vector<core::TView>   iv(node->in_descs.size()), ov(node->out_descs.size());
+    for (size_t i = 0; i < iv.size(); ++i) {
+      HF_CHECK_ARG(inputs[i] != nullptr, "hf_node_execute: null input pointer");
+      st[i] = core::Storage{node->in_descs[i].mem_loc, node->in_descs[i].num_bytes(), static_cast<std::byte *>(inputs[i])};
+      iv[i] = core::TView{node->in_descs[i], &st[i]};
+      iv[i].desc.offset = 0; // the pointer given is the tensor's origin
+    }
+    for (size_t i = 0; i < ov.size(); ++i) {
+      HF_CHECK_ARG(outputs[i] != nullptr, "hf_node_execute: null output pointer");
+      auto &s = st[iv.size() + i];
+      s       = core::Storage{node->out_descs[i].mem_loc, node->out_descs[i].num_bytes(), static_cast<std::byte *>(outputs[i])};
+      ov[i]   = core::TView{node->out_descs[i], &s};
+      ov[i].desc.offset = 0;
+    }
+    std::atomic<bool> cancelled{false};
+    core::SyncCtx     ctx{std::span<core::TView>(iv), std::span<core::TView>(ov), &cancelled};
+    const auto        r = node->task->execute(ctx);
+    if (op_result)
+      *op_result = (int)r;
+    return HF_OK;
+  });
+}
+
+int hf_node_output_desc(const hf_node *node, int i, hf_tdesc *out) {
+  hf::clear_error();
+  HF_CHECK_ARG(node != nullptr && out != nullptr && i >= 0 && i < (int)node->out_descs.size(),
+               "hf_node_output_desc: bad argument");
+  *out = from_desc(node->out_descs[i]);
+  return HF_OK;
+}
+
+int hf_node_destroy(hf_node *node) {
+  return guarded([&]() -> int {
+    delete node;
+    return HF_OK;
+  });
+}
+
+} // extern "C"

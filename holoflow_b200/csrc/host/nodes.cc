@@ -1,0 +1,898 @@
+// The Doppler path's compute nodes (hfb::nodes) over the C ABI.  Every factory mirrors the
+// reference node named in its comment: settings keys, inference checks and messages, output
+// descriptors, in-place and ownership declarations; execution goes through the hf_* entry points
+// on the task's stream.
+#include "holoflow_b200/nodes.hh"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "holoflow_b200.h"
+
+namespace hfb::nodes {
+
+using core::DType;
+using core::MemLoc;
+using core::OpResult;
+using core::SyncCtx;
+
+// ================================================================================================
+// settings
+// ================================================================================================
+void from_json(const nlohmann::json &j, FresnelDiffractionSettings &s) {
+  j.at("lambda").get_to(s.lambda);
+  j.at("dx").get_to(s.dx);
+  j.at("dy").get_to(s.dy);
+  j.at("z").get_to(s.z);
+  s.axes = {-2, -1};
+  if (j.contains("axes"))
+    j.at("axes").get_to(s.axes);
+  if (j.contains("skip_phase_shift"))
+    j.at("skip_phase_shift").get_to(s.skip_phase_shift);
+  if (j.contains("output_magnitude"))
+    j.at("output_magnitude").get_to(s.output_magnitude);
+}
+void from_json(const nlohmann::json &j, AngularSpectrumFilter &f) {
+  j.at("r_inner").get_to(f.r_inner);
+  j.at("r_outer").get_to(f.r_outer);
+  j.at("s_inner").get_to(f.s_inner);
+  j.at("s_outer").get_to(f.s_outer);
+}
+void from_json(const nlohmann::json &j, AngularSpectrumPadding &p) {
+  j.at("width").get_to(p.width);
+  j.at("height").get_to(p.height);
+}
+void from_json(const nlohmann::json &j, AngularSpectrumSettings &s) {
+  j.at("lambda").get_to(s.lambda);
+  j.at("dx").get_to(s.dx);
+  j.at("dy").get_to(s.dy);
+  j.at("z").get_to(s.z);
+  if (j.contains("filter"))
+    s.filter = j.at("filter").get<AngularSpectrumFilter>();
+  if (j.contains("padding"))
+    s.padding = j.at("padding").get<AngularSpectrumPadding>();
+}
+void from_json(const nlohmann::json &j, PcaSettings &s) {
+  j.at("begin").get_to(s.begin);
+  j.at("end").get_to(s.end);
+}
+void from_json(const nlohmann::json &j, FftNorm &n) {
+  if (j.is_null()) {
+    n = FftNorm::Backward;
+    return;
+  }
+  const auto s = j.get<std::string>();
+  if (s == "backward" || s == "none")
+    n = FftNorm::Backward;
+  else if (s == "forward")
+    n = FftNorm::Forward;
+  else if (s == "ortho")
+    n = FftNorm::Ortho;
+  else
+    throw std::invalid_argument("FftNorm: unsupported norm '" + s + "'");
+}
+void from_json(const nlohmann::json &j, FFTSettings &s) {
+  s.axis = j.contains("axis") ? j.at("axis").get<int>() : -1;
+  s.norm = j.contains("norm") ? j.at("norm").get<FftNorm>() : FftNorm::Backward;
+}
+void from_json(const nlohmann::json &j, MeanSettings &s) {
+  s.axis.clear();
+  for (const char *key : {"axis", "axes"}) {
+    if (!j.contains(key))
+      continue;
+    const auto &ja = j.at(key);
+    if (ja.is_null())
+      s.axis.clear();
+    else if (ja.is_number_integer())
+      s.axis = {ja.get<int>()};
+    else if (ja.is_array())
+      ja.get_to(s.axis);
+    else
+      throw std::invalid_argument(std::string("MeanSettings: ") + key + " must be int, array, or null");
+    break;
+  }
+  s.keepdims = j.contains("keepdims") ? j.at("keepdims").get<bool>() : false;
+}
+void from_json(const nlohmann::json &j, ConversionSettings &s) {
+  const auto t = j.at("target").get<std::string>();
+  if (t == "U8")
+    s.target = ConversionSettings::Target::U8;
+  else if (t == "U16")
+    s.target = ConversionSettings::Target::U16;
+  else if (t == "F32")
+    s.target = ConversionSettings::Target::F32;
+  else if (t == "CF32")
+    s.target = ConversionSettings::Target::CF32;
+  else
+    throw std::invalid_argument("Unknown target type for conversion: " + t);
+  const auto st = j.at("strategy").get<std::string>();
+  if (st == "Real")
+    s.strategy = ConversionSettings::Strategy::Real;
+  else if (st == "Scaled")
+    s.strategy = ConversionSettings::Strategy::Scaled;
+  else if (st == "Modulus")
+    s.strategy = ConversionSettings::Strategy::Modulus;
+  else if (st == "Argument")
+    s.strategy = ConversionSettings::Strategy::Argument;
+  else
+    throw std::invalid_argument("Unknown strategy type for conversion: " + st);
+}
+void from_json(const nlohmann::json &j, DopplerMomentsSettings &s) {
+  j.at("time_z_begin").get_to(s.time_z_begin);
+  j.at("time_z_end").get_to(s.time_z_end);
+  auto opt = [&](const char *k, auto &v) {
+    if (j.contains(k))
+      j.at(k).get_to(v);
+  };
+  opt("clutter_rank", s.clutter_rank);
+  opt("propagation", s.propagation);
+  opt("input_format", s.input_format);
+  opt("height", s.height);
+  opt("width", s.width);
+  opt("lambda", s.lambda);
+  opt("dx", s.dx);
+  opt("z", s.z);
+  opt("fs", s.fs);
+  opt("moments", s.moments);
+  opt("fftshift", s.fftshift);
+  opt("form", s.form);
+  if (j.contains("filter"))
+    s.filter = j.at("filter").get<AngularSpectrumFilter>();
+  if (j.contains("padding"))
+    s.padding = j.at("padding").get<AngularSpectrumPadding>();
+}
+
+// ================================================================================================
+// helpers
+// ================================================================================================
+namespace {
+
+struct Check {
+  const char *factory;
+  void        operator()(bool cond, const std::string &msg) const {
+    if (!cond)
+      throw std::invalid_argument(std::string(factory) + " inference error: " + msg);
+  }
+};
+
+// Maps a C-ABI status onto the reference's exception types.
+void hf_ok(int rc, const char *who) {
+  if (rc == HF_OK)
+    return;
+  const std::string msg = std::string(who) + ": " + hf_last_error();
+  if (rc == HF_ERR_INVALID || rc == HF_ERR_UNSUPPORTED)
+    throw std::invalid_argument(msg);
+  throw core::CudaError(msg);
+}
+
+int hf_dtype(DType d) {
+  switch (d) {
+  case DType::U8: return HF_U8;
+  case DType::U16: return HF_U16;
+  case DType::F32: return HF_F32;
+  case DType::CF32: return HF_CF32;
+  }
+  return -1;
+}
+
+size_t prod(const std::vector<size_t> &s, size_t b, size_t e) {
+  size_t n = 1;
+  for (size_t i = b; i < e && i < s.size(); ++i)
+    n *= s[i];
+  return n;
+}
+
+int norm_axis(int axis, size_t rank) { return axis < 0 ? axis + (int)rank : axis; }
+
+// Device buffer owned by a task.
+struct DevBuf {
+  void *p = nullptr;
+  DevBuf() = default;
+  explicit DevBuf(size_t bytes) {
+    if (bytes && cudaMalloc(&p, bytes) != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      throw core::CudaError("device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+  }
+  DevBuf(const DevBuf &)            = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p) { o.p = nullptr; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) {
+      if (p)
+        cudaFree(p);
+      p   = o.p;
+      o.p = nullptr;
+    }
+    return *this;
+  }
+  ~DevBuf() {
+    if (p)
+      cudaFree(p);
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Batch stride (bytes) over the leading dims [0, last) when they collapse into one uniform
+// stride; `ok` is false otherwise.
+size_t collapse_outer(const TDesc &d, size_t last, bool &ok) {
+  ok = true;
+  if (last == 0)
+    return d.num_bytes();
+  for (size_t i = 0; i + 1 < last; ++i)
+    if (d.strides[i] != d.strides[i + 1] * d.shape[i + 1])
+      ok = false;
+  return d.strides[last - 1];
+}
+
+InferResult sync_result(const TDesc &in, const TDesc &out, std::vector<core::InPlace> in_place = {}) {
+  InferResult r;
+  r.input_descs   = {in};
+  r.output_descs  = {out};
+  r.in_place      = std::move(in_place);
+  r.owned_inputs  = {false};
+  r.owned_outputs = {false};
+  r.kind          = core::TaskKind::Sync;
+  return r;
+}
+
+} // namespace
+
+// ================================================================================================
+// FresnelDiffraction (fresnel_diffraction.cu:466-668)
+// ================================================================================================
+namespace {
+class FresnelTask final : public ISyncTask {
+public:
+  hf_fresnel_plan           *plan = nullptr;
+  cudaStream_t               stream{};
+  FresnelDiffractionSettings s;
+  TDesc                      idesc;
+  ~FresnelTask() override {
+    if (plan)
+      hf_fresnel_plan_destroy(plan);
+  }
+  OpResult execute(SyncCtx &ctx) override {
+    auto      &in = ctx.inputs[0];
+    auto      &out = ctx.outputs[0];
+    const auto r  = in.desc.rank();
+    const auto ie = core::size_of(in.desc.dtype), oe = core::size_of(out.desc.dtype);
+    bool       ok_i, ok_o;
+    const auto ib = collapse_outer(in.desc, r - 2, ok_i), ob = collapse_outer(out.desc, r - 2, ok_o);
+    hf_ok(hf_fresnel_exec(plan, in.data(), (int64_t)(ib / ie), (int64_t)(in.desc.strides[r - 2] / ie),
+                          (int64_t)(in.desc.strides[r - 1] / ie), out.data(), (int64_t)(ob / oe),
+                          (int64_t)(out.desc.strides[r - 2] / oe), (int64_t)(out.desc.strides[r - 1] / oe), stream),
+          "FresnelDiffraction");
+    return OpResult::Ok;
+  }
+};
+} // namespace
+
+InferResult FresnelDiffractionFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"FresnelDiffractionFactory"};
+  const auto  s = j.get<FresnelDiffractionSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.rank() >= 2, "input must be a tensor of rank 2 or higher");
+  check(idesc.dtype == DType::CF32 || idesc.dtype == DType::F32, "input must be complex float32 or real float32");
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(s.axes.size() == 2, "axes must contain exactly two dimensions");
+  const int rank = (int)idesc.rank();
+  const int ax0 = norm_axis(s.axes[0], rank), ax1 = norm_axis(s.axes[1], rank);
+  check(ax0 >= 0 && ax0 < rank && ax1 >= 0 && ax1 < rank, "axes out of bounds");
+  check(ax0 != ax1, "axes must be distinct");
+  check(idesc.strides[ax0] % idesc.strides[ax1] == 0, "stride of ax0 (H) must be a multiple of stride of ax1 (W)");
+  check(s.lambda > 0.0f, "wavelength must be positive");
+  check(s.dx > 0.0f, "dx must be positive");
+  check(s.dy > 0.0f, "dy must be positive");
+  check(s.dx == s.dy, "dx must equal dy");
+  check(ax0 == rank - 2 && ax1 == rank - 1, "this implementation transforms the last two axes only");
+  bool ok;
+  collapse_outer(idesc, idesc.rank() - 2, ok);
+  check(ok, "leading dimensions must collapse into one uniformly strided batch");
+  TDesc odesc;
+  if (s.output_magnitude)
+    odesc = TDesc(idesc.shape, DType::F32, idesc.mem_loc);
+  else if (idesc.dtype == DType::CF32)
+    odesc = idesc;
+  else
+    odesc = TDesc(idesc.shape, DType::CF32, idesc.mem_loc);
+  return sync_result(idesc, odesc);
+}
+
+std::unique_ptr<ISyncTask> FresnelDiffractionFactory::create(std::span<const TDesc> input_descs,
+                                                             const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto        t = std::make_unique<FresnelTask>();
+  const auto &d = input_descs[0];
+  const auto  r = d.rank();
+  t->s          = j.get<FresnelDiffractionSettings>();
+  t->idesc      = d;
+  t->stream     = ctx.stream;
+  hf_ok(hf_fresnel_plan_create((int64_t)prod(d.shape, 0, r - 2), (int)d.shape[r - 2], (int)d.shape[r - 1],
+                               hf_dtype(d.dtype), t->s.lambda, t->s.dx, t->s.z, t->s.output_magnitude ? 1 : 0,
+                               t->s.skip_phase_shift ? 1 : 0, &t->plan, ctx.stream),
+        "FresnelDiffraction");
+  return t;
+}
+
+// Same input and settings but z: rebuild the lens only (fresnel_diffraction.cu:634-668).
+std::unique_ptr<ISyncTask> FresnelDiffractionFactory::update(std::unique_ptr<ISyncTask> old,
+                                                             std::span<const TDesc> input_descs,
+                                                             const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  auto *t = dynamic_cast<FresnelTask *>(old.get());
+  if (t && input_descs.size() == 1 && input_descs[0] == t->idesc) {
+    (void)infer(input_descs, j);
+    const auto s = j.get<FresnelDiffractionSettings>();
+    if (s.lambda == t->s.lambda && s.dx == t->s.dx && s.dy == t->s.dy && s.axes == t->s.axes &&
+        s.skip_phase_shift == t->s.skip_phase_shift && s.output_magnitude == t->s.output_magnitude) {
+      if (s.z != t->s.z)
+        hf_ok(hf_fresnel_plan_set_z(t->plan, s.z, ctx.stream), "FresnelDiffraction");
+      t->s      = s;
+      t->stream = ctx.stream;
+      return old;
+    }
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+// ================================================================================================
+// AngularSpectrum (angular_spectrum.cu:446-580)
+// ================================================================================================
+namespace {
+class AngularSpectrumTask final : public ISyncTask {
+public:
+  hf_as_plan  *plan = nullptr;
+  cudaStream_t stream{};
+  ~AngularSpectrumTask() override {
+    if (plan)
+      hf_as_plan_destroy(plan);
+  }
+  OpResult execute(SyncCtx &ctx) override {
+    hf_ok(hf_as_exec(plan, ctx.inputs[0].data(), ctx.outputs[0].data(), stream), "AngularSpectrum");
+    return OpResult::Ok;
+  }
+};
+} // namespace
+
+InferResult AngularSpectrumFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"AngularSpectrumFactory"};
+  const auto  s = j.get<AngularSpectrumSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.rank() >= 2, "input must be a tensor of rank 2 or higher");
+  check(idesc.dtype == DType::CF32 || idesc.dtype == DType::F32, "input must be complex float32 or real float32");
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(idesc.is_contiguous(), "input must be C-contiguous");
+  check(s.lambda > 0.0f, "wavelength must be positive");
+  check(s.dx > 0.0f, "dx must be positive");
+  check(s.dy > 0.0f, "dy must be positive");
+  check(s.dx == s.dy, "dx must equal dy");
+  const size_t r = idesc.rank();
+  const int    height = (int)idesc.shape[r - 2], width = (int)idesc.shape[r - 1];
+  auto         oshape = idesc.shape;
+  if (s.padding) {
+    const auto &p = *s.padding;
+    check(p.width > 0, "padding width must be positive");
+    check(p.height > 0, "padding height must be positive");
+    check(p.width >= width, "padding width must be at least the input width");
+    check(p.height >= height, "padding height must be at least the input height");
+    check((p.width - width) % 2 == 0, "horizontal padding must be even");
+    check((p.height - height) % 2 == 0, "vertical padding must be even");
+    oshape[r - 2] = (size_t)p.height;
+    oshape[r - 1] = (size_t)p.width;
+  }
+  std::vector<core::InPlace> in_place;
+  if (idesc.dtype == DType::CF32 && !s.padding)
+    in_place.push_back({0, 0});
+  return sync_result(idesc, TDesc(oshape, DType::CF32, idesc.mem_loc), std::move(in_place));
+}
+
+std::unique_ptr<ISyncTask> AngularSpectrumFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                          const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  const auto  s = j.get<AngularSpectrumSettings>();
+  const auto &d = input_descs[0];
+  const auto  r = d.rank();
+  auto        t = std::make_unique<AngularSpectrumTask>();
+  t->stream     = ctx.stream;
+  const AngularSpectrumFilter f = s.filter.value_or(AngularSpectrumFilter{});
+  hf_ok(hf_as_plan_create((int64_t)prod(d.shape, 0, r - 2), (int)d.shape[r - 2], (int)d.shape[r - 1], hf_dtype(d.dtype),
+                          s.lambda, s.dx, s.z, s.padding ? s.padding->width : 0, s.padding ? s.padding->height : 0,
+                          s.filter ? 1 : 0, f.r_inner, f.r_outer, f.s_inner, f.s_outer, &t->plan, ctx.stream),
+        "AngularSpectrum");
+  return t;
+}
+
+std::unique_ptr<ISyncTask> AngularSpectrumFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> in,
+                                                          const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(in, j, ctx);
+}
+
+// ================================================================================================
+// Pca (pca.cc:68-193): C = X^T X, ascending eigendecomposition, projection on [begin, end)
+// ================================================================================================
+namespace {
+class PcaTask final : public ISyncTask {
+public:
+  cudaStream_t stream{};
+  PcaSettings  s;
+  int64_t      batch = 0, P = 0;
+  int          F = 0;
+  DevBuf       gram, evecs, evals, info, ws;
+  OpResult     execute(SyncCtx &ctx) override {
+    const void *x = ctx.inputs[0].data();
+    hf_ok(hf_covariance(x, HF_F32, batch, F, P, gram.as<double>(), ws.p, stream), "Pca");
+    hf_ok(hf_eigh_jacobi_f64(gram.as<double>(), evecs.as<double>(), evals.as<double>(), info.as<int>(), F, batch,
+                             stream),
+          "Pca");
+    hf_ok(hf_pca_project(static_cast<const float *>(x), batch, F, P, evecs.as<double>(), s.begin, s.end,
+                         reinterpret_cast<float *>(ctx.outputs[0].data()), stream),
+          "Pca");
+    return OpResult::Ok;
+  }
+};
+} // namespace
+
+InferResult PcaFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"PcaFactory"};
+  const auto  s = j.get<PcaSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.rank() >= 3, "expected input rank >= 3");
+  check(idesc.dtype == DType::F32, "PCA supports F32 input only");
+  check(idesc.mem_loc == MemLoc::Device, "expected input in device memory");
+  check(s.begin < s.end, "expected begin < end");
+  check(s.begin >= 0, "expected begin >= 0");
+  const size_t feat = idesc.rank() - 3;
+  check(s.end <= (int)idesc.shape.at(feat), "expected end <= n_features");
+  check(idesc.is_contiguous(), "expected C-contiguous input");
+  check(idesc.shape.at(feat) <= 128, "at most 128 features");
+  auto oshape  = idesc.shape;
+  oshape[feat] = (size_t)s.components();
+  return sync_result(idesc, TDesc(oshape, idesc.dtype, idesc.mem_loc));
+}
+
+std::unique_ptr<ISyncTask> PcaFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                              const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  const auto &d    = input_descs[0];
+  const auto  r    = d.rank();
+  auto        t    = std::make_unique<PcaTask>();
+  t->stream        = ctx.stream;
+  t->s             = j.get<PcaSettings>();
+  t->batch         = (int64_t)prod(d.shape, 0, r - 3);
+  t->F             = (int)d.shape[r - 3];
+  t->P             = (int64_t)prod(d.shape, r - 2, r);
+  const size_t FF  = (size_t)t->F * t->F;
+  t->gram          = DevBuf(sizeof(double) * FF * t->batch);
+  t->evecs         = DevBuf(sizeof(double) * FF * t->batch);
+  t->evals         = DevBuf(sizeof(double) * t->F * t->batch);
+  t->info          = DevBuf(sizeof(int) * t->batch);
+  t->ws            = DevBuf(std::max<size_t>(16, hf_covariance_workspace_bytes(t->F, t->P) * (size_t)t->batch));
+  return t;
+}
+
+std::unique_ptr<ISyncTask> PcaFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> in,
+                                              const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(in, j, ctx);
+}
+
+// ================================================================================================
+// FFT / RFFT along one axis (fft.cu:234-252, rfft.cu:142-170)
+// ================================================================================================
+namespace {
+class AxisDftTask final : public ISyncTask {
+public:
+  cudaStream_t stream{};
+  int          dtype = 0, norm = 0, T = 0, bins = 0;
+  int64_t      batch = 0, P = 0;
+  OpResult     execute(SyncCtx &ctx) override {
+    hf_ok(hf_temporal_dft(ctx.inputs[0].data(), dtype, batch, T, P, 0, bins, norm, ctx.outputs[0].data(), stream),
+          "FFT");
+    return OpResult::Ok;
+  }
+};
+
+InferResult axis_dft_infer(const char *factory, bool real, std::span<const TDesc> input_descs, const nlohmann::json &j) {
+  const Check check{factory};
+  const auto  s = j.get<FFTSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.rank() >= 1, "input must have rank >= 1");
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(idesc.is_contiguous(), "input must be C-contiguous");
+  if (real)
+    check(idesc.dtype != DType::CF32, "input must be real");
+  const int ax = norm_axis(s.axis, idesc.rank());
+  check(ax >= 0 && ax < (int)idesc.rank(), "axis out of range");
+  auto oshape = idesc.shape;
+  if (real)
+    oshape[ax] = oshape[ax] / 2 + 1;
+  return sync_result(idesc, TDesc(oshape, DType::CF32, idesc.mem_loc));
+}
+
+std::unique_ptr<ISyncTask> axis_dft_create(bool real, std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                           const SyncCreateCtx &ctx) {
+  const auto  s  = j.get<FFTSettings>();
+  const auto &d  = input_descs[0];
+  const int   ax = norm_axis(s.axis, d.rank());
+  auto        t  = std::make_unique<AxisDftTask>();
+  t->stream      = ctx.stream;
+  t->dtype       = hf_dtype(d.dtype);
+  t->norm = s.norm == FftNorm::Backward ? HF_NORM_BACKWARD : (s.norm == FftNorm::Forward ? HF_NORM_FORWARD : HF_NORM_ORTHO);
+  t->batch = (int64_t)prod(d.shape, 0, (size_t)ax);
+  t->T     = (int)d.shape[ax];
+  t->P     = (int64_t)prod(d.shape, (size_t)ax + 1, d.rank());
+  t->bins  = real ? t->T / 2 + 1 : t->T;
+  return t;
+}
+} // namespace
+
+InferResult FFTFactory::infer(std::span<const TDesc> in, const nlohmann::json &j) const {
+  return axis_dft_infer("FFTFactory", false, in, j);
+}
+std::unique_ptr<ISyncTask> FFTFactory::create(std::span<const TDesc> in, const nlohmann::json &j,
+                                              const SyncCreateCtx &ctx) const {
+  (void)infer(in, j);
+  return axis_dft_create(false, in, j, ctx);
+}
+std::unique_ptr<ISyncTask> FFTFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> in,
+                                              const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(in, j, ctx);
+}
+InferResult RFFTFactory::infer(std::span<const TDesc> in, const nlohmann::json &j) const {
+  return axis_dft_infer("RFFTFactory", true, in, j);
+}
+std::unique_ptr<ISyncTask> RFFTFactory::create(std::span<const TDesc> in, const nlohmann::json &j,
+                                               const SyncCreateCtx &ctx) const {
+  (void)infer(in, j);
+  return axis_dft_create(true, in, j, ctx);
+}
+std::unique_ptr<ISyncTask> RFFTFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> in,
+                                               const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(in, j, ctx);
+}
+
+// ================================================================================================
+// Mean (mean.cu:355-400) and MeanAbs (mean_abs.cu:236-275) over one run of adjacent axes
+// ================================================================================================
+namespace {
+class MeanTask final : public ISyncTask {
+public:
+  cudaStream_t stream{};
+  bool         absolute = false;
+  int          dtype    = 0;
+  int64_t      outer = 0, n = 0, inner = 0;
+  OpResult     execute(SyncCtx &ctx) override {
+    if (absolute)
+      hf_ok(hf_mean_abs_axis(ctx.inputs[0].data(), dtype, outer, n, inner,
+                             reinterpret_cast<float *>(ctx.outputs[0].data()), stream),
+            "MeanAbs");
+    else
+      hf_ok(hf_mean_axis(ctx.inputs[0].data(), dtype, outer, n, inner, ctx.outputs[0].data(), stream), "Mean");
+    return OpResult::Ok;
+  }
+};
+
+// Reduced axes as [lo, hi) (all axes when none are given); throws when they are not adjacent.
+std::pair<size_t, size_t> reduced_run(const Check &check, const MeanSettings &s, size_t rank) {
+  if (s.axis.empty())
+    return {0, rank};
+  std::vector<int> ax;
+  for (int a : s.axis) {
+    const int n = norm_axis(a, rank);
+    check(n >= 0 && n < (int)rank, "axis out of range");
+    ax.push_back(n);
+  }
+  std::sort(ax.begin(), ax.end());
+  check(std::adjacent_find(ax.begin(), ax.end()) == ax.end(), "duplicate axis");
+  check(ax.back() - ax.front() + 1 == (int)ax.size(), "reduced axes must be adjacent in this implementation");
+  return {(size_t)ax.front(), (size_t)ax.back() + 1};
+}
+
+InferResult mean_infer(const char *factory, bool absolute, std::span<const TDesc> input_descs, const nlohmann::json &j) {
+  const Check check{factory};
+  const auto  s = j.get<MeanSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(idesc.is_contiguous(), "input must be C-contiguous");
+  if (absolute)
+    check(idesc.dtype == DType::F32 || idesc.dtype == DType::CF32, "input must be F32 or CF32");
+  const auto [lo, hi] = reduced_run(check, s, idesc.rank());
+  std::vector<size_t> oshape;
+  for (size_t i = 0; i < idesc.rank(); ++i) {
+    if (i >= lo && i < hi) {
+      if (s.keepdims)
+        oshape.push_back(1);
+    } else {
+      oshape.push_back(idesc.shape[i]);
+    }
+  }
+  const DType odt = (!absolute && idesc.dtype == DType::CF32) ? DType::CF32 : DType::F32;
+  return sync_result(idesc, TDesc(oshape, odt, idesc.mem_loc));
+}
+
+std::unique_ptr<ISyncTask> mean_create(bool absolute, std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                       const SyncCreateCtx &ctx) {
+  const auto  s = j.get<MeanSettings>();
+  const auto &d = input_descs[0];
+  const auto [lo, hi] = reduced_run(Check{absolute ? "MeanAbsFactory" : "MeanFactory"}, s, d.rank());
+  auto t      = std::make_unique<MeanTask>();
+  t->stream   = ctx.stream;
+  t->absolute = absolute;
+  t->dtype    = hf_dtype(d.dtype);
+  t->outer    = (int64_t)prod(d.shape, 0, lo);
+  t->n        = (int64_t)prod(d.shape, lo, hi);
+  t->inner    = (int64_t)prod(d.shape, hi, d.rank());
+  return t;
+}
+} // namespace
+
+InferResult MeanFactory::infer(std::span<const TDesc> in, const nlohmann::json &j) const {
+  return mean_infer("MeanFactory", false, in, j);
+}
+std::unique_ptr<ISyncTask> MeanFactory::create(std::span<const TDesc> in, const nlohmann::json &j,
+                                               const SyncCreateCtx &ctx) const {
+  (void)infer(in, j);
+  return mean_create(false, in, j, ctx);
+}
+std::unique_ptr<ISyncTask> MeanFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> in,
+                                               const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(in, j, ctx);
+}
+InferResult MeanAbsFactory::infer(std::span<const TDesc> in, const nlohmann::json &j) const {
+  return mean_infer("MeanAbsFactory", true, in, j);
+}
+std::unique_ptr<ISyncTask> MeanAbsFactory::create(std::span<const TDesc> in, const nlohmann::json &j,
+                                                  const SyncCreateCtx &ctx) const {
+  (void)infer(in, j);
+  return mean_create(true, in, j, ctx);
+}
+std::unique_ptr<ISyncTask> MeanAbsFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> in,
+                                                  const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(in, j, ctx);
+}
+
+// ================================================================================================
+// Conversion (conversion.cu:138-150 supported configurations, 389-445 infer/create)
+// ================================================================================================
+namespace {
+struct ConvCfg {
+  DType                          in;
+  ConversionSettings::Target     target;
+  ConversionSettings::Strategy   strategy;
+  DType                          out;
+};
+using CT = ConversionSettings::Target;
+using CS = ConversionSettings::Strategy;
+const ConvCfg kConv[] = {
+    {DType::U8, CT::F32, CS::Real, DType::F32},        {DType::U8, CT::CF32, CS::Real, DType::CF32},
+    {DType::U16, CT::CF32, CS::Real, DType::CF32},     {DType::F32, CT::U8, CS::Scaled, DType::U8},
+    {DType::F32, CT::U16, CS::Scaled, DType::U16},     {DType::F32, CT::CF32, CS::Real, DType::CF32},
+    {DType::CF32, CT::F32, CS::Modulus, DType::F32},   {DType::CF32, CT::F32, CS::Argument, DType::F32},
+};
+const ConvCfg *conv_cfg(DType in, const ConversionSettings &s) {
+  for (const auto &c : kConv)
+    if (c.in == in && c.target == s.target && c.strategy == s.strategy)
+      return &c;
+  return nullptr;
+}
+int hf_strategy(CS s) {
+  switch (s) {
+  case CS::Real: return HF_CONV_REAL;
+  case CS::Scaled: return HF_CONV_SCALED;
+  case CS::Modulus: return HF_CONV_MODULUS;
+  case CS::Argument: return HF_CONV_ARGUMENT;
+  }
+  return -1;
+}
+class ConversionTask final : public ISyncTask {
+public:
+  cudaStream_t stream{};
+  int          in_dt = 0, out_dt = 0, strategy = 0;
+  int64_t      n = 0;
+  DevBuf       minmax{64};
+  OpResult     execute(SyncCtx &ctx) override {
+    hf_ok(hf_convert(ctx.inputs[0].data(), in_dt, ctx.outputs[0].data(), out_dt, strategy, n, minmax.p, stream),
+          "Conversion");
+    return OpResult::Ok;
+  }
+};
+} // namespace
+
+InferResult ConversionFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"ConversionFactory"};
+  const auto  s = j.get<ConversionSettings>();
+  check(input_descs.size() == 1, "Expected exactly one input tensor");
+  const auto &idesc = input_descs[0];
+  check(idesc.mem_loc == MemLoc::Device, "Input tensor must be in device memory");
+  check(idesc.is_contiguous(), "Input tensor must be C-contiguous");
+  const ConvCfg *c = conv_cfg(idesc.dtype, s);
+  check(c != nullptr, "Unsupported conversion configuration");
+  return sync_result(idesc, TDesc(idesc.shape, c->out, MemLoc::Device));
+}
+
+std::unique_ptr<ISyncTask> ConversionFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                     const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  const auto     s = j.get<ConversionSettings>();
+  const ConvCfg *c = conv_cfg(input_descs[0].dtype, s);
+  auto           t = std::make_unique<ConversionTask>();
+  t->stream        = ctx.stream;
+  t->in_dt         = hf_dtype(c->in);
+  t->out_dt        = hf_dtype(c->out);
+  t->strategy      = hf_strategy(s.strategy);
+  t->n             = (int64_t)input_descs[0].num_elements();
+  return t;
+}
+std::unique_ptr<ISyncTask> ConversionFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> in,
+                                                     const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(in, j, ctx);
+}
+
+// ================================================================================================
+// DopplerMoments: windows [n_windows][T][H][W] (or packed [n_windows][T][3 H W / 2] bytes) ->
+// moment images [n_windows][n_moments][OH][OW] through hf_pipeline_exec
+// ================================================================================================
+namespace {
+struct DopplerPlan {
+  hf_desc d{};
+  int     nwin = 0, nmom = 0, OH = 0, OW = 0;
+};
+
+DopplerPlan doppler_plan(const Check &check, const TDesc &idesc, const DopplerMomentsSettings &s) {
+  DopplerPlan dp;
+  hf_desc    &d = dp.d;
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(idesc.is_contiguous(), "input must be C-contiguous");
+  const bool packed = s.input_format == "mono12p";
+  if (packed) {
+    check(idesc.dtype == DType::U8 && idesc.rank() == 3, "mono12p input must be U8 [n_windows][T][3 H W / 2]");
+    check(s.height > 0 && s.width > 0 && (size_t)s.height * s.width * 3 / 2 == idesc.shape[2] &&
+              ((size_t)s.height * s.width) % 2 == 0,
+          "height x width must match the packed frame size");
+    d.height = s.height, d.width = s.width, d.input_dtype = HF_MONO12P;
+  } else {
+    check(idesc.rank() == 4, "input must be [n_windows][T][H][W]");
+    const std::string want = idesc.dtype == DType::U8 ? "u8" : (idesc.dtype == DType::U16 ? "u16" : "f32");
+    check(idesc.dtype != DType::CF32 && s.input_format == want, "input_format does not match the input dtype");
+    d.height = (int)idesc.shape[2], d.width = (int)idesc.shape[3], d.input_dtype = hf_dtype(idesc.dtype);
+  }
+  dp.nwin  = (int)idesc.shape[0];
+  d.frames = (int)idesc.shape[1];
+  d.hop    = d.frames; // windows are consecutive, non-overlapping blocks of the input
+  check(dp.nwin >= 1, "expected at least one window");
+  d.z_begin = s.time_z_begin, d.z_end = s.time_z_end;
+  check(s.time_z_begin >= 0 && s.time_z_end > s.time_z_begin && s.time_z_end <= d.frames, "bad band [time_z_begin, time_z_end)");
+  d.clutter_rank = s.clutter_rank;
+  if (s.propagation == "fresnel")
+    d.propagation = HF_PROP_FRESNEL;
+  else if (s.propagation == "angular_spectrum")
+    d.propagation = HF_PROP_ANGULAR_SPECTRUM;
+  else if (s.propagation == "none")
+    d.propagation = HF_PROP_NONE;
+  else
+    check(false, "propagation must be fresnel, angular_spectrum or none");
+  d.moment_mask = 0;
+  for (const auto &m : s.moments) {
+    check(m == "M0" || m == "M1" || m == "M2", "moments must be among M0, M1, M2");
+    d.moment_mask |= m == "M0" ? HF_M0 : (m == "M1" ? HF_M1 : HF_M2);
+  }
+  check(d.moment_mask != 0, "at least one moment");
+  d.fftshift = s.fftshift ? 1 : 0;
+  check(s.form == "plain" || s.form == "chosen", "form must be plain or chosen");
+  d.form      = s.form == "chosen" ? HF_FORM_CHOSEN : HF_FORM_PLAIN;
+  d.max_batch = dp.nwin;
+  d.lambda = s.lambda, d.pitch = s.dx, d.z = s.z, d.fs = s.fs;
+  if (d.propagation != HF_PROP_NONE)
+    check(s.lambda > 0.f && s.dx > 0.f, "wavelength and dx must be positive");
+  if (s.padding) {
+    check(d.propagation == HF_PROP_ANGULAR_SPECTRUM, "padding applies to angular_spectrum only");
+    d.pad_w = s.padding->width, d.pad_h = s.padding->height;
+  }
+  if (s.filter) {
+    d.as_filter = 1;
+    d.r_inner = s.filter->r_inner, d.r_outer = s.filter->r_outer;
+    d.s_inner = s.filter->s_inner, d.s_outer = s.filter->s_outer;
+  }
+  dp.nmom = __builtin_popcount((unsigned)d.moment_mask);
+  dp.OH   = d.pad_h ? d.pad_h : d.height;
+  dp.OW   = d.pad_w ? d.pad_w : d.width;
+  return dp;
+}
+
+class DopplerTask final : public ISyncTask {
+public:
+  hf_plan     *plan = nullptr;
+  cudaStream_t stream{};
+  DopplerPlan  dp;
+  ~DopplerTask() override {
+    if (plan)
+      hf_plan_destroy(plan);
+  }
+  OpResult execute(SyncCtx &ctx) override {
+    hf_ok(hf_pipeline_exec(plan, ctx.inputs[0].data(), (int64_t)dp.nwin * dp.d.frames, 0, dp.nwin,
+                           reinterpret_cast<float *>(ctx.outputs[0].data()), stream),
+          "DopplerMoments");
+    return OpResult::Ok;
+  }
+};
+} // namespace
+
+InferResult DopplerMomentsFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"DopplerMomentsFactory"};
+  const auto  s = j.get<DopplerMomentsSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto dp = doppler_plan(check, input_descs[0], s);
+  return sync_result(input_descs[0],
+                     TDesc({(size_t)dp.nwin, (size_t)dp.nmom, (size_t)dp.OH, (size_t)dp.OW}, DType::F32, MemLoc::Device));
+}
+
+std::unique_ptr<ISyncTask> DopplerMomentsFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                         const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t    = std::make_unique<DopplerTask>();
+  t->dp     = doppler_plan(Check{"DopplerMomentsFactory"}, input_descs[0], j.get<DopplerMomentsSettings>());
+  t->stream = ctx.stream;
+  hf_ok(hf_plan_create(&t->dp.d, &t->plan, ctx.stream), "DopplerMoments");
+  return t;
+}
+
+// Same input and settings but z: rebuild the lens / transfer function only.
+std::unique_ptr<ISyncTask> DopplerMomentsFactory::update(std::unique_ptr<ISyncTask> old,
+                                                         std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                         const SyncCreateCtx &ctx) const {
+  auto *t = dynamic_cast<DopplerTask *>(old.get());
+  if (t && input_descs.size() == 1) {
+    const auto dp = doppler_plan(Check{"DopplerMomentsFactory"}, input_descs[0], j.get<DopplerMomentsSettings>());
+    hf_desc    a = dp.d, b = t->dp.d;
+    a.z = b.z = 0.f;
+    if (std::memcmp(&a, &b, sizeof(hf_desc)) == 0 && dp.nwin == t->dp.nwin) {
+      if (dp.d.z != t->dp.d.z)
+        hf_ok(hf_plan_set_z(t->plan, dp.d.z, ctx.stream), "DopplerMoments");
+      t->dp     = dp;
+      t->stream = ctx.stream;
+      return old;
+    }
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+// ================================================================================================
+// registry
+// ================================================================================================
+void register_path_kinds(core::Registry &r) {
+  r.register_sync("FresnelDiffraction", std::make_unique<FresnelDiffractionFactory>());
+  r.register_sync("AngularSpectrum", std::make_unique<AngularSpectrumFactory>());
+  r.register_sync("Pca", std::make_unique<PcaFactory>());
+  r.register_sync("FFT", std::make_unique<FFTFactory>());
+  r.register_sync("RFFT", std::make_unique<RFFTFactory>());
+  r.register_sync("Mean", std::make_unique<MeanFactory>());
+  r.register_sync("MeanAbs", std::make_unique<MeanAbsFactory>());
+  r.register_sync("Conversion", std::make_unique<ConversionFactory>());
+  r.register_sync("DopplerMoments", std::make_unique<DopplerMomentsFactory>());
+}
+
+core::Registry &default_registry() {
+  static core::Registry *reg = [] {
+    auto *r = new core::Registry();
+    register_path_kinds(*r);
+    return r;
+  }();
+  return *reg;
+}
+
+} // namespace hfb::nodes

@@ -7,8 +7,9 @@
  * comment says so).  Device pointers must be device-accessible memory of the current device.
  *
  * Each function names the Holoflow interface it replaces (paths relative to the Holoflow source
- * tree).  The C++ node layer (include/holoflow/core/*.hh, kinds registered under the reference's
- * kind strings) is built on top of these calls.
+ * tree).  The C++ node layer (include/holoflow_b200/core.hh, nodes.hh: the task interface with
+ * factories registered under the reference's kind strings) is built on these calls and reached
+ * from C through the hf_node_* functions at the end of this file.
  */
 #ifndef HOLOFLOW_B200_H
 #define HOLOFLOW_B200_H
@@ -260,6 +261,38 @@ int     hf_stream_process(hf_stream *stream, int max_windows, float *out, int ou
 /* Waits for the most recent asynchronous (out_is_host = 2) output copy: on the host when
  * host_block, else by making `s` wait for it. */
 int     hf_stream_output_wait(hf_stream *stream, hf_stream_t s, int host_block);
+
+/* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
+ * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------
+ * Kinds: "FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
+ * "Conversion" (the reference's, with its JSON settings keys) and "DopplerMoments" (the fused
+ * per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
+ * HF_U16, HF_F32, HF_CF32), strides in BYTES (all zero = C-contiguous), mem_loc 1 = device.
+ * infer() failures return HF_ERR_INVALID with "<Factory> inference error: ..." in hf_last_error();
+ * work is enqueued on the stream given at create/update. */
+#define HF_TDESC_MAX_RANK 8
+typedef struct hf_tdesc {
+  int32_t rank, dtype, mem_loc, reserved;
+  int64_t shape[HF_TDESC_MAX_RANK];
+  int64_t strides[HF_TDESC_MAX_RANK];
+  int64_t offset;
+} hf_tdesc;
+typedef struct hf_node hf_node;
+/* Comma-separated list of the registered kinds. */
+int hf_node_kinds(char *buf, size_t cap);
+/* Output descriptors of a node without creating it (ITaskFactory::infer). */
+int hf_node_infer(const char *kind, const char *json_settings, int n_inputs, const hf_tdesc *inputs, int *n_outputs,
+                  hf_tdesc *outputs, int outputs_cap);
+/* infer + create (ISyncTaskFactory::create); the node keeps the descriptors. */
+int hf_node_create(const char *kind, const char *json_settings, int n_inputs, const hf_tdesc *inputs, hf_stream_t s,
+                   hf_node **node);
+/* ISyncTaskFactory::update: reuses the task where the factory can (z-only changes). */
+int hf_node_update(hf_node *node, const char *json_settings, int n_inputs, const hf_tdesc *inputs, hf_stream_t s);
+/* ISyncTask::execute on device tensors given by their origin pointers; *op_result receives the
+ * OpResult (0 = Ok). */
+int hf_node_execute(hf_node *node, void *const *inputs, void *const *outputs, int *op_result);
+int hf_node_output_desc(const hf_node *node, int index, hf_tdesc *out);
+int hf_node_destroy(hf_node *node);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,111 @@
+// holoflow_b200 node layer: the Doppler path's compute nodes behind the restated task interface
+// (core.hh), registered under the reference's kind strings (manager.cc:159-237).  Each factory
+// parses the same JSON settings keys as the reference node, performs the same inference checks
+// with the same "<Factory> inference error: " messages, and executes through the C ABI
+// (include/holoflow_b200.h) on the stream given at create()/update().
+#pragma once
+
+#include <optional>
+
+#include "holoflow_b200/core.hh"
+
+namespace hfb::nodes {
+
+// ---- settings (same keys as the reference) ------------------------------------------------------
+struct FresnelDiffractionSettings { // fresnel_diffraction.cu:40-64
+  float            lambda = 0.f, dx = 0.f, dy = 0.f, z = 0.f;
+  std::vector<int> axes{-2, -1};
+  bool             skip_phase_shift = false;
+  bool             output_magnitude = false;
+};
+struct AngularSpectrumFilter { // angular_spectrum.cu:40-55
+  uint32_t r_inner = 0, r_outer = 0, s_inner = 0, s_outer = 0;
+};
+struct AngularSpectrumPadding { // angular_spectrum.cu:57-66
+  int width = 0, height = 0;
+};
+struct AngularSpectrumSettings { // angular_spectrum.cu:68-99
+  float                                lambda = 0.f, dx = 0.f, dy = 0.f, z = 0.f;
+  std::optional<AngularSpectrumFilter>  filter;
+  std::optional<AngularSpectrumPadding> padding;
+};
+struct PcaSettings { // pca.cc:141-151
+  int begin = 0, end = 0;
+  int components() const { return end - begin; }
+};
+enum class FftNorm { Backward, Forward, Ortho }; // fft_common.cc:45-62
+struct FFTSettings {                             // fft.cu:33-52
+  int     axis = -1;
+  FftNorm norm = FftNorm::Backward;
+};
+struct MeanSettings { // mean.cu:30-70
+  std::vector<int> axis;
+  bool             keepdims = false;
+};
+struct ConversionSettings { // conversion.cu:40-103
+  enum class Target { U8, U16, F32, CF32 } target = Target::F32;
+  enum class Strategy { Real, Scaled, Modulus, Argument } strategy = Strategy::Real;
+};
+// The fused per-window path (no single reference node: it replaces the chain GraphBuilder wires,
+// graph_builder.cc:245-678).  Keys follow the reference's Settings names where one exists.
+struct DopplerMomentsSettings {
+  int                                   time_z_begin = 0, time_z_end = 0; // settings.hh:111-112
+  int                                   clutter_rank = 0;                 // SVD filter rank removed
+  std::string                           propagation  = "fresnel";         // fresnel | angular_spectrum | none
+  std::string                           input_format = "u16";             // u8 | u16 | f32 | mono12p
+  int                                   height = 0, width = 0;            // frame size (mono12p rows)
+  float                                 lambda = 0.f, dx = 0.f, z = 0.f, fs = 37e3f;
+  std::vector<std::string>              moments{"M0", "M1", "M2"};
+  bool                                  fftshift = false;
+  std::string                           form     = "plain";               // plain | chosen
+  std::optional<AngularSpectrumFilter>  filter;
+  std::optional<AngularSpectrumPadding> padding;
+};
+
+void from_json(const nlohmann::json &j, FresnelDiffractionSettings &s);
+void from_json(const nlohmann::json &j, AngularSpectrumFilter &s);
+void from_json(const nlohmann::json &j, AngularSpectrumPadding &s);
+void from_json(const nlohmann::json &j, AngularSpectrumSettings &s);
+void from_json(const nlohmann::json &j, PcaSettings &s);
+void from_json(const nlohmann::json &j, FftNorm &s);
+void from_json(const nlohmann::json &j, FFTSettings &s);
+void from_json(const nlohmann::json &j, MeanSettings &s);
+void from_json(const nlohmann::json &j, ConversionSettings &s);
+void from_json(const nlohmann::json &j, DopplerMomentsSettings &s);
+
+// ---- factories ------------------------------------------------------------------------------------
+using core::InferResult;
+using core::ISyncTask;
+using core::ISyncTaskFactory;
+using core::SyncCreateCtx;
+using core::TDesc;
+
+#define HFB_SYNC_FACTORY(Name)                                                                            \
+  class Name final : public ISyncTaskFactory {                                                            \
+  public:                                                                                                 \
+    InferResult infer(std::span<const TDesc> input_descs, const nlohmann::json &jsettings) const override; \
+    std::unique_ptr<ISyncTask> create(std::span<const TDesc> input_descs, const nlohmann::json &jsettings, \
+                                      const SyncCreateCtx &ctx) const override;                           \
+    std::unique_ptr<ISyncTask> update(std::unique_ptr<ISyncTask> old_task, std::span<const TDesc> input_descs, \
+                                      const nlohmann::json &jsettings, const SyncCreateCtx &ctx) const override; \
+  }
+
+HFB_SYNC_FACTORY(FresnelDiffractionFactory);
+HFB_SYNC_FACTORY(AngularSpectrumFactory);
+HFB_SYNC_FACTORY(PcaFactory);
+HFB_SYNC_FACTORY(FFTFactory);
+HFB_SYNC_FACTORY(RFFTFactory);
+HFB_SYNC_FACTORY(MeanFactory);
+HFB_SYNC_FACTORY(MeanAbsFactory);
+HFB_SYNC_FACTORY(ConversionFactory);
+HFB_SYNC_FACTORY(DopplerMomentsFactory);
+#undef HFB_SYNC_FACTORY
+
+// Registers every node above under its kind string: "FresnelDiffraction", "AngularSpectrum",
+// "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion" (the reference's) and "DopplerMoments".
+void register_path_kinds(core::Registry &registry);
+
+// The process-wide registry the C ABI's hf_node_* functions use.
+core::Registry &default_registry();
+
+} // namespace hfb::nodes

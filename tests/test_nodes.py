@@ -1,0 +1,131 @@
+"""The node layer without a GPU: kinds are registered under the reference's strings, settings are
+parsed with the reference's keys, and infer() returns the reference's output descriptors or fails
+with its "<Factory> inference error: ..." messages (restated from fresnel_diffraction.cu:94-99,
+466-508, angular_spectrum.cu:446-494, pca.cc:157-193, conversion.cu:389-410, mean.cu:30-70)."""
+import pytest
+
+import holoflow_b200 as hf
+from holoflow_b200 import nodes as N
+
+U8, U16, F32, CF32 = 0, 1, 2, 3
+
+
+def desc(shape, dtype=F32, device=True, strides=None):
+    d = hf.HfTDesc()
+    d.rank, d.dtype, d.mem_loc = len(shape), dtype, 1 if device else 0
+    for i, n in enumerate(shape):
+        d.shape[i] = n
+    if strides:
+        for i, s in enumerate(strides):
+            d.strides[i] = s
+    return d
+
+
+FRESNEL = {"lambda": 852e-9, "dx": 12e-6, "dy": 12e-6, "z": 0.25}
+AS = {"lambda": 852e-9, "dx": 12e-6, "dy": 12e-6, "z": 0.30}
+
+
+def out_of(kind, settings, descs):
+    (o,) = N.infer(kind, settings, descs)
+    return N.shape_of(o), o.dtype
+
+
+def invalid(kind, settings, descs, fragment):
+    with pytest.raises(hf.HfError) as e:
+        N.infer(kind, settings, descs)
+    assert e.value.code == hf.HF_ERR_INVALID
+    assert fragment in str(e.value), str(e.value)
+
+
+def test_reference_kinds_are_registered():
+    assert set(N.kinds()) == {"FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
+                              "Conversion", "DopplerMoments"}
+
+
+def test_unknown_kind_and_bad_settings():
+    invalid("Fresnel", FRESNEL, [desc([4, 8, 8], CF32)], "no synchronous task of kind 'Fresnel'")
+    invalid("FresnelDiffraction", {"lambda": 1.0}, [desc([4, 8, 8], CF32)], "settings")
+
+
+def test_fresnel_infer():
+    assert out_of("FresnelDiffraction", FRESNEL, [desc([3, 64, 32], CF32)]) == ((3, 64, 32), CF32)
+    assert out_of("FresnelDiffraction", FRESNEL, [desc([3, 64, 32], F32)]) == ((3, 64, 32), CF32)
+    assert out_of("FresnelDiffraction", {**FRESNEL, "output_magnitude": True}, [desc([64, 32], CF32)]) == ((64, 32), F32)
+    p = "FresnelDiffractionFactory inference error: "
+    invalid("FresnelDiffraction", {**FRESNEL, "dy": 10e-6}, [desc([8, 8], CF32)], p + "dx must equal dy")
+    invalid("FresnelDiffraction", {**FRESNEL, "lambda": 0.0}, [desc([8, 8], CF32)], p + "wavelength must be positive")
+    invalid("FresnelDiffraction", FRESNEL, [desc([8], CF32)], p + "input must be a tensor of rank 2 or higher")
+    invalid("FresnelDiffraction", FRESNEL, [desc([8, 8], U16)], p + "input must be complex float32 or real float32")
+    invalid("FresnelDiffraction", FRESNEL, [desc([8, 8], CF32, device=False)], p + "input must be in device memory")
+    invalid("FresnelDiffraction", {**FRESNEL, "axes": [0]}, [desc([8, 8], CF32)], p + "axes must contain exactly two")
+    invalid("FresnelDiffraction", {**FRESNEL, "axes": [-1, -1]}, [desc([8, 8], CF32)], p + "axes must be distinct")
+    invalid("FresnelDiffraction", FRESNEL, [desc([2, 8, 8], CF32)] * 2, p + "expected exactly one input")
+
+
+def test_angular_spectrum_infer():
+    (o,) = N.infer("AngularSpectrum", AS, [desc([2, 64, 64], CF32)])
+    assert N.shape_of(o) == (2, 64, 64) and o.dtype == CF32
+    pad = {**AS, "padding": {"width": 96, "height": 80}}
+    assert out_of("AngularSpectrum", pad, [desc([2, 64, 64], F32)]) == ((2, 80, 96), CF32)
+    p = "AngularSpectrumFactory inference error: "
+    invalid("AngularSpectrum", {**AS, "padding": {"width": 65, "height": 64}}, [desc([64, 64], CF32)],
+            p + "horizontal padding must be even")
+    invalid("AngularSpectrum", {**AS, "padding": {"width": 32, "height": 64}}, [desc([64, 64], CF32)],
+            p + "padding width must be at least the input width")
+    invalid("AngularSpectrum", AS, [desc([64, 64], CF32, strides=[1024, 8])], p + "input must be C-contiguous")
+
+
+def test_pca_infer():
+    assert out_of("Pca", {"begin": 2, "end": 5}, [desc([3, 16, 8, 8])]) == ((3, 3, 8, 8), F32)
+    p = "PcaFactory inference error: "
+    invalid("Pca", {"begin": 3, "end": 3}, [desc([16, 8, 8])], p + "expected begin < end")
+    invalid("Pca", {"begin": -1, "end": 3}, [desc([16, 8, 8])], p + "expected begin >= 0")
+    invalid("Pca", {"begin": 0, "end": 17}, [desc([16, 8, 8])], p + "expected end <= n_features")
+    invalid("Pca", {"begin": 0, "end": 2}, [desc([8, 8])], p + "expected input rank >= 3")
+
+
+def test_fft_rfft_infer():
+    assert out_of("FFT", {"axis": 1, "norm": "ortho"}, [desc([2, 32, 8, 8], U16)]) == ((2, 32, 8, 8), CF32)
+    assert out_of("RFFT", {"axis": 1}, [desc([2, 64, 8, 8])]) == ((2, 33, 8, 8), CF32)
+    assert out_of("RFFT", {}, [desc([4, 10])]) == ((4, 6), CF32)  # axis defaults to -1
+    invalid("FFT", {"axis": 4}, [desc([2, 32, 8, 8])], "FFTFactory inference error: axis out of range")
+    invalid("RFFT", {"axis": 1}, [desc([2, 32, 8], CF32)], "RFFTFactory inference error: input must be real")
+    with pytest.raises(hf.HfError, match="unsupported norm"):
+        N.infer("FFT", {"axis": 1, "norm": "unitary"}, [desc([2, 32, 8])])
+
+
+def test_mean_infer():
+    assert out_of("Mean", {"axis": -3, "keepdims": True}, [desc([1, 28, 8, 8])]) == ((1, 1, 8, 8), F32)
+    assert out_of("Mean", {"axis": 0}, [desc([1, 8, 8])]) == ((8, 8), F32)
+    assert out_of("Mean", {"axes": [1, 2]}, [desc([2, 3, 4, 5], CF32)]) == ((2, 5), CF32)
+    assert out_of("Mean", {"axis": None}, [desc([2, 3])]) == ((), F32)
+    assert out_of("MeanAbs", {"axis": -3, "keepdims": True}, [desc([1, 28, 8, 8], CF32)]) == ((1, 1, 8, 8), F32)
+    invalid("Mean", {"axis": 5}, [desc([2, 3])], "MeanFactory inference error: axis out of range")
+    with pytest.raises(hf.HfError, match="axis must be int, array, or null"):
+        N.infer("Mean", {"axis": "x"}, [desc([2, 3])])
+
+
+def test_conversion_infer():
+    conv = lambda t, s: {"target": t, "strategy": s}
+    assert out_of("Conversion", conv("CF32", "Real"), [desc([4, 4], U16)]) == ((4, 4), CF32)
+    assert out_of("Conversion", conv("U8", "Scaled"), [desc([4, 4], F32)]) == ((4, 4), U8)
+    assert out_of("Conversion", conv("F32", "Argument"), [desc([4, 4], CF32)]) == ((4, 4), F32)
+    invalid("Conversion", conv("F32", "Real"), [desc([4, 4], U16)],
+            "ConversionFactory inference error: Unsupported conversion configuration")
+    with pytest.raises(hf.HfError, match="Unknown strategy type for conversion: Linear"):
+        N.infer("Conversion", conv("F32", "Linear"), [desc([4, 4], U8)])
+
+
+def test_doppler_moments_infer():
+    s = {"time_z_begin": 6, "time_z_end": 16, "propagation": "angular_spectrum", "lambda": 852e-9, "dx": 12e-6,
+         "z": 0.3, "input_format": "u16", "padding": {"width": 96, "height": 80}}
+    assert out_of("DopplerMoments", s, [desc([2, 32, 64, 64], U16)]) == ((2, 3, 80, 96), F32)
+    s12 = {"time_z_begin": 4, "time_z_end": 32, "propagation": "fresnel", "lambda": 852e-9, "dx": 12e-6, "z": 0.25,
+           "clutter_rank": 4, "input_format": "mono12p", "height": 64, "width": 64, "moments": ["M0"],
+           "form": "chosen"}
+    assert out_of("DopplerMoments", s12, [desc([3, 64, 64 * 64 * 3 // 2], U8)]) == ((3, 1, 64, 64), F32)
+    p = "DopplerMomentsFactory inference error: "
+    invalid("DopplerMoments", {**s12, "width": 32}, [desc([3, 64, 64 * 64 * 3 // 2], U8)],
+            p + "height x width must match the packed frame size")
+    invalid("DopplerMoments", {**s, "time_z_end": 40}, [desc([2, 32, 64, 64], U16)], p + "bad band")
+    invalid("DopplerMoments", {**s, "moments": ["M3"]}, [desc([2, 32, 64, 64], U16)], p + "moments must be among")
