@@ -143,6 +143,22 @@ def cpu_baseline(sample_windows=1):
     return sample_windows / dt, dt, os.cpu_count()
 
 
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The largest `value` over all ranks (device-timed milliseconds); identity on one rank."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, steps: int, units_per_step: int, ms: float) -> float:
+    """Whole-job units per second: every rank processed steps x units_per_step in (max) `ms`."""
+    return world * steps * units_per_step / (ms / 1000.0)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -245,11 +261,8 @@ def main():
     stages = {k: v for k, v in pipe.stage_times().items() if v[0] > 0}
     pipe.timing(False)
     cam_dev.close()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps * B / (ms / 1000.0)
+    ms = max_over_ranks(ms, world, dev)
+    value = aggregate_rate(world, args.steps, B, ms)
 
     # roofline of the dominant stage (algorithmic bytes / its CUDA-event time)
     peak, peak_kind = peaks()
@@ -317,15 +330,11 @@ def main():
         cam.output_wait(stream)
         f1.record(stream)
         torch.cuda.synchronize()
-        ems = f0.elapsed_time(f1)
-        if world > 1:
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(f0.elapsed_time(f1), world, dev)
         step_lat = sorted(a.elapsed_time(b) for a, b in lat)
         p50 = step_lat[len(step_lat) // 2]
         p99 = step_lat[min(len(step_lat) - 1, int(round(0.99 * (len(step_lat) - 1))))]
-        e2e = {"value": round(world * args.steps * B / (ems / 1000.0), 2), "unit": "images/s",
+        e2e = {"value": round(aggregate_rate(world, args.steps, B, ems), 2), "unit": "images/s",
                "h2d_bytes_per_step": nstep_frames * fb, "d2h_bytes_per_step": B * nmom * H * W * 4,
                "ms_per_step": round(ems / args.steps, 4),
                "latency_ms_p50": round(p50, 3), "latency_ms_p99": round(p99, 3),
