@@ -96,6 +96,16 @@ _PROTOS = {
     "hf_stream_ready": (_i64, [_vp]),
     "hf_stream_process": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.POINTER(C.c_int), _vp]),
     "hf_stream_output_wait": (C.c_int, [_vp, _vp, C.c_int]),
+    "hf_server_create": (C.c_int, [_sz, C.c_int, C.POINTER(_vp)]),
+    "hf_server_destroy": (C.c_int, [_vp]),
+    "hf_server_open": (C.c_int, [_vp, C.POINTER(HfDesc), _i64, C.POINTER(C.c_int)]),
+    "hf_server_close": (C.c_int, [_vp, C.c_int]),
+    "hf_server_push": (C.c_int, [_vp, C.c_int, _vp, _i64]),
+    "hf_server_ready": (_i64, [_vp, C.c_int]),
+    "hf_server_step": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int)]),
+    "hf_server_sync": (C.c_int, [_vp]),
+    "hf_server_latencies": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
+    "hf_server_open_count": (C.c_int, [_vp]),
     "hf_node_kinds": (C.c_int, [C.c_char_p, _sz]),
     "hf_node_infer": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(HfTDesc), C.POINTER(C.c_int),
                                 C.POINTER(HfTDesc), C.c_int]),

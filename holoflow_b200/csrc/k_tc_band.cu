@@ -2,18 +2,20 @@
 // tensor cores, lens multiply and the row FFT of every band plane, one image row at a time.
 //
 // Per image row r of window w (W pixels = W/128 M-tiles):
-//   S[p][k] = sum_t (x_t[p] - 2048) W16[t][k] + 2048 sum_t W16[t][k]     (W16 = f16(W))
-// is a [W x 64] x [64 x 2nz] product: A = the row's samples, f16, MN-major (pixels contiguous per
-// frame, as they arrive), B = W16 as real/imaginary columns, K-major; tcgen05.mma M = 128, N = 64,
-// K = 16, f32 accumulators in TMEM (tile j -> columns 64j .. 64j+63, all 512 columns for W = 1024).
-// The epilogue moves 8 bins at a time from TMEM into shared memory (adding the DC correction and
-// multiplying by the Fresnel lens), runs each bin's length-W row FFT in place (four-step, XOR-
-// swizzled exchange) and stores the row of that band plane.
+//   S[p][k] = sum_t (x_t[p] - 2048) (Wh + Wl)[t][k] + 2048 sum_t (Wh + Wl)[t][k]
+// with Wh = f16(W) and Wl = f16(W - Wh), is a [W x 64] x [64 x 2nz] product taken twice (Wh, then
+// Wl, into the same accumulator): A = the row's samples x - 2048 (exact in f16 for 12-bit data),
+// MN-major (pixels contiguous per frame, as they arrive), B = Wh / Wl as real/imaginary columns,
+// K-major; tcgen05.mma M = 128, N = 64, K = 16, f32 accumulators in TMEM (tile j -> columns
+// 64j .. 64j+63, all 512 columns for W = 1024).
+// The epilogue moves 4 bins at a time from TMEM into shared memory (adding the DC correction and
+// multiplying by the Fresnel lens), runs each bin's length-W row FFT in place (four-step, padded
+// exchange) and stores the row of that band plane.
 //
 // Warp roles (384 threads, one CTA per SM, persistent over rows):
-//   warps 0-3  : load + unpack the next row into the A operand, rebuild B, and (thread 0) issue the
-//                MMAs once the epilogue has released TMEM;
-//   warps 4-11 : epilogue (each warp owns the TMEM lane quarter warp % 4).
+//   warps 0-3  : load + unpack the next row into the A operand, rebuild B per window, and (thread 0)
+//                issue the MMAs once the epilogue has released TMEM;
+//   warps 4-11 : epilogue, two teams of four (each warp owns the TMEM lane quarter warp % 4).
 // mbarriers: `full` (MMAs of a row complete: TMEM readable, A/B reusable) and `free` (the 8
 // epilogue warps finished reading TMEM).  Every wait is bounded; an expired wait sets the status
 // word and an abort flag that turns the remaining waits into no-ops, so the kernel always exits.
@@ -96,9 +98,9 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t *sA   = smem;                                  // NTILE x 16 KB
-  uint8_t *sB   = sA + NTILE * kTileBytes;               // 64 rows x 128 B
+  uint8_t *sB   = sA + NTILE * kTileBytes;               // W16 hi, then lo: 2 x 64 rows x 128 B
   constexpr int RS = XBuf<N1>::kSize > W ? XBuf<N1>::kSize : W; // gbuf row stride (room for the exchange)
-  float2  *gbuf = reinterpret_cast<float2 *>(sB + 8192); // 8 bins x RS
+  float2  *gbuf = reinterpret_cast<float2 *>(sB + 16384); // 8 bins x RS
   float2  *twt  = gbuf + 8 * RS;                         // [N1][32] twiddles w_W^(k1 n2)
   float   *colsum = reinterpret_cast<float *>(twt + W);   // [2][64], indexed by window parity
   int64_t *foff = reinterpret_cast<int64_t *>(colsum + 128); // [64] frame offsets of the window
@@ -133,18 +135,21 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
       if (k > 0) // MMAs of the previous row done: A and B may be overwritten
         wait_or_abort(&mbar[0], (uint32_t)((k - 1) & 1), abortv, a.status, 11);
       const bool new_w = w != cur_w;
-      if (new_w) { // per window: frame offsets, B = W16 and its DC correction
+      if (new_w) { // per window: frame offsets, B = (Wh, Wl) and its DC correction
         cur_w = w;
         wpar ^= 1;
         if (tid < 64)
           foff[tid] = (a.ring.frame(w, tid) - a.ring.base);
       }
-      // B (K-major, 128-byte swizzle): row n = 2*bin + {re, im}, K = frame t
+      // B (K-major, 128-byte swizzle): row n = 2*bin + {re, im}, K = frame t.  W is split into
+      // f16 hi + lo parts (lo = f16(W - hi)); both multiply the same A into one accumulator, so
+      // the band carries W to about 22 bits instead of f16's 11 (clutter 100x the signal would
+      // otherwise leak through the filter at the f16 rounding of W).
       const float2 *wm = a.wmat + (int64_t)w * a.wmat_stride;
       if (new_w)
       for (int e = tid; e < 64 * 8; e += kLoaders) {
         const int n = e >> 3, c = e & 7; // one 16-byte chunk = 8 frames
-        __half hv[8];
+        __half hv[8], lv[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const int t = 8 * c + i;
@@ -154,8 +159,11 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
             v              = (n & 1) ? z.y : z.x;
           }
           hv[i] = __float2half_rn(v);
+          lv[i] = __float2half_rn(v - __half2float(hv[i]));
         }
-        *reinterpret_cast<uint4 *>(sB + n * 128 + ((c ^ (n & 7)) << 4)) = *reinterpret_cast<const uint4 *>(hv);
+        const int off = n * 128 + ((c ^ (n & 7)) << 4);
+        *reinterpret_cast<uint4 *>(sB + off)        = *reinterpret_cast<const uint4 *>(hv);
+        *reinterpret_cast<uint4 *>(sB + 8192 + off) = *reinterpret_cast<const uint4 *>(lv);
       }
       if (new_w)
         named_bar(1, kLoaders); // frame offsets visible to every loader
@@ -193,12 +201,13 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
         }
       }
       named_bar(1, kLoaders); // A (and B) complete
-      if (new_w && tid < 64) { // DC correction of the shifted samples: shift * sum_t W16[t][n]
+      if (new_w && tid < 64) { // DC correction of the shifted samples: shift * sum_t (hi + lo)[t][n]
         float sacc = 0.f;
         for (int t = 0; t < 64; ++t) {
           const int    c  = t >> 3;
-          const __half hv = *reinterpret_cast<const __half *>(sB + tid * 128 + ((c ^ (tid & 7)) << 4) + (t & 7) * 2);
-          sacc += __half2float(hv);
+          const int    off = tid * 128 + ((c ^ (tid & 7)) << 4) + (t & 7) * 2;
+          sacc += __half2float(*reinterpret_cast<const __half *>(sB + off)) +
+                  __half2float(*reinterpret_cast<const __half *>(sB + 8192 + off));
         }
         colsum[wpar * 64 + tid] = a.shift * sacc;
       }
@@ -212,9 +221,9 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
 #pragma unroll
           for (int j = 0; j < NTILE; ++j)
 #pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-              const uint64_t ad = tc::sw128_desc(tc::smem_u32(sA + j * kTileBytes + ks * 2048), 8192, 1024);
-              const uint64_t bd = tc::sw128_desc(tc::smem_u32(sB + ks * 32), 16, 1024);
+            for (int ks = 0; ks < 8; ++ks) { // k-steps 0-3 with W hi, 4-7 with W lo
+              const uint64_t ad = tc::sw128_desc(tc::smem_u32(sA + j * kTileBytes + (ks & 3) * 2048), 8192, 1024);
+              const uint64_t bd = tc::sw128_desc(tc::smem_u32(sB + (ks >> 2) * 8192 + (ks & 3) * 32), 16, 1024);
               tc::mma_f16(tbase + 64 * j, ad, bd, idesc, ks > 0 ? 1u : 0u);
             }
         }
@@ -312,7 +321,7 @@ template <int FMT, int N1> int launch_n1(const BandRowsArgs &a, cudaStream_t s) 
   constexpr int W     = N1 * 32;
   constexpr int NTILE = W / 128;
   constexpr int RS    = XBuf<N1>::kSize > W ? XBuf<N1>::kSize : W;
-  const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 8192 + (size_t)8 * RS * 8 + (size_t)W * 8 + 128 * 4 +
+  const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 16384 + (size_t)8 * RS * 8 + (size_t)W * 8 + 128 * 4 +
                       64 * 8 + 16 + 8;
   HF_CUDA(cudaFuncSetAttribute(band_rows_tc_kernel<FMT, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t nrows = (int64_t)a.nwin * a.H;

@@ -262,6 +262,28 @@ int     hf_stream_process(hf_stream *stream, int max_windows, float *out, int ou
  * host_block, else by making `s` wait for it. */
 int     hf_stream_output_wait(hf_stream *stream, hf_stream_t s, int host_block);
 
+/* ---- streaming server: many camera streams on one GPU, continuous batching -------------------
+ * Each open stream owns a plan, a device frame ring and its own CUDA streams.  hf_server_open
+ * admits a stream only while the device keeps `hbm_reserve_bytes` free after the stream's buffers
+ * are created (else HF_ERR_NOMEM: retry after other streams close).  hf_server_step gives every
+ * open stream with ready windows one batch on its own CUDA stream, so batches of different streams
+ * run concurrently; images of stream i go to out[i] (pinned host, [max_batch][n_moments][OH][OW],
+ * NULL to skip the stream) and n_done[i] receives the windows done.  out[i] may be read, and a
+ * later step may reuse it, once hf_server_sync has returned.  A window's frame-to-image latency
+ * (from the push that brought its last frame to its images reaching the host) is collected at
+ * hf_server_sync and read by hf_server_latencies. */
+typedef struct hf_server hf_server;
+int     hf_server_create(size_t hbm_reserve_bytes, int max_streams, hf_server **server);
+int     hf_server_destroy(hf_server *server);
+int     hf_server_open(hf_server *server, const hf_desc *desc, int64_t ring_frames, int *stream_id);
+int     hf_server_close(hf_server *server, int stream_id);
+int     hf_server_push(hf_server *server, int stream_id, const void *frames, int64_t nframes);
+int64_t hf_server_ready(const hf_server *server, int stream_id);
+int     hf_server_step(hf_server *server, float *const *out, int *n_done);
+int     hf_server_sync(hf_server *server);
+int     hf_server_latencies(hf_server *server, float *ms, int cap, int *n);
+int     hf_server_open_count(const hf_server *server);
+
 /* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
  * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------
  * Kinds: "FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",

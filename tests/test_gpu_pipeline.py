@@ -233,3 +233,20 @@ def test_camera_stream_push_stream_and_async_output(cuda):
     for w in range(nsteps * B):
         assert np.array_equal(got[w], expect[w]), w
     assert p.status() == 0
+
+
+@pytest.mark.parametrize("scr_db", [0.0, -20.0, -40.0])
+def test_config2_clutter_error_vs_fp64_oracle(cuda, scr_db):
+    """Config 2: config 1 with a rank-2 global phase/amplitude clutter at SCR 0, -20, -40 dB,
+    top-4 clutter removal, 256 x 256 crop of the scene size.  Relative L2 error of each moment image
+    against the FP64 oracle: < 1e-4 in the plain form, < 1e-3 in the chosen form."""
+    z0, z1 = O.band_bins(4e3, 33e3, 67e3, 64)
+    kw = dict(height=256, width=256, frames=64, hop=16, z_begin=z0, z_end=z1, fs=67e3, z=0.25, clutter_rank=4)
+    frames = S.Interferograms(S.config2(scr_db, 64 + 16, height=256, width=256)).frames(0, 80)
+    ocfg = _oracle_cfg(kw)
+    exp = [O.reconstruct_window(frames[16 * w: 16 * w + 64], ocfg) for w in range(2)]
+    for form, tol in ((0, 1e-4), (1, 1e-3)):
+        got, _ = _run(cuda, frames, {**kw, "form": form}, 2)
+        errs = [O.rel_l2(got[w, m], exp[w][m]) for w in range(2) for m in range(3)]
+        print(f"config2 SCR {scr_db:+.0f} dB form {form}: max rel L2 {max(errs):.3e}")
+        assert max(errs) < tol, errs
