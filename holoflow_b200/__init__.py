@@ -106,6 +106,13 @@ _PROTOS = {
     "hf_server_sync": (C.c_int, [_vp]),
     "hf_server_latencies": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "hf_server_open_count": (C.c_int, [_vp]),
+    "hf_multi_create": (C.c_int, [C.c_int, C.POINTER(HfDesc), C.POINTER(_vp)]),
+    "hf_multi_destroy": (C.c_int, [_vp]),
+    "hf_multi_exec": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(C.c_int),
+                                C.POINTER(_vp), _vp]),
+    "hf_multi_tune": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(C.c_int),
+                                C.POINTER(_vp), C.c_int, _vp, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    "hf_multi_plan": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
     "hf_node_kinds": (C.c_int, [C.c_char_p, _sz]),
     "hf_node_infer": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(HfTDesc), C.POINTER(C.c_int),
                                 C.POINTER(HfTDesc), C.c_int]),

@@ -77,3 +77,41 @@ def config1_scene(height=1024, width=1024, acquisition=0) -> Scene:
 
 def config0_scene(acquisition=0) -> Scene:
     return Scene(512, 512, 37e3, 400, 0.30, seed=1000 + 17 * acquisition)
+
+
+@dataclass
+class Acquisition:
+    """One acquisition of the uneven batch: its scene and processing parameters."""
+    scene: Scene
+    frames: int        # T, window length
+    hop: int
+    z: float           # propagation distance of the reconstruction
+    z_begin: int       # band bins [z_begin, z_end) of the T-point DFT
+    z_end: int
+
+
+def band_bins(f_lo: float, f_hi: float, fs: float, T: int) -> tuple[int, int]:
+    """z0 = ceil(f_lo/df), z1 = floor(f_hi/df) + 1 with df = fs/T, clipped to the one-sided range."""
+    df = fs / T
+    z0 = int(math.ceil(f_lo / df - 1e-9))
+    z1 = min(int(math.floor(f_hi / df + 1e-9)) + 1, T // 2 + 1)
+    return z0, z1
+
+
+def config3_acquisitions(n: int = 16, seed: int = 1003) -> list[Acquisition]:
+    """Seeded uneven acquisitions: frame sizes from {256^2, 512^2, 768^2, 1024^2, 1536 x 1024 (W x H)},
+    window lengths from {32, 64, 128} (hop T/4), z uniform in [0.15, 0.40] m, fs from {37, 67} kHz,
+    band 4-33 kHz at 67 kHz and 6-18 kHz at 37 kHz."""
+    import random
+    rng = random.Random(seed)
+    sizes = [(256, 256), (512, 512), (768, 768), (1024, 1024), (1024, 1536)]
+    out = []
+    for a in range(n):
+        H, W = sizes[rng.randrange(len(sizes))]
+        T = [32, 64, 128][rng.randrange(3)]
+        fs = [37e3, 67e3][rng.randrange(2)]
+        z = rng.uniform(0.15, 0.40)
+        z0, z1 = band_bins(4e3, 33e3, fs, T) if fs > 50e3 else band_bins(6e3, 18e3, fs, T)
+        scene = Scene(H, W, fs, int(round(0.85 * min(H, W))), z, seed=1000 + 3 + 17 * a)
+        out.append(Acquisition(scene, T, max(1, T // 4), z, z0, z1))
+    return out

@@ -284,6 +284,26 @@ int     hf_server_sync(hf_server *server);
 int     hf_server_latencies(hf_server *server, float *ms, int cap, int *n);
 int     hf_server_open_count(const hf_server *server);
 
+/* ---- many acquisitions in one graph launch ----------------------------------------------------
+ * hf_multi_create makes one plan per acquisition (frame size, window length, band, z, fs and form
+ * may all differ).  hf_multi_exec reconstructs nwin[i] (NULL: max_batch) windows of every
+ * acquisition i from its device ring (rings[i], ring_frames[i], first window frame first[i]) into
+ * outs[i] ([nwin][n_moments][OH][OW] float32) as ONE CUDA graph launch on `s`: the graph forks
+ * into branches that each run a share of the acquisitions and joins at the end.  hf_multi_tune
+ * times candidate schedules (number of branches; largest-first or round-robin assignment) on the
+ * given buffers and keeps the fastest; *best_streams receives the branch count (negative for
+ * round-robin) and *best_ms the time of one launch.  The graph is captured on the first exec (and
+ * again whenever the buffers or the schedule change): make that call outside any other capture. */
+typedef struct hf_multi hf_multi;
+int hf_multi_create(int n_acquisitions, const hf_desc *descs, hf_multi **multi);
+int hf_multi_destroy(hf_multi *multi);
+int hf_multi_exec(hf_multi *multi, const void *const *rings, const int64_t *ring_frames, const int64_t *first,
+                  const int *nwin, float *const *outs, hf_stream_t s);
+int hf_multi_tune(hf_multi *multi, const void *const *rings, const int64_t *ring_frames, const int64_t *first,
+                  const int *nwin, float *const *outs, int reps, hf_stream_t s, int *best_streams, float *best_ms);
+/* The plan of acquisition i (owned by the multi). */
+int hf_multi_plan(hf_multi *multi, int i, hf_plan **plan);
+
 /* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
  * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------
  * Kinds: "FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
