@@ -29,12 +29,15 @@ namespace {
 constexpr int kColC = 8; // columns per CTA strip
 
 __device__ __forceinline__ bool wait_stage(uint64_t *mbar, uint32_t parity, volatile int *abort, int *status) {
+  const uint64_t t0 = tc::globaltimer_ns();
   for (uint32_t i = 0; i < tc::kWaitLimit; ++i) {
     if (tc::mbar_try_wait(mbar, parity))
       return true;
-    if ((i & 1023u) == 1023u && *abort)
-      return false;
+    if ((i & 255u) == 255u && (*abort || tc::globaltimer_ns() - t0 > tc::kWaitNs))
+      break;
   }
+  if (*abort)
+    return false;
   if (status)
     atomicCAS(status, 0, 21);
   *abort = 1;

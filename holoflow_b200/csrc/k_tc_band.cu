@@ -36,12 +36,15 @@ constexpr int kTileBytes = 16384; // [K = 64][M = 128] f16 in two 64-pixel MN at
 
 __device__ __forceinline__ bool wait_or_abort(uint64_t *mbar, uint32_t parity, volatile int *abort, int *status,
                                               int code) {
+  const uint64_t t0 = tc::globaltimer_ns();
   for (uint32_t i = 0; i < tc::kWaitLimit; ++i) {
     if (tc::mbar_try_wait(mbar, parity))
       return true;
-    if ((i & 1023u) == 1023u && *abort)
-      return false;
+    if ((i & 255u) == 255u && (*abort || tc::globaltimer_ns() - t0 > tc::kWaitNs))
+      break;
   }
+  if (*abort)
+    return false;
   if (status)
     atomicCAS(status, 0, code);
   *abort = 1;
@@ -54,6 +57,9 @@ __device__ __forceinline__ void named_bar(int id, int n) {
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(mbar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cnt(uint64_t *mbar, uint32_t cnt) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(mbar)), "r"(cnt) : "memory");
 }
 
 template <int FMT> struct GroupLoad; // 32 consecutive samples of one frame
@@ -104,14 +110,15 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
   float2  *twt  = gbuf + 8 * RS;                         // [N1][32] twiddles w_W^(k1 n2)
   float   *colsum = reinterpret_cast<float *>(twt + W);   // [2][64], indexed by window parity
   int64_t *foff = reinterpret_cast<int64_t *>(colsum + 128); // [64] frame offsets of the window
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(foff + 64); // [0] full, [1] free
+  int64_t *rowbuf = foff + 64;                               // [2] row of iteration k, by parity
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(rowbuf + 2); // [0] full, [1] free
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
   int      *abort_flag = reinterpret_cast<int *>(tslot + 1);
   TwTable   tw{twt, W};
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[0], 2); // the MMA commit + the issuing thread's release arrive
     tc::mbar_init(&mbar[1], kEpilogue / 32);
     *abort_flag = 0;
     tc::mbar_fence_init();
@@ -130,10 +137,25 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
   if (tid < kLoaders) {
     // ------------------------------------------------------------------ loader / MMA warps
     int k = 0, cur_w = -1, wpar = 1;
-    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x, ++k) {
-      const int w = (int)(row / a.H), r = (int)(row % a.H);
+    for (;; ++k) {
       if (k > 0) // MMAs of the previous row done: A and B may be overwritten
         wait_or_abort(&mbar[0], (uint32_t)((k - 1) & 1), abortv, a.status, 11);
+      if (tid == 0) // rows are taken dynamically, so a CTA that starts late simply does fewer
+        rowbuf[k & 1] = atomicAdd(a.row_counter, 1);
+      named_bar(1, kLoaders);
+      const int64_t row = rowbuf[k & 1];
+      if (row >= nrows) { // no rows left: complete this phase empty so that the epilogue ends too
+        if (tid == 0) {
+          // Only after the epilogue has released the previous row, and so has seen that row's
+          // phase: completing this phase earlier could put `full` two phases ahead of the
+          // epilogue's parity wait, which could then never succeed.
+          if (k > 0)
+            wait_or_abort(&mbar[1], (uint32_t)((k - 1) & 1), abortv, a.status, 14);
+          mbar_arrive_cnt(&mbar[0], 2);
+        }
+        break;
+      }
+      const int w = (int)(row / a.H), r = (int)(row % a.H);
       const bool new_w = w != cur_w;
       if (new_w) { // per window: frame offsets, B = (Wh, Wl) and its DC correction
         cur_w = w;
@@ -228,6 +250,7 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
             }
         }
         tc::mma_commit(&mbar[0]);
+        mbar_arrive(&mbar[0]); // release: the row index, B and the DC correction are in place
       }
     }
   } else {
@@ -244,14 +267,17 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
     const int bar  = 2 + team;
     const int ngrp = (a.nz + 3) / 4;
     int k = 0, cur_w = -1, wpar = 1;
-    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x, ++k) {
+    for (;; ++k) {
+      wait_or_abort(&mbar[0], (uint32_t)(k & 1), abortv, a.status, 13);
+      tc::fence_after_sync();
+      const int64_t row = rowbuf[k & 1];
+      if (row >= nrows || *abortv)
+        break;
       const int w = (int)(row / a.H), r = (int)(row % a.H);
       if (w != cur_w) {
         cur_w = w;
         wpar ^= 1;
       }
-      wait_or_abort(&mbar[0], (uint32_t)(k & 1), abortv, a.status, 13);
-      tc::fence_after_sync();
       const int g0 = (team + k) & 1;
       if (g0 >= ngrp) { // nothing for this team on this row: TMEM is released at once
         tc::fence_before_sync();
@@ -322,11 +348,13 @@ template <int FMT, int N1> int launch_n1(const BandRowsArgs &a, cudaStream_t s) 
   constexpr int NTILE = W / 128;
   constexpr int RS    = XBuf<N1>::kSize > W ? XBuf<N1>::kSize : W;
   const size_t  smem  = 1024 + (size_t)NTILE * kTileBytes + 16384 + (size_t)8 * RS * 8 + (size_t)W * 8 + 128 * 4 +
-                      64 * 8 + 16 + 8;
+                      64 * 8 + 2 * 8 + 16 + 8;
   HF_CUDA(cudaFuncSetAttribute(band_rows_tc_kernel<FMT, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t nrows = (int64_t)a.nwin * a.H;
   const int     cap   = a.max_ctas > 0 ? std::min(a.max_ctas, sm_count()) : sm_count();
   const int     grid  = (int)std::min<int64_t>(nrows, cap);
+  HF_CHECK_ARG(a.row_counter != nullptr, "band rows: row counter missing");
+  HF_CUDA(cudaMemsetAsync(a.row_counter, 0, sizeof(int), s));
   band_rows_tc_kernel<FMT, N1><<<grid, kBandTcThr, smem, s>>>(a);
   note_launch();
   return launch_status("band_rows_tc_kernel");

@@ -19,6 +19,7 @@ struct BandRowsArgs {
   float         shift;       // sample offset removed before the f16 conversion (2048)
   int          *status;      // device status word (bounded waits)
   int           max_ctas;    // persistent grid size cap (SMs left to concurrent work otherwise)
+  int          *row_counter; // device int, zeroed by the launcher: CTAs take rows from it
 };
 
 bool band_rows_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes);

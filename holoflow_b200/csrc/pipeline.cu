@@ -91,6 +91,7 @@ struct hf_plan {
   float2    *wmat_plain = nullptr;
   FilterSet  set[2];          // [0] for hf_pipeline_exec and stream batches, [1] stream lookahead
   int       *status = nullptr; // device status word: nonzero when a bounded device wait expired
+  int       *row_counter = nullptr; // row queue of the persistent band pass
   void      *cov_ws = nullptr;
   bool       cov_tc = false;   // tensor-core Gram matrix (chosen form)
   bool       rows_tc = false;  // tensor-core band DFT fused with lens + row FFT (chosen form)
@@ -114,6 +115,7 @@ static void plan_free(hf_plan *p) {
     dev_free(fs.wmat);
   }
   dev_free(p->status);
+  dev_free(p->row_counter);
   if (p->cov_ws)
     cudaFree(p->cov_ws);
   p->cov_ws = nullptr;
@@ -197,6 +199,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     br.wmat = wmat, br.wmat_stride = wstride, br.lens = p->lens, br.out = p->band;
     br.out_win = win_px, br.out_plane = p->P, br.out_row = d.width, br.nwin = nwin, br.shift = 2048.f;
     br.status = p->status, br.max_ctas = std::max(1, sm_count() - reserve_sms);
+    br.row_counter = p->row_counter;
     int rec = p->timer.begin(s, ST_BAND_ROWS);
     HF_TRY(launch_band_rows_tc(br, d.input_dtype, s));
     p->timer.end(s, rec);
@@ -366,7 +369,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       if ((rc = launch_band_matrix(nullptr, 1, T, 0, d.z_begin, d.z_end, p->wmat_plain, stream)))
         break;
     }
-    if ((rc = dev_alloc(&p->status, 1, p->bytes)))
+    if ((rc = dev_alloc(&p->status, 1, p->bytes)) || (rc = dev_alloc(&p->row_counter, 1, p->bytes)))
       break;
     if ((rc = cuda_status(cudaMemsetAsync(p->status, 0, sizeof(int), stream), "status reset")))
       break;

@@ -143,13 +143,26 @@ __device__ __forceinline__ void tma_prefetch_desc(const void *tmap) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
 }
 
-// Waits for phase `parity` of `mbar` with an iteration bound; on expiry records `code` in the
-// status word (first writer wins) and returns false instead of hanging.
+// Device time in nanoseconds (the global timer).
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for phase `parity` of `mbar`, bounded both by iterations and by kWaitNs of device time
+// (a try_wait may suspend, so an iteration count alone can take very long); on expiry records
+// `code` in the status word (first writer wins) and returns false instead of hanging.
 constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr uint64_t kWaitNs    = 2000000000ull; // 2 s
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *mbar, uint32_t parity, int *status, int code) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
     if (mbar_try_wait(mbar, parity))
       return true;
+    if ((i & 255u) == 255u && globaltimer_ns() - t0 > kWaitNs)
+      break;
+  }
   if (status)
     atomicCAS(status, 0, code);
   return false;
