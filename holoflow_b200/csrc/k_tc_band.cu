@@ -62,13 +62,21 @@ __device__ __forceinline__ void mbar_arrive_cnt(uint64_t *mbar, uint32_t cnt) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(mbar)), "r"(cnt) : "memory");
 }
 
-template <int FMT> struct GroupLoad; // 32 consecutive samples of one frame
+// 32 consecutive samples of one frame: `raw` issues the 16-byte loads of their packed bytes,
+// `unpack` turns the packed words into the 32 sample values.  Splitting the two lets the loaders
+// keep the next round's loads in flight while they unpack the current one.
+template <int FMT> struct GroupLoad;
 template <> struct GroupLoad<HF_MONO12P> {
-  static constexpr int kBytes = 48;
-  __device__ static void load(const uint8_t *src, uint32_t (&v)[32]) {
+  static constexpr int kBytes = 48, kWords = 12, kPerRound = 4; // groups in flight per thread
+  __device__ static void raw(const uint8_t *src, uint32_t (&w)[kWords]) {
     const uint4 *s = reinterpret_cast<const uint4 *>(src);
-    const uint4  a = __ldg(s), b = __ldg(s + 1), c = __ldg(s + 2);
-    const uint32_t w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const uint4 a = __ldg(s + i);
+      w[4 * i] = a.x, w[4 * i + 1] = a.y, w[4 * i + 2] = a.z, w[4 * i + 3] = a.w;
+    }
+  }
+  __device__ static void unpack(const uint32_t (&w)[kWords], uint32_t (&v)[32]) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       uint32_t p[8];
@@ -80,18 +88,20 @@ template <> struct GroupLoad<HF_MONO12P> {
   }
 };
 template <> struct GroupLoad<HF_U16> {
-  static constexpr int kBytes = 64;
-  __device__ static void load(const uint8_t *src, uint32_t (&v)[32]) {
+  static constexpr int kBytes = 64, kWords = 16, kPerRound = 2;
+  __device__ static void raw(const uint8_t *src, uint32_t (&w)[kWords]) {
     const uint4 *s = reinterpret_cast<const uint4 *>(src);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint4    a    = __ldg(s + q);
-      const uint32_t w[4] = {a.x, a.y, a.z, a.w};
+    for (int i = 0; i < 4; ++i) {
+      const uint4 a = __ldg(s + i);
+      w[4 * i] = a.x, w[4 * i + 1] = a.y, w[4 * i + 2] = a.z, w[4 * i + 3] = a.w;
+    }
+  }
+  __device__ static void unpack(const uint32_t (&w)[kWords], uint32_t (&v)[32]) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        v[8 * q + 2 * i]     = w[i] & 0xFFFFu;
-        v[8 * q + 2 * i + 1] = w[i] >> 16;
-      }
+    for (int i = 0; i < 16; ++i) {
+      v[2 * i]     = w[i] & 0xFFFFu;
+      v[2 * i + 1] = w[i] >> 16;
     }
   }
 };
@@ -191,34 +201,48 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
         named_bar(1, kLoaders); // frame offsets visible to every loader
       // A: tile j = pixels [128 j, 128 j + 128) of row r; element (m, t) at
       //    (m/64)*8192 + (t/8)*1024 + (t%8)*128 + ((m%64/8) ^ (t%8))*16 + (m%8)*2.
-      //    Loads of two tiles are issued before any of them is unpacked.
-      for (int j0 = 0; j0 < NTILE; j0 += 2) {
-        uint32_t v[4][32];
+      //    Work item u of a round is one 32-sample group (frame t, pixels 32 grp ..) of tile j;
+      //    the packed words of round rd + 1 are loaded before round rd is unpacked.
+      {
+        using GL            = GroupLoad<FMT>;
+        constexpr int U     = GL::kPerRound;               // groups per thread per round
+        constexpr int TPR   = U / 2;                       // tiles per round
+        constexpr int NR    = (NTILE + TPR - 1) / TPR;     // rounds per row
+        uint32_t      raw[2][U][GL::kWords];
+        auto load_round = [&](int rd, uint32_t (&dst)[U][GL::kWords]) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int j = j0 + (u >> 1), item = tid + (u & 1) * kLoaders;
-          const int t = item >> 2, grp = item & 3;
-          const int64_t px0 = (int64_t)r * W + 128 * j + 32 * grp;
-          if (j < NTILE)
-            GroupLoad<FMT>::load(a.ring.base + foff[t] + px0 * GroupLoad<FMT>::kBytes / 32, v[u]);
-        }
+          for (int u = 0; u < U; ++u) {
+            const int j = rd * TPR + (u >> 1), item = tid + (u & 1) * kLoaders;
+            const int t = item >> 2, grp = item & 3;
+            if (j < NTILE)
+              GL::raw(a.ring.base + foff[t] + ((int64_t)r * W + 128 * j + 32 * grp) * GL::kBytes / 32, dst[u]);
+          }
+        };
+        load_round(0, raw[0]);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int j = j0 + (u >> 1), item = tid + (u & 1) * kLoaders;
-          const int t = item >> 2, grp = item & 3;
-          if (j >= NTILE)
-            continue;
-          uint8_t *tile = sA + j * kTileBytes;
+        for (int rd = 0; rd < NR; ++rd) {
+          if (rd + 1 < NR)
+            load_round(rd + 1, raw[(rd + 1) & 1]);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int m0 = 32 * grp + 8 * q;
-            __half2 h[4];
+          for (int u = 0; u < U; ++u) {
+            const int j = rd * TPR + (u >> 1), item = tid + (u & 1) * kLoaders;
+            const int t = item >> 2, grp = item & 3;
+            if (j >= NTILE)
+              continue;
+            uint32_t v[32];
+            GL::unpack(raw[rd & 1][u], v);
+            uint8_t *tile = sA + j * kTileBytes;
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-              h[i] = __floats2half2_rn((float)v[u][8 * q + 2 * i] - a.shift, (float)v[u][8 * q + 2 * i + 1] - a.shift);
-            const int chunk = (m0 & 63) >> 3;
-            uint8_t  *dst   = tile + (m0 >> 6) * 8192 + (t >> 3) * 1024 + (t & 7) * 128 + ((chunk ^ (t & 7)) << 4);
-            *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(h);
+            for (int q = 0; q < 4; ++q) {
+              const int m0 = 32 * grp + 8 * q;
+              __half2 h[4];
+#pragma unroll
+              for (int i = 0; i < 4; ++i)
+                h[i] = __floats2half2_rn((float)v[8 * q + 2 * i] - a.shift, (float)v[8 * q + 2 * i + 1] - a.shift);
+              const int chunk = (m0 & 63) >> 3;
+              uint8_t  *dst   = tile + (m0 >> 6) * 8192 + (t >> 3) * 1024 + (t & 7) * 128 + ((chunk ^ (t & 7)) << 4);
+              *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(h);
+            }
           }
         }
       }
