@@ -192,15 +192,7 @@ __global__ void fresnel_lens_kernel(float2 *lens, int W, int H, float lambda, fl
   const int row = blockIdx.y * blockDim.y + threadIdx.y;
   if (col >= W || row >= H)
     return;
-  const int   size  = W > H ? W : H;
-  const float half  = (float)size / 2.0f;
-  const float x     = __fmul_rn(__fsub_rn((float)(col + (size - W) / 2), half), dx);
-  const float y     = __fmul_rn(__fsub_rn((float)(row + (size - H) / 2), half), dx);
-  const float k     = __fdiv_rn(CUDART_PI_F, __fmul_rn(lambda, z));
-  const float phase = __fmul_rn(k, __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
-  float       s, c;
-  sincosf(phase, &s, &c);
-  lens[(int64_t)row * W + col] = make_float2(c, s);
+  lens[(int64_t)row * W + col] = fresnel_lens_value(col, row, W, H, fresnel_lens_k(lambda, z), dx);
 }
 
 __device__ float as_filter_weight(int x, int y, int W, int H, AsFilter f) {

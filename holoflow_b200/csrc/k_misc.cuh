@@ -28,6 +28,24 @@ int launch_mean_axis(const void *in, int in_dtype, int64_t outer, int64_t n, int
 int launch_band_moments(const void *planes, int in_dtype, int nz, int64_t P, const MomentWeights &w,
                         int mask, float *out, cudaStream_t s);
 int launch_fresnel_lens(float2 *lens, int W, int H, float lambda, float z, float dx, cudaStream_t s);
+
+// One value of the Fresnel quadratic-phase lens (fresnel_diffraction.cu:326-341): centred
+// coordinates x = ((col + (S - W)/2) - S/2) dx and y likewise, S = max(W, H), phase
+// pi / (lambda z) (x^2 + y^2), each step rounded in float32 as the reference evaluates it.
+// The lens table and the fused band pass both call this, so their values agree bit for bit.
+__device__ __forceinline__ float fresnel_lens_k(float lambda, float z) {
+  return __fdiv_rn(3.14159265358979323846f, __fmul_rn(lambda, z));
+}
+__device__ __forceinline__ float2 fresnel_lens_value(int col, int row, int W, int H, float k, float dx) {
+  const int   size  = W > H ? W : H;
+  const float half  = (float)size / 2.0f;
+  const float x     = __fmul_rn(__fsub_rn((float)(col + (size - W) / 2), half), dx);
+  const float y     = __fmul_rn(__fsub_rn((float)(row + (size - H) / 2), half), dx);
+  const float phase = __fmul_rn(k, __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
+  float       s, c;
+  sincosf(phase, &s, &c);
+  return make_float2(c, s);
+}
 int launch_as_tf(float2 *tf, int W, int H, float lambda, float z, float dx, int use_filter,
                  const AsFilter &f, cudaStream_t s);
 

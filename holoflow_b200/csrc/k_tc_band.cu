@@ -22,6 +22,7 @@
 #include <cuda_fp16.h>
 
 #include "fft_core.cuh"
+#include "k_misc.cuh"
 #include "k_tc_band.cuh"
 #include "tc_common.cuh"
 
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
   volatile int  *abortv = abort_flag;
   constexpr uint32_t idesc = tc::idesc_f16(128, 64, true, false);
   const int64_t nrows = (int64_t)a.nwin * a.H;
+  const float   lens_k = a.lens != nullptr ? fresnel_lens_k(a.lambda, a.z) : 0.f;
 
   if (tid < kLoaders) {
     // ------------------------------------------------------------------ loader / MMA warps
@@ -310,10 +312,13 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
           mbar_arrive(&mbar[1]);
         continue;
       }
+      // the lens values of this lane's pixels (same expression as the lens table, so the same
+      // values), computed here rather than loaded: no global-load wait at the start of a row
       float2 L[NTILE];
 #pragma unroll
       for (int j = 0; j < NTILE; ++j)
-        L[j] = a.lens != nullptr ? __ldg(a.lens + (int64_t)r * W + 128 * j + 32 * q + lane) : make_float2(1.f, 0.f);
+        L[j] = a.lens != nullptr ? fresnel_lens_value(128 * j + 32 * q + lane, r, W, a.H, lens_k, a.dx)
+                                 : make_float2(1.f, 0.f);
       const float *cs = colsum + wpar * 64;
       for (int g = g0; g < ngrp; g += 2) {
         uint32_t v[NTILE][8];

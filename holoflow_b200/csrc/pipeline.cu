@@ -197,6 +197,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     BandRowsArgs br{};
     br.ring = fr, br.T = d.frames, br.H = d.height, br.W = d.width, br.nz = p->nz;
     br.wmat = wmat, br.wmat_stride = wstride, br.lens = p->lens, br.out = p->band;
+    br.lambda = d.lambda, br.z = d.z, br.dx = d.pitch;
     br.out_win = win_px, br.out_plane = p->P, br.out_row = d.width, br.nwin = nwin, br.shift = 2048.f;
     br.status = p->status, br.max_ctas = std::max(1, sm_count() - reserve_sms);
     br.row_counter = p->row_counter;
