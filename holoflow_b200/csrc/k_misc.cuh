@@ -32,18 +32,35 @@ int launch_fresnel_lens(float2 *lens, int W, int H, float lambda, float z, float
 // One value of the Fresnel quadratic-phase lens (fresnel_diffraction.cu:326-341): centred
 // coordinates x = ((col + (S - W)/2) - S/2) dx and y likewise, S = max(W, H), phase
 // pi / (lambda z) (x^2 + y^2), each step rounded in float32 as the reference evaluates it.
-// The lens table and the fused band pass both call this, so their values agree bit for bit.
+// The lens table evaluates it with sincosf; the fused band pass evaluates the same float32 phase
+// with cis_reduced below.
 __device__ __forceinline__ float fresnel_lens_k(float lambda, float z) {
   return __fdiv_rn(3.14159265358979323846f, __fmul_rn(lambda, z));
 }
+__device__ __forceinline__ float fresnel_lens_phase(int col, int row, int W, int H, float k, float dx) {
+  const int   size = W > H ? W : H;
+  const float half = (float)size / 2.0f;
+  const float x    = __fmul_rn(__fsub_rn((float)(col + (size - W) / 2), half), dx);
+  const float y    = __fmul_rn(__fsub_rn((float)(row + (size - H) / 2), half), dx);
+  return __fmul_rn(k, __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
+}
 __device__ __forceinline__ float2 fresnel_lens_value(int col, int row, int W, int H, float k, float dx) {
-  const int   size  = W > H ? W : H;
-  const float half  = (float)size / 2.0f;
-  const float x     = __fmul_rn(__fsub_rn((float)(col + (size - W) / 2), half), dx);
-  const float y     = __fmul_rn(__fsub_rn((float)(row + (size - H) / 2), half), dx);
-  const float phase = __fmul_rn(k, __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
-  float       s, c;
-  sincosf(phase, &s, &c);
+  float s, c;
+  sincosf(fresnel_lens_phase(col, row, W, H, k, dx), &s, &c);
+  return make_float2(c, s);
+}
+
+// exp(i phase) for |phase| < 256 * 2 pi: Cody-Waite reduction to [-pi, pi] with 2 pi split into
+// 6.28125 (8 significant bits, so n * 6.28125 is exact for n < 256 and the first subtraction is
+// exact) plus the float32 remainder 2 pi - 6.28125, then the hardware sine / cosine, whose
+// absolute error on [-pi, pi] is below 5e-7.  Used where the phase is evaluated per element inside
+// a hot kernel (the chosen form's band pass), instead of the lens table's sincosf.
+__device__ __forceinline__ float2 cis_reduced(float phase) {
+  const float n = rintf(phase * 0.159154943091895336f); // 1 / (2 pi)
+  float       r = fmaf(-n, 6.28125f, phase);
+  r             = fmaf(-n, 1.93530717958647692e-3f, r);
+  float s, c;
+  __sincosf(r, &s, &c);
   return make_float2(c, s);
 }
 int launch_as_tf(float2 *tf, int W, int H, float lambda, float z, float dx, int use_filter,

@@ -312,12 +312,13 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
           mbar_arrive(&mbar[1]);
         continue;
       }
-      // the lens values of this lane's pixels (same expression as the lens table, so the same
-      // values), computed here rather than loaded: no global-load wait at the start of a row
+      // the lens values of this lane's pixels: the lens table's float32 phase, turned into
+      // exp(i phase) here (reduced argument, hardware sine/cosine) rather than loaded, so a row
+      // starts without a global-load wait
       float2 L[NTILE];
 #pragma unroll
       for (int j = 0; j < NTILE; ++j)
-        L[j] = a.lens != nullptr ? fresnel_lens_value(128 * j + 32 * q + lane, r, W, a.H, lens_k, a.dx)
+        L[j] = a.lens != nullptr ? cis_reduced(fresnel_lens_phase(128 * j + 32 * q + lane, r, W, a.H, lens_k, a.dx))
                                  : make_float2(1.f, 0.f);
       const float *cs = colsum + wpar * 64;
       for (int g = g0; g < ngrp; g += 2) {

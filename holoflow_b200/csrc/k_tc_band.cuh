@@ -13,7 +13,7 @@ struct BandRowsArgs {
   const float2 *wmat;        // [nwin][T][nz] filter+DFT matrices (float32)
   int64_t       wmat_stride; // complex elements between windows (0 = shared)
   const float2 *lens;        // non-null: multiply by the Fresnel lens of (lambda, z, dx), computed
-                             // in the kernel with the lens table's own expression
+                             // in the kernel from the lens table's float32 phase
   float         lambda, z, dx;
   float2       *out;         // row-transformed band planes [nwin][nz][H][W]
   int64_t       out_win, out_plane, out_row;
