@@ -364,6 +364,235 @@ __global__ void __launch_bounds__(128) cov_tc_i8_kernel(FrameRing ring, int64_t 
   }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Shared-frame variant for T = 64 and a hop that is a multiple of 8 (8..32): a CTA owns a group of
+// up to four consecutive windows, i.e. the frames w0*hop + [0, F) with F = 64 + 3 hop, and stages
+// every frame of the group once per 128-pixel tile instead of once per window.
+//  - Operand rows come in 8-frame pairs of swizzle atoms, [h of frames 8p..8p+7][l of the same
+//    frames], so window wl's 128 operand rows [h;l] are the 16 consecutive atoms from pair
+//    wl*hop/8: one descriptor offset selects them, and its M = N = 128 kind::i8 MMAs accumulate
+//    D_wl into its own 128 TMEM columns (512 columns for four windows, one CTA per SM).
+//  - Packed samples travel global -> shared through a ring of per-thread cp.async copies, D tiles
+//    deep; each thread unpacks exactly the bytes it copied, so no barrier guards the raw ring.
+//  - The split needs no pixel value: for x in [0, 4096), x - 2048 = 64 ((x >> 6) - 32) + (x & 63),
+//    so the 6-bit fields of the packed stream are masked out in 16-bit lanes, packed to bytes with
+//    byte permutes and re-centred with one byte-wise subtraction; frame sums are 64 S(x >> 6) +
+//    S(x & 63) from byte dot products.  8-bit samples use x - 128 = 64 ((x >> 6) - 2) + (x & 63).
+// Operand row r of a window holds frame 8 (r / 16) + r % 8, kind h when (r / 8) is even; the h-row
+// and l-row of a frame sit 8 lanes apart in one warp and are folded with a shuffle before the
+// integer atomics.
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// 24 packed bits (two 12-bit pixels p0 | p1 << 12) -> 16-bit lanes of their low and high 6 bits
+__device__ __forceinline__ void split_pair12(uint32_t t, uint32_t &lo, uint32_t &hi) {
+  lo = (t & 0x3Fu) | ((t << 4) & 0x003F0000u);
+  hi = ((t >> 6) & 0x3Fu) | ((t >> 2) & 0x003F0000u);
+}
+
+template <int FMT, int HOP8> struct GroupCov {
+  static constexpr int F    = 64 + 24 * HOP8;              // frames of a four-window group
+  static constexpr int NT   = 4 * F;                       // one (frame, 32-pixel run) per thread
+  static constexpr int RB   = FMT == HF_MONO12P ? 48 : 32; // packed bytes of a 32-pixel run
+  static constexpr int D    = F <= 112 ? 4 : 3;            // raw ring depth (tiles)
+  static constexpr int S    = F <= 136 ? 3 : 2;            // operand stages
+  static constexpr int STG  = 256 * F;                     // 2F rows x 128 B
+  static constexpr size_t smem = 1024 + (size_t)S * STG + (size_t)D * NT * RB + S * 8 + 16;
+};
+
+template <int FMT, int HOP8>
+__global__ void __launch_bounds__(GroupCov<FMT, HOP8>::NT, 1)
+    cov_tc_group_kernel(FrameRing ring, int64_t P, int nwin, uint32_t ncols, unsigned long long *acc,
+                        unsigned long long *sums, int *status) {
+  using G                = GroupCov<FMT, HOP8>;
+  constexpr int T        = 64;
+  constexpr int HOP      = 8 * HOP8;
+  constexpr uint32_t kHS = FMT == HF_MONO12P ? 0x20202020u : 0x02020202u; // shift / 64 per byte
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t  *raw   = smem + G::S * G::STG;
+  uint64_t *mbar  = reinterpret_cast<uint64_t *>(raw + (size_t)G::D * G::NT * G::RB);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + G::S);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int w0  = 4 * blockIdx.y;
+  const int g   = min(4, nwin - w0);   // windows of this group
+  const int Fg  = T + (g - 1) * HOP;   // frames of this group
+  if (tid == 0) {
+    for (int s = 0; s < G::S; ++s)
+      tc::mbar_init(&mbar[s], 1);
+    tc::mbar_fence_init();
+  }
+  if (warp == 0)
+    tc::tmem_alloc(tslot, ncols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *tslot;
+  constexpr uint32_t idesc = tc::idesc_i8(128, 128, false, false);
+
+  const int      f      = tid >> 2, grp = tid & 3;
+  const bool     active = f < Fg;
+  const uint8_t *fbase  = active ? ring.frame(w0, f) : nullptr;
+  uint8_t       *myraw  = raw + (size_t)tid * G::RB;
+  // this thread's rows in the stage: frame f -> pair f / 8, row f % 8 of the pair's h and l atoms
+  const int rr = f & 7, pr = f >> 3;
+
+  const int64_t ntiles = (P + kTcPX - 1) / kTcPX;
+  auto issue = [&](int64_t tile, int slot) {
+    const int64_t p = tile * kTcPX + grp * 32;
+    if (active && tile < ntiles && p < P) {
+      const uint8_t *src = fbase + p * TcBpp<FMT>::num / TcBpp<FMT>::den;
+      uint8_t       *dst = myraw + (size_t)slot * G::NT * G::RB;
+#pragma unroll
+      for (int i = 0; i < G::RB / 16; ++i)
+        cp_async16(dst + 16 * i, src + 16 * i);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int d = 0; d < G::D - 1; ++d)
+    issue(blockIdx.x + (int64_t)d * gridDim.x, d);
+
+  uint32_t sx = 0u, sl = 0u; // sums of the high and low 6-bit fields
+  int      nj = 0;
+  bool     ok = true;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++nj) {
+    const int s = nj % G::S;
+    issue(tile + (int64_t)(G::D - 1) * gridDim.x, (nj + G::D - 1) % G::D);
+    bool w_ok = true;
+    if (nj >= G::S)
+      w_ok = tc::mbar_wait_bounded(&mbar[s], (uint32_t)((nj / G::S) - 1) & 1u, status, 5);
+    cp_async_wait<G::D - 1>();
+    const bool valid = active && tile * kTcPX + grp * 32 < P;
+    if (w_ok && active) {
+      uint32_t hw[8], lw[8];
+      if (valid) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(myraw + (size_t)(nj % G::D) * G::NT * G::RB);
+        uint32_t     wv[G::RB / 4];
+#pragma unroll
+        for (int i = 0; i < G::RB / 16; ++i) {
+          const uint4 v = src[i];
+          wv[4 * i] = v.x, wv[4 * i + 1] = v.y, wv[4 * i + 2] = v.z, wv[4 * i + 3] = v.w;
+        }
+        if constexpr (FMT == HF_MONO12P) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) { // 8 pixels from 3 words
+            const uint32_t a0 = wv[3 * q], a1 = wv[3 * q + 1], a2 = wv[3 * q + 2];
+            uint32_t       l0, h0, l1, h1, l2, h2, l3, h3;
+            split_pair12(a0, l0, h0);
+            split_pair12(__funnelshift_r(a0, a1, 24), l1, h1);
+            split_pair12(__funnelshift_r(a1, a2, 16), l2, h2);
+            split_pair12(a2 >> 8, l3, h3);
+            lw[2 * q]     = __byte_perm(l0, l1, 0x6420);
+            lw[2 * q + 1] = __byte_perm(l2, l3, 0x6420);
+            hw[2 * q]     = __byte_perm(h0, h1, 0x6420);
+            hw[2 * q + 1] = __byte_perm(h2, h3, 0x6420);
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            lw[i] = wv[i] & 0x3F3F3F3Fu;
+            hw[i] = (wv[i] >> 6) & 0x03030303u;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          sx    = __dp4a(hw[i], 0x01010101u, sx);
+          sl    = __dp4a(lw[i], 0x01010101u, sl);
+          hw[i] = __vsub4(hw[i], kHS);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          hw[i] = lw[i] = 0u;
+      }
+      uint8_t *hrow = smem + s * G::STG + pr * 2048 + rr * 128;
+#pragma unroll
+      for (int hc = 0; hc < 2; ++hc) {
+        const int c = 2 * grp + hc;
+        *reinterpret_cast<uint4 *>(hrow + ((c ^ rr) << 4)) =
+            make_uint4(hw[4 * hc], hw[4 * hc + 1], hw[4 * hc + 2], hw[4 * hc + 3]);
+        *reinterpret_cast<uint4 *>(hrow + 1024 + ((c ^ rr) << 4)) =
+            make_uint4(lw[4 * hc], lw[4 * hc + 1], lw[4 * hc + 2], lw[4 * hc + 3]);
+      }
+    }
+    tc::fence_proxy_async_smem();
+    ok = __syncthreads_and(w_ok) != 0;
+    if (!ok)
+      break;
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint8_t *st = smem + s * G::STG;
+      for (int wl = 0; wl < g; ++wl) {
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+          const uint64_t d = tc::sw128_desc(tc::smem_u32(st + wl * HOP8 * 2048 + ks * 32), 16, 1024);
+          tc::mma_i8(tbase + 128 * wl, d, d, idesc, (nj > 0 || ks > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(&mbar[s]);
+    }
+  }
+  cp_async_wait<0>(); // no copy may land in shared memory after the CTA has left
+  if (nj > 0 && ok) {
+    const int last = nj - 1;
+    ok = tc::mbar_wait_bounded(&mbar[last % G::S], (uint32_t)(last / G::S) & 1u, status, 6);
+  }
+  ok = __syncthreads_and(ok) != 0;
+  tc::fence_after_sync();
+
+  // frame sums: the four runs of a frame are adjacent lanes; each window holding frame f gets it
+  unsigned long long fs = 64ull * sx + sl;
+  fs += __shfl_xor_sync(0xFFFFFFFFu, fs, 1);
+  fs += __shfl_xor_sync(0xFFFFFFFFu, fs, 2);
+  if (active && grp == 0)
+    for (int wl = 0; wl < g; ++wl) {
+      const int t = f - wl * HOP;
+      if (t >= 0 && t < T)
+        atomicAdd(&sums[(int64_t)(w0 + wl) * T + t], fs);
+    }
+
+  constexpr int NQ = G::NT / 128; // complete warp quads: each reads all 128 TMEM lanes
+  if (nj > 0 && ok && warp < 4 * NQ) {
+    const int       q      = warp & 3;
+    const int       r      = 32 * q + lane;
+    const bool      is_h   = ((r >> 3) & 1) == 0;
+    const int       a      = 8 * (r >> 4) + (r & 7);
+    const long long wh     = is_h ? 4096 : 64, wlw = is_h ? 64 : 1;
+    for (int wl = warp >> 2; wl < g; wl += NQ) {
+      unsigned long long *aw = acc + (int64_t)(w0 + wl) * T * T + a * T;
+#pragma unroll
+      for (int cb = 0; cb < 4; ++cb) {
+        uint32_t v[32];
+        tc::tmem_ld32(tbase + ((uint32_t)(32 * q) << 16) + 128 * wl + 32 * cb, v);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            // columns 16 half + c (h of frame b) and 16 half + 8 + c (l of frame b)
+            long long e = wh * (long long)(int)v[16 * half + c] + wlw * (long long)(int)v[16 * half + 8 + c];
+            e += __shfl_xor_sync(0xFFFFFFFFu, e, 8);
+            if (is_h)
+              atomicAdd(&aw[16 * cb + 8 * half + c], (unsigned long long)e);
+          }
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tbase, ncols);
+  }
+}
+
 // int64 accumulator -> float64 Gram with the shift undone exactly.
 __global__ void cov_i8_finalize_kernel(const unsigned long long *acc, const unsigned long long *sums, int T,
                                        int64_t P, long long shift, double *gram) {
@@ -378,12 +607,19 @@ __global__ void cov_i8_finalize_kernel(const unsigned long long *acc, const unsi
   gram[(int64_t)w * T * T + e] = (double)g;
 }
 
+int launch_i8_finalize(const unsigned long long *acc, const unsigned long long *sums, int T, int64_t P,
+                       long long shift, int nwin, double *gram, cudaStream_t s) {
+  cov_i8_finalize_kernel<<<dim3((T * T + 255) / 256, nwin), 256, 0, s>>>(acc, sums, T, P, shift, gram);
+  note_launch();
+  return launch_status("cov_i8_finalize_kernel");
+}
+
 template <int FMT, int T>
 int launch_tc(const FrameRing &ring, int64_t P, int nwin, void *ws, double *gram, int *status,
               cudaStream_t s) {
   const size_t smem = 1024 + (size_t)kTcStages * 2 * T * 128 + kTcStages * 8 + 8 + T * 8;
   const int64_t ntiles = (P + kTcPX - 1) / kTcPX;
-  int ctas = (int)std::max<int64_t>(1, std::min<int64_t>((3LL * sm_count() + nwin - 1) / nwin, ntiles));
+  const int ctas = (int)std::max<int64_t>(1, std::min<int64_t>(3LL * sm_count() / nwin, ntiles));
   CovArgs a;
   a.ring    = ring;
   a.T       = T;
@@ -409,7 +645,9 @@ int launch_tc_i8(const FrameRing &ring, int64_t P, int nwin, void *ws, double *g
   // at most ~256K pixels per CTA keeps every int32 accumulator entry below 63*63*256K < 2^31
   const int64_t min_ctas = (P + (1 << 18) - 1) >> 18;
   const int     per_sm   = T == 64 ? 3 : 1;
-  int ctas = (int)std::max<int64_t>(min_ctas, std::min<int64_t>(((int64_t)per_sm * sm_count() + nwin - 1) / nwin, ntiles));
+  // one wave: the CTAs of all windows fit the SMs at once (a partial second wave doubles the time)
+  const int ctas = (int)std::max<int64_t>(
+      min_ctas, std::min<int64_t>(std::max<int64_t>(1, (int64_t)per_sm * sm_count() / nwin), ntiles));
   auto *acc  = reinterpret_cast<unsigned long long *>(ws);
   auto *sums = acc + (size_t)nwin * T * T;
   HF_CUDA(cudaMemsetAsync(acc, 0, ((size_t)nwin * T * T + (size_t)nwin * T) * sizeof(unsigned long long), s));
@@ -418,10 +656,42 @@ int launch_tc_i8(const FrameRing &ring, int64_t P, int nwin, void *ws, double *g
                                                                status);
   note_launch();
   HF_TRY(launch_status("cov_tc_i8_kernel"));
-  cov_i8_finalize_kernel<<<dim3((T * T + 255) / 256, nwin), 256, 0, s>>>(acc, sums, T, P,
-                                                                        FMT == HF_U8 ? 128 : 2048, gram);
+  return launch_i8_finalize(acc, sums, T, P, FMT == HF_U8 ? 128 : 2048, nwin, gram, s);
+}
+
+template <int FMT, int HOP8>
+int launch_tc_group(const FrameRing &ring, int64_t P, int nwin, void *ws, double *gram, int *status,
+                    cudaStream_t s) {
+  using G               = GroupCov<FMT, HOP8>;
+  constexpr int T       = 64;
+  const int     ngroups = (nwin + 3) / 4;
+  const int64_t ntiles  = (P + kTcPX - 1) / kTcPX;
+  const int64_t min_ctas = (P + (1 << 18) - 1) >> 18; // int32 accumulator bound, as above
+  // one CTA per SM (it holds the whole TMEM), the SMs split evenly between the window groups
+  const int ctas = (int)std::max<int64_t>(
+      min_ctas, std::min<int64_t>(std::max<int64_t>(1, (int64_t)sm_count() / ngroups), ntiles));
+  const uint32_t ncols = nwin >= 3 ? 512u : 256u;
+  auto *acc  = reinterpret_cast<unsigned long long *>(ws);
+  auto *sums = acc + (size_t)nwin * T * T;
+  HF_CUDA(cudaMemsetAsync(acc, 0, ((size_t)nwin * T * T + (size_t)nwin * T) * sizeof(unsigned long long), s));
+  HF_CUDA(cudaFuncSetAttribute(cov_tc_group_kernel<FMT, HOP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)G::smem));
+  cov_tc_group_kernel<FMT, HOP8><<<dim3(ctas, ngroups), G::NT, G::smem, s>>>(ring, P, nwin, ncols, acc, sums,
+                                                                              status);
   note_launch();
-  return launch_status("cov_i8_finalize_kernel");
+  HF_TRY(launch_status("cov_tc_group_kernel"));
+  return launch_i8_finalize(acc, sums, T, P, FMT == HF_U8 ? 128 : 2048, nwin, gram, s);
+}
+
+template <int FMT>
+int launch_group_hop(const FrameRing &ring, int64_t P, int nwin, void *ws, double *gram, int *status,
+                     cudaStream_t s) {
+  switch (ring.hop / 8) {
+  case 1: return launch_tc_group<FMT, 1>(ring, P, nwin, ws, gram, status, s);
+  case 2: return launch_tc_group<FMT, 2>(ring, P, nwin, ws, gram, status, s);
+  case 3: return launch_tc_group<FMT, 3>(ring, P, nwin, ws, gram, status, s);
+  default: return launch_tc_group<FMT, 4>(ring, P, nwin, ws, gram, status, s);
+  }
 }
 
 } // namespace
@@ -443,6 +713,11 @@ bool cov_tc_supported(int fmt, int T, int64_t P, int64_t frame_bytes) {
 int launch_covariance_tc(const FrameRing &ring, int fmt, int T, int64_t P, int nwin, void *ws,
                          double *gram, int *status, cudaStream_t s) {
   HF_CHECK_ARG(cov_tc_supported(fmt, T, P, ring.frame_bytes), "tensor-core covariance: unsupported shape");
+  // overlapping 64-frame windows on an 8-frame grid: stage each frame once per window group
+  if ((fmt == HF_MONO12P || fmt == HF_U8) && T == 64 && nwin >= 2 && ring.hop >= 8 && ring.hop <= 32 &&
+      ring.hop % 8 == 0)
+    return fmt == HF_MONO12P ? launch_group_hop<HF_MONO12P>(ring, P, nwin, ws, gram, status, s)
+                             : launch_group_hop<HF_U8>(ring, P, nwin, ws, gram, status, s);
   // samples of at most 12 bits: exact int8 split; 16-bit samples: f16 operands
   if (fmt == HF_MONO12P)
     return T == 64 ? launch_tc_i8<HF_MONO12P, 64>(ring, P, nwin, ws, gram, status, s)

@@ -126,6 +126,46 @@ def test_chosen_form_tensor_core_gram(cuda, T, H, W):
     assert np.array_equal(g, g.T)
 
 
+@pytest.mark.parametrize("hop,nwin,dtype,first,H", [
+    (16, 8, "mono12p", 0, 128), (16, 5, "mono12p", 37, 128), (8, 2, "mono12p", 3, 128),
+    (24, 3, "mono12p", 11, 128), (32, 6, "mono12p", 50, 128), (16, 7, "u8", 9, 128),
+    (8, 4, "u8", 0, 128), (16, 8, "mono12p", 5, 512)])
+def test_chosen_form_grouped_gram(cuda, hop, nwin, dtype, first, H):
+    """Batches of overlapping 64-frame windows on an 8-frame hop grid share each staged frame
+    between the windows of a group of four; every window's Gram matrix stays the exact integer
+    Gram of its own frames, for full and partial groups, 12- and 8-bit samples, and windows that
+    wrap around the end of the frame ring."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    T, W = 64, H
+    n = T + hop * (nwin - 1)
+    rng = np.random.default_rng(hop * 100 + nwin)
+    top = 4096 if dtype == "mono12p" else 256
+    frames = rng.integers(0, top, size=(n, H * W)).astype(np.uint16)
+    frames[0, :] = top - 1  # saturated and zero frames exercise the extreme fields
+    frames[1, :] = 0
+    # ring slot (first + f) % n holds window frame f
+    slots = (first + np.arange(n)) % n
+    ring_np = np.empty_like(frames)
+    ring_np[slots] = frames
+    if dtype == "mono12p":
+        ring = torch.from_numpy(O.pack12(ring_np.reshape(-1))).to(cuda)
+        in_dtype = hf.HF_MONO12P
+    else:
+        ring = torch.from_numpy(ring_np.astype(np.uint8).reshape(-1)).to(cuda)
+        in_dtype = hf.HF_U8
+    cfg = pl.PipelineConfig(height=H, width=W, frames=T, hop=hop, z_begin=4, z_end=32, fs=67e3, z=0.25,
+                            clutter_rank=4, form=hf.HF_FORM_CHOSEN, max_batch=nwin, input_dtype=in_dtype)
+    p = pl.Pipeline(cfg)
+    p.run(ring, n, first, nwin)
+    assert p.status() == 0
+    for w in range(nwin):
+        gram, _ = p.inspect(w)
+        X = frames[w * hop:w * hop + T].astype(np.float64)
+        assert np.array_equal(gram.cpu().numpy(), X @ X.T), w
+
+
 @pytest.mark.parametrize("H,W,nwin", [(256, 256, 3), (512, 512, 2), (1024, 1024, 2)])
 def test_chosen_form_fresnel_vs_oracle(cuda, H, W, nwin):
     """Chosen form (int8 tensor-core Gram, f16 tensor-core band DFT fused with lens + row FFT):
