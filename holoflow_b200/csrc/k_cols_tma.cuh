@@ -14,6 +14,7 @@ struct ColMomArgs {
   float  *out;           // moment images [nwin][n_moments][out rows][out cols]
   int64_t out_win, out_plane, out_row;
   int    *status;        // receives 21 if a stage wait expires
+  int     fast;          // chosen form: hardware square-root approximation, fused moment sums
 };
 
 // `tmap`: 2D float32 tensor map over the band planes viewed as [rows][2 * W] (complex as two

@@ -211,6 +211,8 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
         constexpr int TPR   = U / 2;                       // tiles per round
         constexpr int NR    = (NTILE + TPR - 1) / TPR;     // rounds per row
         uint32_t      raw[2][U][GL::kWords];
+        // x - shift exactly, without an integer conversion: (2^23 + x) - (2^23 + shift)
+        const float   magic = 8388608.f + a.shift;
         auto load_round = [&](int rd, uint32_t (&dst)[U][GL::kWords]) {
 #pragma unroll
           for (int u = 0; u < U; ++u) {
@@ -240,7 +242,8 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
               __half2 h[4];
 #pragma unroll
               for (int i = 0; i < 4; ++i)
-                h[i] = __floats2half2_rn((float)v[8 * q + 2 * i] - a.shift, (float)v[8 * q + 2 * i + 1] - a.shift);
+                h[i] = __floats2half2_rn(__uint_as_float(0x4B000000u | v[8 * q + 2 * i]) - magic,
+                                         __uint_as_float(0x4B000000u | v[8 * q + 2 * i + 1]) - magic);
               const int chunk = (m0 & 63) >> 3;
               uint8_t  *dst   = tile + (m0 >> 6) * 8192 + (t >> 3) * 1024 + (t & 7) * 128 + ((chunk ^ (t & 7)) << 4);
               *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(h);

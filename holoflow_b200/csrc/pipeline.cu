@@ -171,6 +171,7 @@ static int cols_moments(hf_plan *p, int nwin, float *out, cudaStream_t s) {
     ca.H = d.height, ca.W = d.width, ca.nz = p->nz, ca.rows_per_win = (int64_t)p->nz * d.height;
     ca.out = out, ca.out_win = (int64_t)p->nmom * oplane, ca.out_plane = oplane, ca.out_row = p->OW;
     ca.status = p->status;
+    ca.fast   = d.form == HF_FORM_CHOSEN;
     HF_TRY(launch_col_moments_tma(p->band_tmap, ca, p->mom, nwin, s));
   } else {
     ColPass cp{};
