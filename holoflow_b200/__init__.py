@@ -47,6 +47,14 @@ class HfDesc(C.Structure):
 _vp, _i32, _i64, _f32, _sz = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_size_t
 
 
+class HoloHeader(C.Structure):
+    """hf_holo_header: the 64-byte packed .holo header (holofile.hh:87-104 field order)."""
+    _pack_ = 1
+    _fields_ = [("magic_number", C.c_uint32), ("version", C.c_uint16), ("bits_per_pixel", C.c_uint16),
+                ("frame_width", C.c_uint32), ("frame_height", C.c_uint32), ("frame_count", C.c_uint32),
+                ("data_size_in_bytes", C.c_uint64), ("endianness", C.c_uint8), ("padding", C.c_char * 35)]
+
+
 class HfTDesc(C.Structure):
     """hf_tdesc: holoflow::core::TDesc across the C ABI (strides in bytes, zero = contiguous)."""
     _fields_ = [("rank", C.c_int32), ("dtype", C.c_int32), ("mem_loc", C.c_int32), ("reserved", C.c_int32),
@@ -121,6 +129,18 @@ _PROTOS = {
     "hf_node_execute": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_int)]),
     "hf_node_output_desc": (C.c_int, [_vp, C.c_int, C.POINTER(HfTDesc)]),
     "hf_node_destroy": (C.c_int, [_vp]),
+    "hf_node_output_ptr": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.POINTER(C.c_int)]),
+    "hf_holo_open": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "hf_holo_header_get": (C.c_int, [_vp, C.POINTER(HoloHeader)]),
+    "hf_holo_footer": (C.c_int, [_vp, C.c_char_p, _sz, C.POINTER(_sz)]),
+    "hf_holo_seek": (C.c_int, [_vp, _i64]),
+    "hf_holo_tell": (C.c_int, [_vp, C.POINTER(_i64)]),
+    "hf_holo_read": (C.c_int, [_vp, _vp, _i64]),
+    "hf_holo_close": (C.c_int, [_vp]),
+    "hf_holo_create": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint16, C.c_char_p,
+                                 C.POINTER(_vp)]),
+    "hf_holo_write": (C.c_int, [_vp, _vp, _i64]),
+    "hf_holo_finish": (C.c_int, [_vp]),
     "hf_plan_stage_times": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
 }

@@ -16,6 +16,8 @@ struct hf_node {
   const core::ISyncTaskFactory     *factory = nullptr;
   std::unique_ptr<core::ISyncTask>  task;
   std::vector<core::TDesc>          in_descs, out_descs;
+  std::vector<bool>                 owned;     // outputs the task publishes itself
+  std::vector<void *>               published; // output origins as of the last execute
 };
 
 namespace {
@@ -117,7 +119,12 @@ int hf_node_create(const char *kind, const char *json, int n_in, const hf_tdesc 
     n->factory   = &nodes::default_registry().get_sync(kind);
     n->in_descs  = to_descs(n_in, in);
     const auto j = parse(json);
-    n->out_descs = n->factory->infer(n->in_descs, j).output_descs;
+    auto inf     = n->factory->infer(n->in_descs, j);
+    n->out_descs = inf.output_descs;
+    n->owned.assign(n->out_descs.size(), false);
+    for (size_t i = 0; i < inf.owned_outputs.size() && i < n->owned.size(); ++i)
+      n->owned[i] = inf.owned_outputs[i];
+    n->published.assign(n->out_descs.size(), nullptr);
     n->task      = n->factory->create(n->in_descs, j, core::SyncCreateCtx{reinterpret_cast<cudaStream_t>(s)});
     *node        = n.release();
     return HF_OK;
@@ -129,11 +136,15 @@ int hf_node_update(hf_node *node, const char *json, int n_in, const hf_tdesc *in
     HF_CHECK_ARG(node != nullptr && node->task != nullptr, "hf_node_update: node was not created");
     const auto descs = to_descs(n_in, in);
     const auto j     = parse(json);
-    auto       out   = node->factory->infer(descs, j).output_descs;
+    auto       inf   = node->factory->infer(descs, j);
     node->task       = node->factory->update(std::move(node->task), descs, j,
                                              core::SyncCreateCtx{reinterpret_cast<cudaStream_t>(s)});
     node->in_descs   = descs;
-    node->out_descs  = std::move(out);
+    node->out_descs  = std::move(inf.output_descs);
+    node->owned.assign(node->out_descs.size(), false);
+    for (size_t i = 0; i < inf.owned_outputs.size() && i < node->owned.size(); ++i)
+      node->owned[i] = inf.owned_outputs[i];
+    node->published.assign(node->out_descs.size(), nullptr);
     return HF_OK;
   });
 }
@@ -141,8 +152,7 @@ int hf_node_update(hf_node *node, const char *json, int n_in, const hf_tdesc *in
 int hf_node_execute(hf_node *node, void *const *inputs, void *const *outputs, int *op_result) {
   return guarded([&]() -> int {
     HF_CHECK_ARG(node != nullptr && node->task != nullptr, "hf_node_execute: node was not created");
-    HF_CHECK_ARG((node->in_descs.empty() || inputs != nullptr) && (node->out_descs.empty() || outputs != nullptr),
-                 "hf_node_execute: null tensor array");
+    HF_CHECK_ARG(node->in_descs.empty() || inputs != nullptr, "hf_node_execute: null tensor array");
     std::vector<core::Storage> st(node->in_descs.size() + node->out_descs.size());
     std::vector<core::TView>   iv(node->in_descs.size()), ov(node->out_descs.size());
     for (size_t i = 0; i < iv.size(); ++i) {
@@ -152,15 +162,18 @@ int hf_node_execute(hf_node *node, void *const *inputs, void *const *outputs, in
       iv[i].desc.offset = 0; // the pointer given is the tensor's origin
     }
     for (size_t i = 0; i < ov.size(); ++i) {
-      HF_CHECK_ARG(outputs[i] != nullptr, "hf_node_execute: null output pointer");
+      void *p = outputs ? outputs[i] : nullptr;
+      HF_CHECK_ARG(node->owned[i] || p != nullptr, "hf_node_execute: null output pointer");
       auto &s = st[iv.size() + i];
-      s       = core::Storage{node->out_descs[i].mem_loc, node->out_descs[i].num_bytes(), static_cast<std::byte *>(outputs[i])};
+      s       = core::Storage{node->out_descs[i].mem_loc, node->out_descs[i].num_bytes(), static_cast<std::byte *>(p)};
       ov[i]   = core::TView{node->out_descs[i], &s};
       ov[i].desc.offset = 0;
     }
     std::atomic<bool> cancelled{false};
     core::SyncCtx     ctx{std::span<core::TView>(iv), std::span<core::TView>(ov), &cancelled};
     const auto        r = node->task->execute(ctx);
+    for (size_t i = 0; i < ov.size(); ++i)
+      node->published[i] = ov[i].data();
     if (op_result)
       *op_result = (int)r;
     return HF_OK;
@@ -172,6 +185,16 @@ int hf_node_output_desc(const hf_node *node, int i, hf_tdesc *out) {
   HF_CHECK_ARG(node != nullptr && out != nullptr && i >= 0 && i < (int)node->out_descs.size(),
                "hf_node_output_desc: bad argument");
   *out = from_desc(node->out_descs[i]);
+  return HF_OK;
+}
+
+int hf_node_output_ptr(const hf_node *node, int i, void **ptr, int *owned) {
+  hf::clear_error();
+  HF_CHECK_ARG(node != nullptr && ptr != nullptr && i >= 0 && i < (int)node->out_descs.size(),
+               "hf_node_output_ptr: bad argument");
+  *ptr = node->published[i];
+  if (owned)
+    *owned = node->owned[i] ? 1 : 0;
   return HF_OK;
 }
 

@@ -884,6 +884,7 @@ void register_path_kinds(core::Registry &r) {
   r.register_sync("MeanAbs", std::make_unique<MeanAbsFactory>());
   r.register_sync("Conversion", std::make_unique<ConversionFactory>());
   r.register_sync("DopplerMoments", std::make_unique<DopplerMomentsFactory>());
+  r.register_sync("Holofile", std::make_unique<HolofileFactory>());
 }
 
 core::Registry &default_registry() {

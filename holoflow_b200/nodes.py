@@ -13,7 +13,16 @@ from typing import Any, Optional, Sequence
 import torch
 
 from . import HfError, HfTDesc, check, lib
-from .pipeline import _ptr, _stream
+from .pipeline import _ptr, _stream as _cuda_stream
+
+
+def _stream(stream=None) -> C.c_void_p:
+    """The stream handle for create/update: torch's current stream, or the null handle where no
+    CUDA device exists (host-only nodes such as a Live or CPUCached "Holofile" source need no
+    stream; a compute node given it fails inside the library with HF_ERR_CUDA)."""
+    if stream is None and not torch.cuda.is_available():
+        return C.c_void_p(0)
+    return _cuda_stream(stream)
 
 _DT = {torch.uint8: 0, torch.int16: 1, torch.float32: 2, torch.complex64: 3}
 _TORCH = {0: torch.uint8, 1: torch.int16, 2: torch.float32, 3: torch.complex64}  # U16 carried as int16
@@ -73,12 +82,23 @@ class Node:
         check(lib().hf_node_output_desc(self._n, i, C.byref(d)))
         return d
 
-    def execute(self, inputs: Sequence[torch.Tensor], outputs: Sequence[torch.Tensor]) -> int:
-        ins = (C.c_void_p * max(1, len(inputs)))(*[_ptr(t).value for t in inputs])
-        outs = (C.c_void_p * max(1, len(outputs)))(*[_ptr(t).value for t in outputs])
+    def execute(self, inputs: Sequence[Any], outputs: Sequence[Optional[torch.Tensor]]) -> int:
+        """Inputs are tensors or raw origin pointers (ints, e.g. another node's output_ptr()).
+        An output the node owns (a cached "Holofile" source) is given as None; its pointer is then
+        available from output_ptr()."""
+        def addr(t):
+            return int(t) if isinstance(t, int) else _ptr(t).value
+        ins = (C.c_void_p * max(1, len(inputs)))(*[addr(t) for t in inputs])
+        outs = (C.c_void_p * max(1, len(outputs)))(*[None if t is None else _ptr(t).value for t in outputs])
         r = C.c_int()
         check(lib().hf_node_execute(self._n, ins, outs, C.byref(r)))
         return r.value
+
+    def output_ptr(self, i: int = 0) -> tuple[int, bool]:
+        """(origin pointer of output i as of the last execute, whether the node owns it)."""
+        p, owned = C.c_void_p(), C.c_int()
+        check(lib().hf_node_output_ptr(self._n, i, C.byref(p), C.byref(owned)))
+        return (p.value or 0), bool(owned.value)
 
     def close(self) -> None:
         if self._n:

@@ -307,8 +307,8 @@ int hf_multi_plan(hf_multi *multi, int i, hf_plan **plan);
 /* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
  * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------
  * Kinds: "FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
- * "Conversion" (the reference's, with its JSON settings keys) and "DopplerMoments" (the fused
- * per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
+ * "Conversion", "Holofile" (the reference's, with its JSON settings keys) and "DopplerMoments"
+ * (the fused per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
  * HF_U16, HF_F32, HF_CF32), strides in BYTES (all zero = C-contiguous), mem_loc 1 = device.
  * infer() failures return HF_ERR_INVALID with "<Factory> inference error: ..." in hf_last_error();
  * work is enqueued on the stream given at create/update. */
@@ -330,11 +330,54 @@ int hf_node_create(const char *kind, const char *json_settings, int n_inputs, co
                    hf_node **node);
 /* ISyncTaskFactory::update: reuses the task where the factory can (z-only changes). */
 int hf_node_update(hf_node *node, const char *json_settings, int n_inputs, const hf_tdesc *inputs, hf_stream_t s);
-/* ISyncTask::execute on device tensors given by their origin pointers; *op_result receives the
- * OpResult (0 = Ok). */
+/* ISyncTask::execute on tensors given by their origin pointers; *op_result receives the
+ * OpResult (0 = Ok).  An output the node owns (InferResult::owned_outputs, e.g. a cached
+ * "Holofile" source) takes NULL here: the node publishes its own pointer, which
+ * hf_node_output_ptr returns after the call. */
 int hf_node_execute(hf_node *node, void *const *inputs, void *const *outputs, int *op_result);
 int hf_node_output_desc(const hf_node *node, int index, hf_tdesc *out);
+/* Origin pointer of output `index` as of the last hf_node_execute (the caller's pointer for a
+ * caller-provided output, the node's own for an owned one); *owned = 1 if the node owns it. */
+int hf_node_output_ptr(const hf_node *node, int index, void **ptr, int *owned);
 int hf_node_destroy(hf_node *node);
+
+/* ---- .holo acquisition files (holofile/include/holofile/holofile.hh:87-152) -------------------
+ * A 64-byte little-endian header (magic "HOLO", version 66, bits_per_pixel, width, height,
+ * frame_count, data_size_in_bytes, endianness), the frames, then an optional JSON footer.
+ * bits_per_pixel 8 and 16 are the reference's pixel types; 12 holds Mono12p frames (2 pixels in
+ * 3 bytes, the HF_MONO12P layout).  Errors: HF_ERR_INVALID for a malformed file (message
+ * "Holofile: Incomplete header" / "Invalid magic number" / "Invalid frame size" as the
+ * reference's exceptions), HF_ERR_STATE for I/O failures and reading past the last frame
+ * ("Holofile: End of file reached"). */
+#pragma pack(push, 1)
+typedef struct hf_holo_header {
+  uint32_t magic_number;
+  uint16_t version, bits_per_pixel;
+  uint32_t frame_width, frame_height, frame_count;
+  uint64_t data_size_in_bytes; /* at byte 20: the struct is packed */
+  uint8_t  endianness;
+  char     padding[35];
+} hf_holo_header; /* byte-for-byte the file's 64-byte header */
+#pragma pack(pop)
+typedef struct hf_holo_reader hf_holo_reader;
+typedef struct hf_holo_writer hf_holo_writer;
+int hf_holo_open(const char *path, hf_holo_reader **reader);
+int hf_holo_header_get(const hf_holo_reader *reader, hf_holo_header *header);
+/* The footer JSON text (NUL-terminated) in buf; *len receives its length, 0 when the file has
+ * no valid footer.  buf may be NULL to query the length. */
+int hf_holo_footer(const hf_holo_reader *reader, char *buf, size_t cap, size_t *len);
+int hf_holo_seek(hf_holo_reader *reader, int64_t frame_index);
+int hf_holo_tell(const hf_holo_reader *reader, int64_t *frame_index);
+/* Reads `count` frames at the cursor into host memory `dst` (pageable or pinned). */
+int hf_holo_read(hf_holo_reader *reader, void *dst, int64_t count);
+int hf_holo_close(hf_holo_reader *reader);
+/* Creates `path` with a header for frame_count frames of width x height at bits_per_pixel
+ * (8, 12 or 16) and the footer JSON text (NULL or empty for an empty object). */
+int hf_holo_create(const char *path, uint32_t frame_count, uint32_t width, uint32_t height, uint16_t bits_per_pixel,
+                   const char *footer_json, hf_holo_writer **writer);
+int hf_holo_write(hf_holo_writer *writer, const void *src, int64_t count);
+/* Appends the footer and closes the file. */
+int hf_holo_finish(hf_holo_writer *writer);
 
 #ifdef __cplusplus
 }

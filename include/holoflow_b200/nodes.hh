@@ -62,7 +62,18 @@ struct DopplerMomentsSettings {
   std::optional<AngularSpectrumPadding> padding;
 };
 
+// Source node reading a .holo file (holotask/include/holotask/sources/holofile.hh:30-50).
+struct HolofileSettings {
+  enum class LoadKind { Live, CPUCached, GPUCached } load_kind = LoadKind::Live;
+  std::string        path;
+  int                start_frame = 0, end_frame = 0, batch_size = 0;
+  std::optional<int> max_fps;           // playback cap in frames per second
+  bool               keep_cursor = true; // keep the read position across update()
+};
+
 void from_json(const nlohmann::json &j, FresnelDiffractionSettings &s);
+void from_json(const nlohmann::json &j, HolofileSettings::LoadKind &s);
+void from_json(const nlohmann::json &j, HolofileSettings &s);
 void from_json(const nlohmann::json &j, AngularSpectrumFilter &s);
 void from_json(const nlohmann::json &j, AngularSpectrumPadding &s);
 void from_json(const nlohmann::json &j, AngularSpectrumSettings &s);
@@ -99,10 +110,12 @@ HFB_SYNC_FACTORY(MeanFactory);
 HFB_SYNC_FACTORY(MeanAbsFactory);
 HFB_SYNC_FACTORY(ConversionFactory);
 HFB_SYNC_FACTORY(DopplerMomentsFactory);
+HFB_SYNC_FACTORY(HolofileFactory); // frames [batch, H, W] (12-bit: packed rows [batch, H, 3W/2] U8)
 #undef HFB_SYNC_FACTORY
 
 // Registers every node above under its kind string: "FresnelDiffraction", "AngularSpectrum",
-// "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion" (the reference's) and "DopplerMoments".
+// "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion", "Holofile" (the reference's) and
+// "DopplerMoments".
 void register_path_kinds(core::Registry &registry);
 
 // The process-wide registry the C ABI's hf_node_* functions use.

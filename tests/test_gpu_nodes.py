@@ -181,3 +181,38 @@ def test_doppler_moments_node_mono12p_chosen_and_z_update(cuda):
             exp = O.reconstruct_window(frames[64 * w: 64 * w + 64], cfg)
             for m in range(3):
                 assert rel(got[w, m].cpu().numpy(), exp[m]) < 1e-3, (z, w, m)
+
+
+def test_holofile_gpu_cached_source_feeds_doppler_moments(cuda, tmp_path):
+    """A 12-bit .holo loaded once into device memory ("Holofile", GPUCached) hands out each batch
+    of packed frames as a view into its cache; fed to "DopplerMoments" as one 64-frame window, the
+    moment images equal those of the same frames uploaded directly (same kernels, same bytes)."""
+    import torch
+    from holoflow_b200 import holofile as HF
+    N = _n()
+    H = W = 128
+    frames = S.Interferograms(S.config1(128, height=H, width=W)).frames(0, 128)
+    packed = O.pack12(frames.reshape(-1)).reshape(128, H * W * 3 // 2)
+    path = str(tmp_path / "acq.holo")
+    HF.write(path, packed, 12, width=W, height=H, footer={"fs": 67000})
+    src = N.Node("Holofile", {"path": path, "load_kind": "GPUCached", "start_frame": 0, "end_frame": 128,
+                              "batch_size": 64}, [])
+    od = src.output_desc(0)
+    assert N.shape_of(od) == (64, H, W * 3 // 2) and od.mem_loc == 1
+    s = {"time_z_begin": 4, "time_z_end": 32, "propagation": "fresnel", "lambda": LAM, "dx": DX, "z": 0.25,
+         "fs": 67e3, "clutter_rank": 4, "input_format": "mono12p", "height": H, "width": W, "form": "chosen"}
+    win = N.desc_of(torch.empty((1, 64, H * W * 3 // 2), dtype=torch.uint8, device=cuda))
+    dop = N.Node("DopplerMoments", s, [win])
+    got = torch.empty((1, 3, H, W), dtype=torch.float32, device=cuda)
+    for b in range(3):  # the third batch wraps back to frame 0
+        assert src.execute([], [None]) == 0
+        ptr, owned = src.output_ptr(0)
+        assert owned and ptr
+        assert dop.execute([ptr], [got]) == 0
+        torch.cuda.synchronize()
+        first = 64 * (b % 2)
+        direct = torch.from_numpy(packed[first:first + 64].reshape(1, 64, -1).copy()).to(cuda)
+        (ref,) = N.run_sync_factory("DopplerMoments", s, [direct])
+        assert torch.equal(got, ref), b
+    dop.close()
+    src.close()

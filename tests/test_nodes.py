@@ -39,7 +39,7 @@ def invalid(kind, settings, descs, fragment):
 
 def test_reference_kinds_are_registered():
     assert set(N.kinds()) == {"FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
-                              "Conversion", "DopplerMoments"}
+                              "Conversion", "Holofile", "DopplerMoments"}
 
 
 def test_unknown_kind_and_bad_settings():
