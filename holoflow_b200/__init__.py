@@ -55,6 +55,11 @@ class HoloHeader(C.Structure):
                 ("data_size_in_bytes", C.c_uint64), ("endianness", C.c_uint8), ("padding", C.c_char * 35)]
 
 
+class HfEllipse(C.Structure):
+    """hf_ellipse: the percentile clip's region (normalized centre and radii, angle in degrees)."""
+    _fields_ = [("cx", C.c_float), ("cy", C.c_float), ("rx", C.c_float), ("ry", C.c_float), ("angle", C.c_float)]
+
+
 class HfTDesc(C.Structure):
     """hf_tdesc: holoflow::core::TDesc across the C ABI (strides in bytes, zero = contiguous)."""
     _fields_ = [("rank", C.c_int32), ("dtype", C.c_int32), ("mem_loc", C.c_int32), ("reserved", C.c_int32),
@@ -129,6 +134,19 @@ _PROTOS = {
     "hf_node_execute": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_int)]),
     "hf_node_output_desc": (C.c_int, [_vp, C.c_int, C.POINTER(HfTDesc)]),
     "hf_node_destroy": (C.c_int, [_vp]),
+    "hf_fftshift": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.POINTER(_i64), C.c_uint32, _vp]),
+    "hf_flatfield_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_float, C.c_float, _vp, C.POINTER(_vp)]),
+    "hf_flatfield_is_fourier": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "hf_flatfield_exec": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "hf_flatfield_destroy": (C.c_int, [_vp]),
+    "hf_pctclip_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.POINTER(HfEllipse), _vp,
+                                    C.POINTER(_vp)]),
+    "hf_pctclip_roi_count": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "hf_pctclip_exec": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "hf_pctclip_destroy": (C.c_int, [_vp]),
+    "hf_slideavg_create": (C.c_int, [_i64, C.c_int, C.c_int, _vp, C.POINTER(_vp)]),
+    "hf_slideavg_push": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_int), _vp]),
+    "hf_slideavg_destroy": (C.c_int, [_vp]),
     "hf_node_output_ptr": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.POINTER(C.c_int)]),
     "hf_holo_open": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
     "hf_holo_header_get": (C.c_int, [_vp, C.POINTER(HoloHeader)]),

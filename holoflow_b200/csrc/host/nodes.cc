@@ -872,6 +872,230 @@ std::unique_ptr<ISyncTask> DopplerMomentsFactory::update(std::unique_ptr<ISyncTa
 }
 
 // ================================================================================================
+// Post-moment display chain: FFTShiftNp (holonp/src/fftshift.cu:185-290), Flatfield
+// (holotask/src/syncs/flatfield.cu:296-453), PctClip (holotask/src/syncs/pct_clip.cu:230-333)
+// ================================================================================================
+void from_json(const nlohmann::json &j, FFTShiftSettings &s) {
+  s.axes.clear();
+  if (j.contains("axes") && !j.at("axes").is_null())
+    j.at("axes").get_to(s.axes);
+}
+void from_json(const nlohmann::json &j, FlatfieldSettings &s) {
+  j.at("sigma_y").get_to(s.sigma_y);
+  j.at("sigma_x").get_to(s.sigma_x);
+}
+void from_json(const nlohmann::json &j, PctClipSettings &s) {
+  j.at("min_pct").get_to(s.min_pct);
+  j.at("max_pct").get_to(s.max_pct);
+  const auto &r = j.at("roi");
+  r.at("cx").get_to(s.roi.cx);
+  r.at("cy").get_to(s.roi.cy);
+  r.at("rx").get_to(s.roi.rx);
+  r.at("ry").get_to(s.roi.ry);
+  r.at("angle").get_to(s.roi.angle);
+}
+
+namespace {
+// The reference's FFTShift checks throw "FFTShift: <msg>" (fftshift.cu:30-34).
+void shift_check(bool cond, const std::string &msg) {
+  if (!cond)
+    throw std::invalid_argument("FFTShift: " + msg);
+}
+
+uint32_t shift_axes_mask(const std::vector<int> &axes, int ndim) {
+  if (axes.empty())
+    return ndim >= 32 ? 0xFFFFFFFFu : ((1u << ndim) - 1u);
+  uint32_t mask = 0;
+  for (int a : axes) {
+    if (a < 0)
+      a += ndim;
+    shift_check(a >= 0 && a < ndim, "axis out of range");
+    shift_check(!(mask & (1u << a)), "axes must be unique");
+    mask |= 1u << a;
+  }
+  return mask;
+}
+
+class FFTShiftTask final : public ISyncTask {
+public:
+  TDesc        idesc;
+  uint32_t     mask = 0;
+  cudaStream_t stream{};
+  OpResult     execute(SyncCtx &ctx) override {
+    std::vector<int64_t> shape(idesc.shape.begin(), idesc.shape.end());
+    hf_ok(hf_fftshift(ctx.inputs[0].data(), ctx.outputs[0].data(), (int)core::size_of(idesc.dtype),
+                      (int)shape.size(), shape.data(), mask, stream),
+          "FFTShift");
+    return OpResult::Ok;
+  }
+};
+
+class FlatfieldTask final : public ISyncTask {
+public:
+  hf_flatfield     *ff = nullptr;
+  FlatfieldSettings settings;
+  TDesc             idesc;
+  cudaStream_t      stream{};
+  ~FlatfieldTask() override { hf_flatfield_destroy(ff); }
+  OpResult execute(SyncCtx &ctx) override {
+    hf_ok(hf_flatfield_exec(ff, reinterpret_cast<const float *>(ctx.inputs[0].data()),
+                            reinterpret_cast<float *>(ctx.outputs[0].data()), stream),
+          "Flatfield");
+    return OpResult::Ok;
+  }
+};
+
+class PctClipTask final : public ISyncTask {
+public:
+  hf_pctclip     *pc = nullptr;
+  PctClipSettings settings;
+  TDesc           idesc;
+  cudaStream_t    stream{};
+  ~PctClipTask() override { hf_pctclip_destroy(pc); }
+  OpResult execute(SyncCtx &ctx) override {
+    hf_ok(hf_pctclip_exec(pc, reinterpret_cast<const float *>(ctx.inputs[0].data()),
+                          reinterpret_cast<float *>(ctx.outputs[0].data()), nullptr, stream),
+          "PctClip");
+    return OpResult::Ok;
+  }
+};
+
+bool same_desc(const TDesc &a, const TDesc &b) {
+  return a.shape == b.shape && a.strides == b.strides && a.dtype == b.dtype && a.mem_loc == b.mem_loc &&
+         a.offset == b.offset;
+}
+} // namespace
+
+InferResult FFTShiftFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const auto s = j.get<FFTShiftSettings>();
+  shift_check(input_descs.size() == 1, "expected exactly 1 input");
+  const auto &idesc = input_descs[0];
+  shift_check(idesc.mem_loc == MemLoc::Device, "only Device tensors are supported");
+  shift_check(idesc.is_contiguous(), "input must be C-contiguous");
+  const int ndim = (int)idesc.rank();
+  shift_check(ndim > 0, "input ndim must be > 0");
+  shift_check(ndim <= 16, "input ndim too large");
+  (void)shift_axes_mask(s.axes, ndim);
+  shift_check(idesc.num_elements() > 0, "input tensor has zero elements");
+  return sync_result(idesc, idesc);
+}
+
+std::unique_ptr<ISyncTask> FFTShiftFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                   const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t    = std::make_unique<FFTShiftTask>();
+  t->idesc  = input_descs[0];
+  t->mask   = shift_axes_mask(j.get<FFTShiftSettings>().axes, (int)t->idesc.rank());
+  t->stream = ctx.stream;
+  return t;
+}
+
+std::unique_ptr<ISyncTask> FFTShiftFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> input_descs,
+                                                   const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult FlatfieldFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"FlatfieldFactory"};
+  const auto  s = j.get<FlatfieldSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.rank() >= 2, "input must be a tensor of rank 2 or higher");
+  check(idesc.dtype == DType::F32, "input must be float32");
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(idesc.is_contiguous(), "input must be C-contiguous");
+  check(idesc.num_elements() > 0, "input must not be empty");
+  check(s.sigma_y > 0.0f, "sigma_y must be positive");
+  check(s.sigma_x > 0.0f, "sigma_x must be positive");
+  return sync_result(idesc, idesc);
+}
+
+std::unique_ptr<ISyncTask> FlatfieldFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                    const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<FlatfieldTask>();
+  t->settings = j.get<FlatfieldSettings>();
+  t->idesc    = input_descs[0];
+  t->stream   = ctx.stream;
+  const size_t r = t->idesc.rank();
+  int64_t      planes = 1;
+  for (size_t i = 0; i + 2 < r; ++i)
+    planes *= (int64_t)t->idesc.shape[i];
+  const int rc = hf_flatfield_create(planes, (int)t->idesc.shape[r - 2], (int)t->idesc.shape[r - 1],
+                                     t->settings.sigma_y, t->settings.sigma_x, ctx.stream, &t->ff);
+  if (rc == HF_ERR_INVALID) // sigma too small for a kernel: the reference's inference error
+    Check{"FlatfieldFactory"}(false, "sigma is too small to form a Gaussian kernel");
+  hf_ok(rc, "Flatfield");
+  return t;
+}
+
+std::unique_ptr<ISyncTask> FlatfieldFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> input_descs,
+                                                    const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<FlatfieldTask *>(old.get());
+  if (t && t->settings.sigma_y == j.get<FlatfieldSettings>().sigma_y &&
+      t->settings.sigma_x == j.get<FlatfieldSettings>().sigma_x && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult PctClipFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"PctClipFactory"};
+  const auto  s = j.get<PctClipSettings>();
+  check(s.min_pct >= 0.0f, "min_pct must be >= 0");
+  check(s.min_pct <= 100.0f, "min_pct must be <= 100");
+  check(s.max_pct >= 0.0f, "max_pct must be >= 0");
+  check(s.max_pct <= 100.0f, "max_pct must be <= 100");
+  check(s.min_pct < s.max_pct, "min_pct must be < max_pct");
+  check(s.roi.rx > 0.0f, "roi.rx must be > 0");
+  check(s.roi.rx <= 1.0f, "roi.rx must be <= 1");
+  check(s.roi.ry > 0.0f, "roi.ry must be > 0");
+  check(s.roi.ry <= 1.0f, "roi.ry must be <= 1");
+  check(s.roi.cx >= 0.0f, "roi.cx must be >= 0");
+  check(s.roi.cx <= 1.0f, "roi.cx must be <= 1");
+  check(s.roi.cy >= 0.0f, "roi.cy must be >= 0");
+  check(s.roi.cy <= 1.0f, "roi.cy must be <= 1");
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.dtype == DType::F32, "input must be float32");
+  check(idesc.rank() == 3, "input must be 3D");
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(idesc.is_contiguous(), "input must be C-contiguous");
+  return sync_result(idesc, idesc);
+}
+
+std::unique_ptr<ISyncTask> PctClipFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                  const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<PctClipTask>();
+  t->settings = j.get<PctClipSettings>();
+  t->idesc    = input_descs[0];
+  t->stream   = ctx.stream;
+  const hf_ellipse roi{t->settings.roi.cx, t->settings.roi.cy, t->settings.roi.rx, t->settings.roi.ry,
+                       t->settings.roi.angle};
+  hf_ok(hf_pctclip_create((int)t->idesc.shape[0], (int)t->idesc.shape[1], (int)t->idesc.shape[2],
+                          t->settings.min_pct, t->settings.max_pct, &roi, ctx.stream, &t->pc),
+        "PctClip");
+  return t;
+}
+
+std::unique_ptr<ISyncTask> PctClipFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> input_descs,
+                                                  const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<PctClipTask *>(old.get());
+  if (t && t->settings == j.get<PctClipSettings>() && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+// ================================================================================================
 // registry
 // ================================================================================================
 void register_path_kinds(core::Registry &r) {
@@ -885,6 +1109,9 @@ void register_path_kinds(core::Registry &r) {
   r.register_sync("Conversion", std::make_unique<ConversionFactory>());
   r.register_sync("DopplerMoments", std::make_unique<DopplerMomentsFactory>());
   r.register_sync("Holofile", std::make_unique<HolofileFactory>());
+  r.register_sync("FFTShiftNp", std::make_unique<FFTShiftFactory>());
+  r.register_sync("Flatfield", std::make_unique<FlatfieldFactory>());
+  r.register_sync("PctClip", std::make_unique<PctClipFactory>());
 }
 
 core::Registry &default_registry() {

@@ -307,8 +307,8 @@ int hf_multi_plan(hf_multi *multi, int i, hf_plan **plan);
 /* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
  * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------
  * Kinds: "FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
- * "Conversion", "Holofile" (the reference's, with its JSON settings keys) and "DopplerMoments"
- * (the fused per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
+ * "Conversion", "FFTShiftNp", "Flatfield", "PctClip", "Holofile" (the reference's, with its JSON
+ * settings keys) and "DopplerMoments" (the fused per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
  * HF_U16, HF_F32, HF_CF32), strides in BYTES (all zero = C-contiguous), mem_loc 1 = device.
  * infer() failures return HF_ERR_INVALID with "<Factory> inference error: ..." in hf_last_error();
  * work is enqueued on the stream given at create/update. */
@@ -340,6 +340,51 @@ int hf_node_output_desc(const hf_node *node, int index, hf_tdesc *out);
  * caller-provided output, the node's own for an owned one); *owned = 1 if the node owns it. */
 int hf_node_output_ptr(const hf_node *node, int index, void **ptr, int *owned);
 int hf_node_destroy(hf_node *node);
+
+/* ---- post-moment display chain (graph_builder.cc:633-676) -------------------------------------
+ * The steps between a moment image and the display: fftshift, flatfield, sliding average,
+ * percentile clip, then hf_convert(..., HF_CONV_SCALED) to U8.  Work is enqueued on `s`;
+ * create functions allocate their device state on the current device (hf_pctclip_create also
+ * synchronizes `s` once to count the region's pixels, as the reference does at create). */
+
+/* holonp FFTShift (holonp/src/fftshift.cu:98-134): out[j] = in[(j + n/2) mod n] along every axis
+ * k with bit k of axes_mask set (axis 0 = outermost); in and out must not alias. */
+int hf_fftshift(const void *in, void *out, int elem_size, int ndim, const int64_t *shape, uint32_t axes_mask,
+                hf_stream_t s);
+
+/* Flatfield (holotask/src/syncs/flatfield.cu): out = in - Gaussian(in) on each [height][width]
+ * plane of planes; sigmas in pixels.  Kernels of fewer than 65 taps run spatially with
+ * clamp-at-edge borders, longer ones as the analytic Fourier high-pass (image sides in
+ * {64..1536}, height <= 1024); hf_flatfield_is_fourier tells which. */
+typedef struct hf_flatfield hf_flatfield;
+int hf_flatfield_create(int64_t planes, int height, int width, float sigma_y, float sigma_x, hf_stream_t s,
+                        hf_flatfield **ff);
+int hf_flatfield_is_fourier(const hf_flatfield *ff, int *fourier);
+int hf_flatfield_exec(hf_flatfield *ff, const float *in, float *out, hf_stream_t s);
+int hf_flatfield_destroy(hf_flatfield *ff);
+
+/* PctClip (holotask/src/syncs/pct_clip.cu): clips [depth][height][width] to the values at
+ * ranks int(pct / 100 * (count - 1)) of the pixels inside the ellipse (normalized centre, radii
+ * and angle in degrees, applied to every slice).  `bounds` (optional, device float[2]) receives
+ * the two values. */
+typedef struct hf_ellipse {
+  float cx, cy, rx, ry, angle;
+} hf_ellipse;
+typedef struct hf_pctclip hf_pctclip;
+int hf_pctclip_create(int depth, int height, int width, float min_pct, float max_pct, const hf_ellipse *roi,
+                      hf_stream_t s, hf_pctclip **pc);
+int hf_pctclip_roi_count(const hf_pctclip *pc, int *count);
+int hf_pctclip_exec(hf_pctclip *pc, const float *in, float *out, float *bounds, hf_stream_t s);
+int hf_pctclip_destroy(hf_pctclip *pc);
+
+/* SlidingAverage (holotask/src/asyncs/slide_avg.cu): the mean of the last window_size images,
+ * kept as a float32 running average (avg += x / n; avg -= x_old / n).  The first discard_first
+ * images are dropped; *ready becomes 1 (and `out`, if given, holds the average) once window_size
+ * images have entered. */
+typedef struct hf_slideavg hf_slideavg;
+int hf_slideavg_create(int64_t npix, int window_size, int discard_first, hf_stream_t s, hf_slideavg **sa);
+int hf_slideavg_push(hf_slideavg *sa, const float *in, float *out, int *ready, hf_stream_t s);
+int hf_slideavg_destroy(hf_slideavg *sa);
 
 /* ---- .holo acquisition files (holofile/include/holofile/holofile.hh:87-152) -------------------
  * A 64-byte little-endian header (magic "HOLO", version 66, bits_per_pixel, width, height,

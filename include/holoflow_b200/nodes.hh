@@ -71,7 +71,28 @@ struct HolofileSettings {
   bool               keep_cursor = true; // keep the read position across update()
 };
 
+// Post-moment display chain (holonp/include/holonp/fftshift.hh, holotask/syncs/flatfield.hh,
+// holotask/syncs/pct_clip.hh): the same keys.
+struct FFTShiftSettings {
+  std::vector<int> axes; // empty: every axis
+};
+struct FlatfieldSettings {
+  float sigma_y = 0.f, sigma_x = 0.f; // Gaussian sigmas in pixels
+};
+struct PctClipSettings {
+  struct Ellipse {
+    float cx = 0.5f, cy = 0.5f, rx = 0.5f, ry = 0.5f, angle = 0.f; // normalized; angle in degrees
+    bool  operator==(const Ellipse &) const = default;
+  };
+  float   min_pct = 0.f, max_pct = 100.f;
+  Ellipse roi;
+  bool    operator==(const PctClipSettings &) const = default;
+};
+
 void from_json(const nlohmann::json &j, FresnelDiffractionSettings &s);
+void from_json(const nlohmann::json &j, FFTShiftSettings &s);
+void from_json(const nlohmann::json &j, FlatfieldSettings &s);
+void from_json(const nlohmann::json &j, PctClipSettings &s);
 void from_json(const nlohmann::json &j, HolofileSettings::LoadKind &s);
 void from_json(const nlohmann::json &j, HolofileSettings &s);
 void from_json(const nlohmann::json &j, AngularSpectrumFilter &s);
@@ -110,12 +131,15 @@ HFB_SYNC_FACTORY(MeanFactory);
 HFB_SYNC_FACTORY(MeanAbsFactory);
 HFB_SYNC_FACTORY(ConversionFactory);
 HFB_SYNC_FACTORY(DopplerMomentsFactory);
+HFB_SYNC_FACTORY(FFTShiftFactory);  // kind "FFTShiftNp"
+HFB_SYNC_FACTORY(FlatfieldFactory);
+HFB_SYNC_FACTORY(PctClipFactory);
 HFB_SYNC_FACTORY(HolofileFactory); // frames [batch, H, W] (12-bit: packed rows [batch, H, 3W/2] U8)
 #undef HFB_SYNC_FACTORY
 
 // Registers every node above under its kind string: "FresnelDiffraction", "AngularSpectrum",
-// "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion", "Holofile" (the reference's) and
-// "DopplerMoments".
+// "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion", "FFTShiftNp", "Flatfield", "PctClip",
+// "Holofile" (the reference's) and "DopplerMoments".
 void register_path_kinds(core::Registry &registry);
 
 // The process-wide registry the C ABI's hf_node_* functions use.

@@ -544,3 +544,114 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     d = np.linalg.norm((a - b).ravel())
     n = np.linalg.norm(b.ravel())
     return float(d / n) if n else float(d)
+
+
+# ----------------------------------------------------------------------------------------------
+# Post-moment display chain (graph_builder.cc:633-676)
+# ----------------------------------------------------------------------------------------------
+def fftshift_ref(x: np.ndarray, axes: Optional[Sequence[int]] = None) -> np.ndarray:
+    """holonp/src/fftshift.cu:98-134: out[j] = x[(j + n // 2) % n] along each shifted axis (numpy's
+    fftshift for even n, its ifftshift for odd n)."""
+    out = x
+    for a in (range(x.ndim) if axes is None else axes):
+        out = np.roll(out, -(x.shape[a] // 2), axis=a)
+    return out
+
+
+def gaussian_taps(sigma: float) -> np.ndarray:
+    """make_gaussian_kernel (flatfield.cu:57-77): radius ceil(3 sigma) in float32, taps
+    exp(-i^2 / (2 sigma^2)) normalized to sum 1 (float64 here)."""
+    r = int(math.ceil(float(np.float32(3.0) * np.float32(sigma))))
+    if r <= 0:
+        raise ValueError("sigma is too small to form a Gaussian kernel")
+    i = np.arange(-r, r + 1, dtype=np.float64)
+    w = np.exp(-(i * i) / (2.0 * float(sigma) ** 2))
+    return w / w.sum()
+
+
+def flatfield_uses_fourier(height: int, width: int, sigma_y: float, sigma_x: float) -> bool:
+    """should_use_fft_flatfield (flatfield.cu:169-174): kernels of 65 taps or more."""
+    n = max(len(gaussian_taps(sigma_y)), len(gaussian_taps(sigma_x)))
+    return height > 1 and width > 1 and n >= 65
+
+
+def flatfield_spatial(x: np.ndarray, sigma_y: float, sigma_x: float) -> np.ndarray:
+    """flatfield.cu:179-221: out = x - Gy * (Gx * x) with clamp-at-edge borders, per [H][W] plane."""
+    x = np.asarray(x, dtype=np.float64)
+    ky, kx = gaussian_taps(sigma_y), gaussian_taps(sigma_x)
+    ry, rx = len(ky) // 2, len(kx) // 2
+    H, W = x.shape[-2:]
+    xi = np.clip(np.arange(W)[:, None] + np.arange(-rx, rx + 1)[None, :], 0, W - 1)   # [W][taps]
+    tmp = np.einsum("...yk,k->...y", x[..., :, xi].reshape(*x.shape[:-1], W, len(kx)), kx)
+    yi = np.clip(np.arange(H)[:, None] + np.arange(-ry, ry + 1)[None, :], 0, H - 1)   # [H][taps]
+    bg = np.einsum("...hkw,k->...hw", tmp[..., yi, :], ky)
+    return x - bg
+
+
+def _six_decimals(v: float) -> float:
+    """std::to_string(float): the value the reference's JIT source holds (flatfield.cu:124-131)."""
+    return float("%f" % float(np.float32(v)))
+
+
+def flatfield_fourier(x: np.ndarray, sigma_y: float, sigma_x: float) -> np.ndarray:
+    """flatfield.cu:121-158, 229-233: R2C FFT, x (1 - exp(-2 pi^2 (sx^2 fx^2 + sy^2 fy^2))) * SCALE,
+    C2R FFT (unnormalized), with sigma and SCALE = 1 / (W H) at six decimals as the JIT source has
+    them."""
+    x = np.asarray(x, dtype=np.float64)
+    H, W = x.shape[-2:]
+    sy, sx = _six_decimals(sigma_y), _six_decimals(sigma_x)
+    scale = _six_decimals(1.0 / (W * H))
+    fx = np.arange(W // 2 + 1) / W
+    y = np.arange(H)
+    fy = np.where(y <= H // 2, y, y - H) / H
+    low = np.exp(-2.0 * math.pi ** 2 * (sx * sx * fx[None, :] ** 2 + sy * sy * fy[:, None] ** 2))
+    gain = (1.0 - low) * scale
+    spec = np.fft.rfft2(x, axes=(-2, -1)) * gain
+    return np.fft.irfft2(spec, s=(H, W), axes=(-2, -1)) * (W * H)
+
+
+def ellipse_mask(depth: int, height: int, width: int, cx: float, cy: float, rx: float, ry: float,
+                 angle: float) -> np.ndarray:
+    """in_ellipse (pct_clip.cu:91-110) in float32 for a zero angle (cos = 1, sin = 0 exactly)."""
+    if angle != 0.0:
+        raise ValueError("the float32 restatement covers angle 0 only")
+    f = np.float32
+    xn = (np.arange(width, dtype=f) + f(0.5)) / f(width)
+    yn = (np.arange(height, dtype=f) + f(0.5)) / f(height)
+    dx, dy = xn[None, :] - f(cx), yn[:, None] - f(cy)
+    m = (dx * dx) / (f(rx) * f(rx)) + (dy * dy) / (f(ry) * f(ry)) <= f(1.0)
+    return np.broadcast_to(m, (depth, height, width))
+
+
+def pct_clip(x: np.ndarray, min_pct: float, max_pct: float, mask: np.ndarray):
+    """pct_clip.cu:117-145, 283-296: sort the masked values, take ranks int(p/100 (n-1)) in float32,
+    clip every pixel to them.  Returns (clipped float32, lo, hi)."""
+    v = np.sort(np.asarray(x, dtype=np.float32)[mask])
+    n = v.size
+    lo_i = int(np.float32(min_pct) / np.float32(100.0) * np.float32(n - 1))
+    hi_i = int(np.float32(max_pct) / np.float32(100.0) * np.float32(n - 1))
+    lo, hi = v[lo_i], v[hi_i]
+    return np.minimum(np.maximum(np.asarray(x, dtype=np.float32), lo), hi), lo, hi
+
+
+def slide_avg(images: Sequence[np.ndarray], window: int, discard_first: int = 0) -> list:
+    """slide_avg.cu:211-250 in float32: avg += x / n; avg -= x_(k-n) / n (zeros before the first
+    n images); one output per image once n images have entered."""
+    f = np.float32
+    n = f(window)
+    avg, ring, outs, k = None, [], [], 0
+    for i, img in enumerate(images):
+        if i < discard_first:
+            continue
+        img = np.asarray(img, dtype=f)
+        if avg is None:
+            avg = np.zeros_like(img)
+            ring = [np.zeros_like(img) for _ in range(window)]
+        old = ring[k % window]
+        avg = (avg + img / n).astype(f)
+        avg = (avg - old / n).astype(f)
+        ring[k % window] = img
+        k += 1
+        if k >= window:
+            outs.append(avg.copy())
+    return outs

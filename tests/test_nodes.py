@@ -39,7 +39,7 @@ def invalid(kind, settings, descs, fragment):
 
 def test_reference_kinds_are_registered():
     assert set(N.kinds()) == {"FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
-                              "Conversion", "Holofile", "DopplerMoments"}
+                              "Conversion", "Holofile", "FFTShiftNp", "Flatfield", "PctClip", "DopplerMoments"}
 
 
 def test_unknown_kind_and_bad_settings():
@@ -129,3 +129,28 @@ def test_doppler_moments_infer():
             p + "height x width must match the packed frame size")
     invalid("DopplerMoments", {**s, "time_z_end": 40}, [desc([2, 32, 64, 64], U16)], p + "bad band")
     invalid("DopplerMoments", {**s, "moments": ["M3"]}, [desc([2, 32, 64, 64], U16)], p + "moments must be among")
+
+
+def test_display_chain_infer():
+    """FFTShiftNp (fftshift.cu:185-210), Flatfield (flatfield.cu:296-323), PctClip
+    (pct_clip.cu:230-270): output descriptors and messages."""
+    assert out_of("FFTShiftNp", {"axes": [-2, -1]}, [desc([1, 64, 48])]) == ((1, 64, 48), F32)
+    assert out_of("FFTShiftNp", {}, [desc([3, 5], U8)]) == ((3, 5), U8)
+    for s, msg in [({"axes": [2]}, "axis out of range"), ({"axes": [0, -2]}, "axes must be unique")]:
+        invalid("FFTShiftNp", s, [desc([4, 4])], "FFTShift: " + msg)
+    invalid("FFTShiftNp", {}, [desc([4, 4], device=False)], "FFTShift: only Device tensors are supported")
+    assert out_of("Flatfield", {"sigma_y": 3.0, "sigma_x": 2.0}, [desc([2, 64, 64])]) == ((2, 64, 64), F32)
+    p = "FlatfieldFactory inference error: "
+    invalid("Flatfield", {"sigma_y": 0.0, "sigma_x": 2.0}, [desc([64, 64])], p + "sigma_y must be positive")
+    invalid("Flatfield", {"sigma_y": 1.0, "sigma_x": -1.0}, [desc([64, 64])], p + "sigma_x must be positive")
+    invalid("Flatfield", {"sigma_y": 1.0, "sigma_x": 1.0}, [desc([64])], p + "input must be a tensor of rank 2 or higher")
+    invalid("Flatfield", {"sigma_y": 1.0, "sigma_x": 1.0}, [desc([8, 8], U16)], p + "input must be float32")
+    roi = {"cx": 0.5, "cy": 0.5, "rx": 0.5, "ry": 0.5, "angle": 0.0}
+    pc = {"min_pct": 1.0, "max_pct": 99.0, "roi": roi}
+    assert out_of("PctClip", pc, [desc([1, 32, 32])]) == ((1, 32, 32), F32)
+    p = "PctClipFactory inference error: "
+    invalid("PctClip", {**pc, "min_pct": 99.0}, [desc([1, 8, 8])], p + "min_pct must be < max_pct")
+    invalid("PctClip", {**pc, "max_pct": 101.0}, [desc([1, 8, 8])], p + "max_pct must be <= 100")
+    invalid("PctClip", {**pc, "roi": {**roi, "rx": 0.0}}, [desc([1, 8, 8])], p + "roi.rx must be > 0")
+    invalid("PctClip", {**pc, "roi": {**roi, "cy": 1.5}}, [desc([1, 8, 8])], p + "roi.cy must be <= 1")
+    invalid("PctClip", pc, [desc([8, 8])], p + "input must be 3D")
