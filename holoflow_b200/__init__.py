@@ -17,6 +17,7 @@ LIB_PATH = _HERE / "_lib" / "libholoflow_b200.so"
 # status codes / enums (include/holoflow_b200.h)
 HF_OK, HF_ERR_INVALID, HF_ERR_CUDA, HF_ERR_UNSUPPORTED, HF_ERR_NOMEM, HF_ERR_TIMEOUT = 0, -1, -2, -3, -4, -5
 HF_ERR_STATE, HF_ERR_CANCELLED = -6, -7
+HF_TIME_RFFT, HF_TIME_FFT = 0, 1  # one-sided band / two-sided method (graph_builder.cc:270-287)
 HF_U8, HF_U16, HF_F32, HF_CF32, HF_MONO12P = 0, 1, 2, 3, 16
 HF_CONV_REAL, HF_CONV_SCALED, HF_CONV_MODULUS, HF_CONV_ARGUMENT = 0, 1, 2, 3
 HF_NORM_BACKWARD, HF_NORM_FORWARD, HF_NORM_ORTHO = 0, 1, 2
@@ -40,7 +41,7 @@ class HfDesc(C.Structure):
         ("lambda_", C.c_float), ("pitch", C.c_float), ("z", C.c_float), ("fs", C.c_float),
         ("pad_w", C.c_int32), ("pad_h", C.c_int32), ("as_filter", C.c_int32),
         ("r_inner", C.c_uint32), ("r_outer", C.c_uint32), ("s_inner", C.c_uint32),
-        ("s_outer", C.c_uint32),
+        ("s_outer", C.c_uint32), ("time_method", C.c_int32),
     ]
 
 

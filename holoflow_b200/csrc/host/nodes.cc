@@ -137,6 +137,7 @@ void from_json(const nlohmann::json &j, DopplerMomentsSettings &s) {
   opt("moments", s.moments);
   opt("fftshift", s.fftshift);
   opt("form", s.form);
+  opt("time_method", s.time_method);
   if (j.contains("filter"))
     s.filter = j.at("filter").get<AngularSpectrumFilter>();
   if (j.contains("padding"))
@@ -776,6 +777,9 @@ DopplerPlan doppler_plan(const Check &check, const TDesc &idesc, const DopplerMo
   check(dp.nwin >= 1, "expected at least one window");
   d.z_begin = s.time_z_begin, d.z_end = s.time_z_end;
   check(s.time_z_begin >= 0 && s.time_z_end > s.time_z_begin && s.time_z_end <= d.frames, "bad band [time_z_begin, time_z_end)");
+  check(s.time_method == "rfft" || s.time_method == "fft", "time_method must be rfft or fft");
+  d.time_method = s.time_method == "fft" ? HF_TIME_FFT : HF_TIME_RFFT;
+  check((s.time_z_end - s.time_z_begin) * (d.time_method == HF_TIME_FFT ? 2 : 1) <= 64, "at most 64 band planes");
   d.clutter_rank = s.clutter_rank;
   if (s.propagation == "fresnel")
     d.propagation = HF_PROP_FRESNEL;

@@ -41,14 +41,20 @@ inline float norm_scale(int norm, int n) {
 inline bool real_fmt(int f) { return f == HF_U8 || f == HF_U16 || f == HF_F32 || f == HF_MONO12P; }
 
 // f_k = start + k*df evaluated in double and cast (arange.cu:62-75); f_k^2 in float32
-// (graph_builder.cc:624-627).
-inline void fill_weights(MomentSpec &m, int T, int z0, int nz, double fs) {
-  const double df = fs / (double)T;
-  const double f0 = z0 * df;
+// (graph_builder.cc:624-627).  The two-sided method's nz planes are the positive band's nz / 2
+// and then the negative band's, weighted arange(f0 - fs, f1 - fs, df) (graph_builder.cc:590-594).
+inline void fill_weights(MomentSpec &m, int T, int z0, int nz, double fs, bool two_sided = false) {
+  const double df  = fs / (double)T;
+  const double f0  = z0 * df;
+  const int    nzh = two_sided ? nz / 2 : nz;
   for (int k = 0; k < kMaxBands; ++k) {
-    const float f = k < nz ? (float)(f0 + df * (double)k) : 0.f;
-    m.w1[k]       = f;
-    m.w2[k]       = f * f;
+    float f = 0.f;
+    if (k < nzh)
+      f = (float)(f0 + df * (double)k);
+    else if (k < nz)
+      f = (float)((f0 - fs) + df * (double)(k - nzh));
+    m.w1[k] = f;
+    m.w2[k] = f * f;
   }
 }
 

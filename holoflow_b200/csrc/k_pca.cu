@@ -441,11 +441,17 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(const double *a_
     info[blockIdx.x] = (sweep >= max_sweeps) ? sweep : 0;
 }
 
-// W = (I - V V^T) D[:, z0:z1]; one CTA per window.
-__global__ void band_matrix_kernel(const double *evecs, int T, int rank, int z0, int z1,
+// W = (I - V V^T) D[:, bins]; one CTA per window.  bins = [z0, z1), followed for the two-sided
+// method by [T - z1, T - z0) (graph_builder.cc:270-287: the positive then the negative band).
+__device__ __forceinline__ int band_bin(int kk, int z0, int z1, int T) {
+  const int nzh = z1 - z0;
+  return kk < nzh ? z0 + kk : T - z1 + (kk - nzh);
+}
+
+__global__ void band_matrix_kernel(const double *evecs, int T, int rank, int z0, int z1, int two_sided,
                                    float2 *wmat) {
   extern __shared__ __align__(16) double bsm[];
-  const int     nz = z1 - z0;
+  const int     nz = (z1 - z0) * (two_sided ? 2 : 1);
   const double *V  = evecs + (int64_t)blockIdx.x * T * T;
   double       *cr = bsm;            // [rank][nz] re
   double       *ci = bsm + rank * nz; // [rank][nz] im
@@ -455,7 +461,7 @@ __global__ void band_matrix_kernel(const double *evecs, int T, int rank, int z0,
     double    sr = 0.0, si = 0.0;
     for (int t = 0; t < T; ++t) {
       double s, c;
-      sincospi(-2.0 * (double)((t * (z0 + kk)) % T) / (double)T, &s, &c);
+      sincospi(-2.0 * (double)((t * band_bin(kk, z0, z1, T)) % T) / (double)T, &s, &c);
       sr += V[t * T + col] * c;
       si += V[t * T + col] * s;
     }
@@ -466,7 +472,7 @@ __global__ void band_matrix_kernel(const double *evecs, int T, int rank, int z0,
   for (int e = threadIdx.x; e < T * nz; e += blockDim.x) {
     const int t = e / nz, kk = e % nz;
     double    s, c;
-    sincospi(-2.0 * (double)((t * (z0 + kk)) % T) / (double)T, &s, &c);
+    sincospi(-2.0 * (double)((t * band_bin(kk, z0, z1, T)) % T) / (double)T, &s, &c);
     double wr = c, wi = s;
     for (int m = 0; m < rank; ++m) {
       const double v = V[t * T + (T - rank + m)];
@@ -546,12 +552,12 @@ int launch_jacobi(const double *a, double *evecs, double *evals, int *info, int 
 }
 
 int launch_band_matrix(const double *evecs, int64_t batch, int T, int rank, int z0, int z1,
-                       float2 *wmat, cudaStream_t s) {
-  HF_CHECK_ARG(T > 0 && z0 >= 0 && z1 > z0 && rank >= 0 && rank <= T, "band matrix: bad range");
-  const size_t smem = (size_t)2 * std::max(rank, 1) * (z1 - z0) * sizeof(double);
+                       float2 *wmat, cudaStream_t s, bool two_sided) {
+  HF_CHECK_ARG(T > 0 && z0 >= 0 && z1 > z0 && z1 <= T && rank >= 0 && rank <= T, "band matrix: bad range");
+  const size_t smem = (size_t)2 * std::max(rank, 1) * (z1 - z0) * (two_sided ? 2 : 1) * sizeof(double);
   HF_CUDA(cudaFuncSetAttribute(band_matrix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem));
-  band_matrix_kernel<<<(unsigned)batch, 256, smem, s>>>(evecs, T, rank, z0, z1, wmat);
+  band_matrix_kernel<<<(unsigned)batch, 256, smem, s>>>(evecs, T, rank, z0, z1, two_sided ? 1 : 0, wmat);
   note_launch();
   return launch_status("band_matrix_kernel");
 }

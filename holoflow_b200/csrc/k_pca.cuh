@@ -43,8 +43,9 @@ int launch_jacobi(const double *a, double *evecs, double *evals, int *info, int 
                   cudaStream_t s);
 
 // W = (I - V V^T) D[:, z0:z1] as complex64 [batch][T][nz]; V = last `rank` columns of evecs.
+// two_sided: columns for bins [z0, z1) then [T - z1, T - z0) (2 (z1 - z0) columns)
 int launch_band_matrix(const double *evecs, int64_t batch, int T, int rank, int z0, int z1,
-                       float2 *wmat, cudaStream_t s);
+                       float2 *wmat, cudaStream_t s, bool two_sided = false);
 
 int launch_pca_project(const float *in, int64_t batch, int T, int64_t P, const double *evecs,
                        int begin, int end, float *out, cudaStream_t s);

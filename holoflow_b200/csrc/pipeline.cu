@@ -155,7 +155,8 @@ static int phase_eigen(hf_plan *p, const FilterSet &fs, int nwin, cudaStream_t s
   const hf_desc &d   = p->d;
   const int      rec = p->timer.begin(s, ST_EIGEN);
   HF_TRY(launch_jacobi(fs.gram, fs.evecs, fs.evals, fs.info, d.frames, nwin, s));
-  HF_TRY(launch_band_matrix(fs.evecs, nwin, d.frames, d.clutter_rank, d.z_begin, d.z_end, fs.wmat, s));
+  HF_TRY(launch_band_matrix(fs.evecs, nwin, d.frames, d.clutter_rank, d.z_begin, d.z_end, fs.wmat, s,
+                            d.time_method == HF_TIME_FFT));
   p->timer.end(s, rec);
   return HF_OK;
 }
@@ -294,7 +295,9 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
   HF_CHECK_ARG(d.hop >= 1, "plan: hop must be >= 1");
   HF_CHECK_ARG(d.z_begin >= 0 && d.z_end > d.z_begin && d.z_end <= d.frames,
                "plan: band must satisfy 0 <= z_begin < z_end <= frames");
-  HF_CHECK_ARG(d.z_end - d.z_begin <= kMaxBands, "plan: at most 64 band bins");
+  HF_CHECK_ARG(d.time_method == HF_TIME_RFFT || d.time_method == HF_TIME_FFT, "plan: unknown time method");
+  HF_CHECK_ARG((d.z_end - d.z_begin) * (d.time_method == HF_TIME_FFT ? 2 : 1) <= kMaxBands,
+               "plan: at most 64 band planes (32 bins for the two-sided method)");
   HF_CHECK_ARG(d.input_dtype == HF_MONO12P || d.input_dtype == HF_U16 || d.input_dtype == HF_U8 ||
                    d.input_dtype == HF_F32,
                "plan: input dtype must be MONO12P, U16, U8 or F32");
@@ -322,7 +325,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
     return fail(HF_ERR_NOMEM, "plan: host allocation failed");
   p->d           = d;
   p->P           = d.height * d.width;
-  p->nz          = d.z_end - d.z_begin;
+  p->nz          = (d.z_end - d.z_begin) * (d.time_method == HF_TIME_FFT ? 2 : 1);
   p->nmom        = __builtin_popcount(d.moment_mask);
   p->OH          = OH;
   p->OW          = OW;
@@ -332,7 +335,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
   p->mom.mask     = d.moment_mask;
   p->mom.fftshift = d.fftshift;
   p->mom.inv_nz   = 1.0f / (float)p->nz;
-  fill_weights(p->mom, d.frames, d.z_begin, p->nz, d.fs > 0.f ? d.fs : 37e3);
+  fill_weights(p->mom, d.frames, d.z_begin, p->nz, d.fs > 0.f ? d.fs : 37e3, d.time_method == HF_TIME_FFT);
 
   const int64_t B  = d.max_batch;
   const int     T  = d.frames;
@@ -368,14 +371,17 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
     } else {
       if ((rc = dev_alloc(&p->wmat_plain, (size_t)T * p->nz, p->bytes)))
         break;
-      if ((rc = launch_band_matrix(nullptr, 1, T, 0, d.z_begin, d.z_end, p->wmat_plain, stream)))
+      if ((rc = launch_band_matrix(nullptr, 1, T, 0, d.z_begin, d.z_end, p->wmat_plain, stream,
+                                   d.time_method == HF_TIME_FFT)))
         break;
     }
     if ((rc = dev_alloc(&p->status, 1, p->bytes)) || (rc = dev_alloc(&p->row_counter, 1, p->bytes)))
       break;
     if ((rc = cuda_status(cudaMemsetAsync(p->status, 0, sizeof(int), stream), "status reset")))
       break;
+    // the tensor-core band pass holds 2 (z1 - z0) real columns per pixel: the one-sided band only
     p->rows_tc = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
+                 d.time_method == HF_TIME_RFFT &&
                  band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
     if (d.propagation == HF_PROP_FRESNEL && p->fast && col_moments_tma_supported(d.height, d.width)) {
       const uint64_t rows = (uint64_t)B * p->nz * d.height;

@@ -97,13 +97,14 @@ class PipelineConfig:
     r_outer: int = 0
     s_inner: int = 0
     s_outer: int = 0
+    time_method: int = 0  # HF_TIME_RFFT; HF_TIME_FFT = two-sided band, 2 (z_end - z_begin) planes
 
     def desc(self) -> HfDesc:
         return HfDesc(self.height, self.width, self.frames, self.hop, self.z_begin, self.z_end,
                       self.input_dtype, self.propagation, self.clutter_rank, self.moment_mask,
                       self.fftshift, self.form, self.max_batch, self.lam, self.pitch, self.z, self.fs,
                       self.pad_w, self.pad_h, self.as_filter, self.r_inner, self.r_outer,
-                      self.s_inner, self.s_outer)
+                      self.s_inner, self.s_outer, self.time_method)
 
     @property
     def frame_bytes(self) -> int:
@@ -140,7 +141,7 @@ class Pipeline:
         return out
 
     def inspect(self, w: int = 0):
-        T, nz = self.cfg.frames, self.cfg.z_end - self.cfg.z_begin
+        T, nz = self.cfg.frames, (self.cfg.z_end - self.cfg.z_begin) * (2 if self.cfg.time_method else 1)
         gram = torch.empty((T, T), dtype=torch.float64, device="cuda") if self.cfg.clutter_rank else None
         wm = torch.empty((T, nz), dtype=torch.complex64, device="cuda")
         check(lib().hf_pipeline_inspect(self._plan, w, _ptr(gram), _ptr(wm), _stream()))

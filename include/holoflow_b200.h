@@ -197,7 +197,12 @@ typedef struct hf_desc {
   int32_t pad_w, pad_h;      /* angular-spectrum padding (0 = none)                           */
   int32_t as_filter;         /* angular-spectrum raised-sine annulus on/off                   */
   uint32_t r_inner, r_outer, s_inner, s_outer;
+  int32_t time_method;       /* HF_TIME_RFFT (0): the band [z0, z1); HF_TIME_FFT: the two-sided
+                                method, [z0, z1) then [T - z1, T - z0), 2 (z1 - z0) planes
+                                (graph_builder.cc:270-287, weights 590-594)                   */
 } hf_desc;
+#define HF_TIME_RFFT 0
+#define HF_TIME_FFT 1
 
 typedef struct hf_plan hf_plan;
 /* Allocates every device buffer the path needs for max_batch windows (reference create()). */

@@ -58,6 +58,7 @@ struct DopplerMomentsSettings {
   std::vector<std::string>              moments{"M0", "M1", "M2"};
   bool                                  fftshift = false;
   std::string                           form     = "plain";               // plain | chosen
+  std::string                           time_method = "rfft";            // rfft | fft (settings.hh TimeMethod)
   std::optional<AngularSpectrumFilter>  filter;
   std::optional<AngularSpectrumPadding> padding;
 };

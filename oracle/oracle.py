@@ -240,10 +240,17 @@ def svd_filter(frames: np.ndarray, rank: int) -> np.ndarray:
     return (Xf - V @ (V.T @ Xf)).reshape(X.shape)
 
 
-def band_matrix(T: int, z0: int, z1: int, V: Optional[np.ndarray] = None) -> np.ndarray:
-    """W = (I - V V^T) D[:, z0:z1], the T x Nz complex matrix one window's filter+DFT reduces to."""
+def band_bin_list(T: int, z0: int, z1: int, method: str = "rfft") -> np.ndarray:
+    """The DFT bins of the band planes: [z0, z1), and for the two-sided FFT method also the
+    negative band [T - z1, T - z0) after it (graph_builder.cc:270-287: slice, slice, concatenate)."""
+    pos = np.arange(z0, z1)
+    return np.concatenate([pos, np.arange(T - z1, T - z0)]) if method == "fft" else pos
+
+
+def band_matrix(T: int, z0: int, z1: int, V: Optional[np.ndarray] = None, method: str = "rfft") -> np.ndarray:
+    """W = (I - V V^T) D[:, bins], the T x Nz complex matrix one window's filter+DFT reduces to."""
     t = np.arange(T)[:, None]
-    k = np.arange(z0, z1)[None, :]
+    k = band_bin_list(T, z0, z1, method)[None, :]
     D = np.exp(-2j * np.pi * (t * k % T) / T)
     if V is not None and V.shape[1]:
         D = D - V @ (V.T @ D)
@@ -494,17 +501,18 @@ class PathConfig:
     as_filter: Optional[dict] = None
     as_padding: Optional[dict] = None
     phase_mode: str = "f32"
+    time_method: str = "rfft"      # "rfft" (one-sided band) | "fft" (two-sided, 2 Nz planes)
 
     @property
     def nz(self) -> int:
-        return self.z1 - self.z0
+        return (self.z1 - self.z0) * (2 if self.time_method == "fft" else 1)
 
 
 def band_planes(window: np.ndarray, cfg: PathConfig) -> np.ndarray:
     """[Nz, H, W] complex: SVD filter (optional) then the band DFT along time."""
     X = np.asarray(window, dtype=np.float64).reshape(cfg.frames, -1)
     V = clutter_basis(X, cfg.clutter_rank) if cfg.clutter_rank else None
-    Wm = band_matrix(cfg.frames, cfg.z0, cfg.z1, V)
+    Wm = band_matrix(cfg.frames, cfg.z0, cfg.z1, V, cfg.time_method)
     S = Wm.T @ X  # [Nz, P]
     return S.reshape(cfg.nz, cfg.height, cfg.width)
 
@@ -524,7 +532,7 @@ def propagate(planes: np.ndarray, cfg: PathConfig) -> np.ndarray:
 def reconstruct_window(window: np.ndarray, cfg: PathConfig) -> np.ndarray:
     """One T-frame window -> float64 [3, H', W'] (M0, M1, M2)."""
     mag = propagate(band_planes(window, cfg), cfg)
-    w = freq_weights(cfg.frames, cfg.z0, cfg.z1, cfg.fs)
+    w = freq_weights(cfg.frames, cfg.z0, cfg.z1, cfg.fs, cfg.time_method)
     return moments_from_magnitude(mag, w, cfg.fftshift)
 
 

@@ -290,3 +290,39 @@ def test_config2_clutter_error_vs_fp64_oracle(cuda, scr_db):
         errs = [O.rel_l2(got[w, m], exp[w][m]) for w in range(2) for m in range(3)]
         print(f"config2 SCR {scr_db:+.0f} dB form {form}: max rel L2 {max(errs):.3e}")
         assert max(errs) < tol, errs
+
+
+@pytest.mark.parametrize("form,prop,H", [(0, "fresnel", 256), (1, "fresnel", 256), (1, "fresnel", 1024),
+                                         (0, "angular_spectrum", 128)])
+def test_two_sided_fft_time_method(cuda, form, prop, H):
+    """The reference's FFT time method (graph_builder.cc:270-287): the band [z0, z1) and the
+    negative band [T - z1, T - z0) concatenated, 2 Nz planes propagated, moments weighted
+    [f0 .. f1) then [f0 - fs .. f1 - fs) (590-594); against the float64 oracle within the form's
+    tolerance (1e-4 plain, 1e-3 chosen)."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    W = H
+    nwin = 2
+    n = 64 + 16 * (nwin - 1)
+    z0, z1 = O.band_bins(4e3, 33e3, 67e3, 64) if prop == "fresnel" else (6, 16)
+    frames = S.Interferograms(S.config1(n, height=H, width=W)).frames(0, n)
+    ring = torch.from_numpy(O.pack12(frames.reshape(-1))).to(cuda)
+    cfg = pl.PipelineConfig(height=H, width=W, frames=64, hop=16, z_begin=z0, z_end=z1, fs=67e3, z=0.25,
+                            clutter_rank=4, form=form, max_batch=nwin, time_method=hf.HF_TIME_FFT,
+                            propagation=hf.HF_PROP_FRESNEL if prop == "fresnel" else hf.HF_PROP_ANGULAR_SPECTRUM)
+    p = pl.Pipeline(cfg)
+    got = p.run(ring, n, 0, nwin).cpu().numpy()
+    assert p.status() == 0
+    ocfg = O.PathConfig(H, W, 64, 16, z0, z1, fs=67e3, z=0.25, clutter_rank=4, propagation=prop,
+                        time_method="fft")
+    tol = 1e-4 if form == 0 else 1e-3
+    for w in range(nwin):
+        exp = O.reconstruct_window(frames[16 * w:16 * w + 64], ocfg)
+        for m in range(3):
+            err = O.rel_l2(got[w, m], exp[m])
+            assert err < tol, (w, m, err)
+    # the negative band's weights are negative: M1 differs from the one-sided method's
+    one = pl.Pipeline(pl.PipelineConfig(**{**cfg.__dict__, "time_method": hf.HF_TIME_RFFT}))
+    got1 = one.run(ring, n, 0, nwin).cpu().numpy()
+    assert O.rel_l2(got1[0, 1], got[0, 1]) > 0.1

@@ -154,3 +154,14 @@ def test_display_chain_infer():
     invalid("PctClip", {**pc, "roi": {**roi, "rx": 0.0}}, [desc([1, 8, 8])], p + "roi.rx must be > 0")
     invalid("PctClip", {**pc, "roi": {**roi, "cy": 1.5}}, [desc([1, 8, 8])], p + "roi.cy must be <= 1")
     invalid("PctClip", pc, [desc([8, 8])], p + "input must be 3D")
+
+
+def test_doppler_moments_two_sided_time_method():
+    s = {"time_z_begin": 4, "time_z_end": 32, "propagation": "fresnel", "lambda": 852e-9, "dx": 12e-6, "z": 0.25,
+         "input_format": "u16", "time_method": "fft"}
+    assert out_of("DopplerMoments", s, [desc([1, 64, 64, 64], U16)]) == ((1, 3, 64, 64), F32)
+    p = "DopplerMomentsFactory inference error: "
+    invalid("DopplerMoments", {**s, "time_method": "stft"}, [desc([1, 64, 64, 64], U16)],
+            p + "time_method must be rfft or fft")
+    invalid("DopplerMoments", {**s, "time_z_begin": 0, "time_z_end": 33}, [desc([1, 64, 64, 64], U16)],
+            p + "at most 64 band planes")
