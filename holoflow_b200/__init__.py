@@ -140,6 +140,10 @@ _PROTOS = {
     "hf_flatfield_is_fourier": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "hf_flatfield_exec": (C.c_int, [_vp, _vp, _vp, _vp]),
     "hf_flatfield_destroy": (C.c_int, [_vp]),
+    "hf_filter2d_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, _vp, C.POINTER(_vp)]),
+    "hf_filter2d_exec": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "hf_filter2d_destroy": (C.c_int, [_vp]),
     "hf_pctclip_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.POINTER(HfEllipse), _vp,
                                     C.POINTER(_vp)]),
     "hf_pctclip_roi_count": (C.c_int, [_vp, C.POINTER(C.c_int)]),

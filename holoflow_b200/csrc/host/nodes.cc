@@ -888,6 +888,12 @@ void from_json(const nlohmann::json &j, FlatfieldSettings &s) {
   j.at("sigma_y").get_to(s.sigma_y);
   j.at("sigma_x").get_to(s.sigma_x);
 }
+void from_json(const nlohmann::json &j, Filter2DSettings &s) {
+  j.at("r_inner").get_to(s.r_inner);
+  j.at("r_outer").get_to(s.r_outer);
+  j.at("s_inner").get_to(s.s_inner);
+  j.at("s_outer").get_to(s.s_outer);
+}
 void from_json(const nlohmann::json &j, PctClipSettings &s) {
   j.at("min_pct").get_to(s.min_pct);
   j.at("max_pct").get_to(s.max_pct);
@@ -945,6 +951,19 @@ public:
     hf_ok(hf_flatfield_exec(ff, reinterpret_cast<const float *>(ctx.inputs[0].data()),
                             reinterpret_cast<float *>(ctx.outputs[0].data()), stream),
           "Flatfield");
+    return OpResult::Ok;
+  }
+};
+
+class Filter2DTask final : public ISyncTask {
+public:
+  hf_filter2d     *f = nullptr;
+  Filter2DSettings settings;
+  TDesc            idesc;
+  cudaStream_t     stream{};
+  ~Filter2DTask() override { hf_filter2d_destroy(f); }
+  OpResult execute(SyncCtx &ctx) override {
+    hf_ok(hf_filter2d_exec(f, ctx.inputs[0].data(), ctx.outputs[0].data(), stream), "Filter2D");
     return OpResult::Ok;
   }
 };
@@ -1047,6 +1066,53 @@ std::unique_ptr<ISyncTask> FlatfieldFactory::update(std::unique_ptr<ISyncTask> o
   return create(input_descs, j, ctx);
 }
 
+// filter2d.cu:262-297: the same checks; complex input is filtered in place
+InferResult Filter2DFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"Filter2DFactory"};
+  (void)j.get<Filter2DSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &idesc = input_descs[0];
+  check(idesc.rank() >= 2, "input must be a tensor of rank 2 or higher");
+  check(idesc.dtype == DType::CF32 || idesc.dtype == DType::F32, "input must be complex float32 or real float32");
+  check(idesc.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(idesc.is_contiguous(), "input must be C-contiguous");
+  std::vector<core::InPlace> in_place;
+  if (idesc.dtype == DType::CF32)
+    in_place.push_back({0, 0});
+  return sync_result(idesc, idesc, std::move(in_place));
+}
+
+std::unique_ptr<ISyncTask> Filter2DFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                   const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<Filter2DTask>();
+  t->settings = j.get<Filter2DSettings>();
+  t->idesc    = input_descs[0];
+  t->stream   = ctx.stream;
+  const size_t r = t->idesc.rank();
+  int64_t      planes = 1;
+  for (size_t i = 0; i + 2 < r; ++i)
+    planes *= (int64_t)t->idesc.shape[i];
+  const auto &s = t->settings;
+  hf_ok(hf_filter2d_create(planes, (int)t->idesc.shape[r - 2], (int)t->idesc.shape[r - 1],
+                           t->idesc.dtype == DType::F32 ? 1 : 0, s.r_inner, s.r_outer, s.s_inner, s.s_outer, ctx.stream,
+                           &t->f),
+        "Filter2D");
+  return t;
+}
+
+std::unique_ptr<ISyncTask> Filter2DFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> input_descs,
+                                                   const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<Filter2DTask *>(old.get());
+  if (t && t->settings == j.get<Filter2DSettings>() && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
 InferResult PctClipFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
   const Check check{"PctClipFactory"};
   const auto  s = j.get<PctClipSettings>();
@@ -1115,6 +1181,7 @@ void register_path_kinds(core::Registry &r) {
   r.register_sync("Holofile", std::make_unique<HolofileFactory>());
   r.register_sync("FFTShiftNp", std::make_unique<FFTShiftFactory>());
   r.register_sync("Flatfield", std::make_unique<FlatfieldFactory>());
+  r.register_sync("Filter2D", std::make_unique<Filter2DFactory>());
   r.register_sync("PctClip", std::make_unique<PctClipFactory>());
 }
 

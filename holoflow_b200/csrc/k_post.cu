@@ -31,6 +31,7 @@
 
 #include "hf_common.cuh"
 #include "k_fft2d.cuh"
+#include "k_post.cuh"
 
 namespace hf {
 namespace {
@@ -146,6 +147,47 @@ __global__ void flatfield_gain_kernel(float2 *gain, int H, int W, float sy, floa
 __global__ void real_part_kernel(const float2 *__restrict__ c, float *__restrict__ out, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = c[i].x;
+}
+
+// ------------------------------------------------------------------------------------------------
+// filter2d (holotask/src/syncs/filter2d.cu:109-199): the band-pass annulus a (1 - b) in the
+// transform's natural frequency order.  Complex input: the reference builds the centred mask,
+// swaps its corners (fftshift for even sides) and stores (g, g) -- a complex factor sqrt(2)
+// e^(i pi / 4) that is kept here.  Real input: the R2C half spectrum's (g, 0) with the
+// `smooth > 0` guards, extended to the full spectrum by the symmetry of |f|.
+// ------------------------------------------------------------------------------------------------
+__device__ float annulus(float dist, float ri, float ro, float si, float so, bool guards) {
+  float a = 0.0f, b = 0.0f;
+  if (dist < ro)
+    a = 1.0f;
+  else if ((!guards || so > 0.0f) && dist < ro + so)
+    a = cosf((dist - ro) / so * 3.14159265358979323846f / 2);
+  if (dist < ri)
+    b = 1.0f;
+  else if ((!guards || si > 0.0f) && dist < ri + si)
+    b = cosf((dist - ri) / si * 3.14159265358979323846f / 2);
+  return a * (1 - b);
+}
+
+__global__ void filter2d_table_kernel(float2 *tab, int W, int H, uint32_t ri, uint32_t ro, uint32_t si, uint32_t so,
+                                      int real_in) {
+  const int64_t n = (int64_t)H * W;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / W), x = (int)(i % W);
+    float     g;
+    if (real_in) {
+      const int   xf = x <= W / 2 ? x : W - x;
+      const int   fy = y <= H / 2 ? y : y - H;
+      const float dist = hypotf((float)xf, (float)fy);
+      g                = annulus(dist, (float)ri, (float)ro, (float)si, (float)so, true);
+      tab[i]           = make_float2(g, 0.f);
+    } else {
+      const int   xc = (x + W / 2) % W, yc = (y + H / 2) % H; // the centred mask's pixel here
+      const float rx = (float)xc - (float)W / 2, ry = (float)yc - (float)H / 2;
+      g              = annulus(hypotf(rx, ry), (float)ri, (float)ro, (float)si, (float)so, false);
+      tab[i]         = make_float2(g, g);
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -282,6 +324,41 @@ int grid_for(int64_t n, int block = 256) {
 float six_decimals(float v) { return std::stof(std::to_string(v)); }
 
 } // namespace
+
+// out = IFFT2(FFT2(in) x tab) per [H][W] plane, unnormalized both ways (as the reference's cuFFT
+// pair): rows forward into the scratch spectrum c0, the columns' transfer-function sandwich with
+// the mask in place, rows inverse into `out` (complex) or into c1 and its real part (real).
+int launch_filter2d(const float2 *tab, int64_t planes, int H, int W, int real_in, const void *in, void *out,
+                    float2 *c0, float2 *c1, cudaStream_t s) {
+  const int64_t P = (int64_t)H * W;
+  RowPass       rp{};
+  rp.in = in, rp.in_real = real_in, rp.in_win = planes * P, rp.in_plane = P, rp.in_row = W, rp.in_col = 1;
+  rp.IH = H, rp.IW = W, rp.oy = 0, rp.ox = 0, rp.H = H, rp.N = W, rp.nplanes = (int)planes, rp.inverse = 0;
+  rp.out = c0, rp.out_win = planes * P, rp.out_plane = P, rp.out_row = W;
+  HF_TRY(launch_row_pass(rp, 1, s));
+  ColPass cp{};
+  cp.in = c0, cp.in_win = planes * P, cp.in_plane = P, cp.in_row = W, cp.H = H, cp.W = W, cp.nplanes = (int)planes;
+  cp.out = c0, cp.out_win = planes * P, cp.out_plane = P, cp.out_row = W, cp.out_col = 1, cp.tf = tab, cp.inverse = 0;
+  HF_TRY(launch_col_pass(cp, COL_TF_SANDWICH, nullptr, 1, s));
+  RowPass ri = rp;
+  ri.in = c0, ri.in_real = 0, ri.inverse = 1;
+  ri.out = real_in ? c1 : static_cast<float2 *>(out);
+  HF_TRY(launch_row_pass(ri, 1, s));
+  if (!real_in)
+    return HF_OK;
+  real_part_kernel<<<grid_for(planes * P), 256, 0, s>>>(c1, static_cast<float *>(out), planes * P);
+  note_launch();
+  return launch_status("real_part_kernel");
+}
+
+// The annulus mask in natural frequency order for a complex (real_in = 0) or real input.
+int launch_filter2d_table(float2 *tab, int H, int W, int real_in, uint32_t ri, uint32_t ro, uint32_t si, uint32_t so,
+                          cudaStream_t s) {
+  filter2d_table_kernel<<<grid_for((int64_t)H * W), 256, 0, s>>>(tab, W, H, ri, ro, si, so, real_in);
+  note_launch();
+  return launch_status("filter2d_table_kernel");
+}
+
 } // namespace hf
 
 using namespace hf;
@@ -294,6 +371,12 @@ struct hf_flatfield {
   float  *tmp  = nullptr; // spatial: horizontal pass
   float2 *gain = nullptr; // Fourier: [H][W] gain
   float2 *c0 = nullptr, *c1 = nullptr;
+};
+
+struct hf_filter2d {
+  int64_t planes = 0;
+  int     H = 0, W = 0, real_in = 0;
+  float2 *tab = nullptr, *c0 = nullptr, *c1 = nullptr;
 };
 
 struct hf_pctclip {
@@ -316,6 +399,14 @@ void release(hf_flatfield *f) {
   if (f) {
     cudaFree(f->tmp);
     cudaFree(f->gain);
+    cudaFree(f->c0);
+    cudaFree(f->c1);
+    delete f;
+  }
+}
+void release(hf_filter2d *f) {
+  if (f) {
+    cudaFree(f->tab);
     cudaFree(f->c0);
     cudaFree(f->c1);
     delete f;
@@ -487,6 +578,47 @@ int hf_flatfield_exec(hf_flatfield *f, const float *in, float *out, hf_stream_t 
 }
 
 int hf_flatfield_destroy(hf_flatfield *f) {
+  clear_error();
+  release(f);
+  return HF_OK;
+}
+
+int hf_filter2d_create(int64_t planes, int height, int width, int real_input, uint32_t r_inner, uint32_t r_outer,
+                       uint32_t s_inner, uint32_t s_outer, hf_stream_t s, hf_filter2d **out) {
+  clear_error();
+  HF_CHECK_ARG(out != nullptr, "Filter2D: null argument");
+  *out = nullptr;
+  HF_CHECK_ARG(planes >= 1 && height >= 1 && width >= 1, "Filter2D: input must not be empty");
+  if (!(fft_fast_length(height) && fft_fast_length(width) && height <= 1024))
+    return fail(HF_ERR_UNSUPPORTED,
+                "Filter2D: image sides must be in {64, 128, 256, 512, 768, 1024, 1536} (height <= 1024)");
+  auto *f = new (std::nothrow) hf_filter2d();
+  if (!f)
+    return fail(HF_ERR_NOMEM, "Filter2D: host allocation failed");
+  f->planes = planes, f->H = height, f->W = width, f->real_in = real_input ? 1 : 0;
+  const size_t npx = (size_t)planes * height * width;
+  int          rc  = cuda_status(cudaMalloc(&f->tab, (size_t)height * width * sizeof(float2)), "Filter2D: mask");
+  if (rc == HF_OK)
+    rc = cuda_status(cudaMalloc(&f->c0, npx * sizeof(float2)), "Filter2D: spectrum");
+  if (rc == HF_OK && real_input)
+    rc = cuda_status(cudaMalloc(&f->c1, npx * sizeof(float2)), "Filter2D: spectrum");
+  if (rc == HF_OK)
+    rc = launch_filter2d_table(f->tab, height, width, f->real_in, r_inner, r_outer, s_inner, s_outer, s);
+  if (rc != HF_OK) {
+    release(f);
+    return rc;
+  }
+  *out = f;
+  return HF_OK;
+}
+
+int hf_filter2d_exec(hf_filter2d *f, const void *in, void *out, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(f != nullptr && in != nullptr && out != nullptr, "Filter2D: null argument");
+  return launch_filter2d(f->tab, f->planes, f->H, f->W, f->real_in, in, out, f->c0, f->c1, s);
+}
+
+int hf_filter2d_destroy(hf_filter2d *f) {
   clear_error();
   release(f);
   return HF_OK;

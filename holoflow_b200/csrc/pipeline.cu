@@ -21,6 +21,7 @@
 #include "k_fft2d.cuh"
 #include "k_misc.cuh"
 #include "k_pca.cuh"
+#include "k_post.cuh"
 #include "k_tc_band.cuh"
 #include "tma_host.cuh"
 
@@ -99,9 +100,13 @@ struct hf_plan {
   CUtensorMap band_tmap{};
   size_t     bytes = 0;
   StageTimer timer;
+  // Filter2D on the band planes before the Fresnel lens (graph_builder.cc:124-126, 568-576)
+  bool    filter2d = false;
+  float2 *f2d      = nullptr; // [H][W] annulus mask in natural frequency order
 };
 
 static void plan_free(hf_plan *p) {
+  dev_free(p->f2d);
   dev_free(p->lens);
   dev_free(p->tf);
   dev_free(p->band);
@@ -129,6 +134,10 @@ static int plan_tables(hf_plan *p, cudaStream_t s) {
   if (d.propagation == HF_PROP_ANGULAR_SPECTRUM) {
     AsFilter f{d.r_inner, d.r_outer, d.s_inner, d.s_outer};
     HF_TRY(launch_as_tf(p->tf, p->OW, p->OH, d.lambda, d.z, d.pitch, d.as_filter, f, s));
+  }
+  if (p->filter2d && p->f2d == nullptr) { // z-independent: built once
+    HF_TRY(dev_alloc(&p->f2d, (size_t)p->P, p->bytes));
+    HF_TRY(launch_filter2d_table(p->f2d, d.height, d.width, 0, d.r_inner, d.r_outer, d.s_inner, d.s_outer, s));
   }
   return HF_OK;
 }
@@ -212,11 +221,13 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
   BandArgs ba{};
   ba.ring = fr, ba.T = d.frames, ba.P = p->P, ba.H = d.height, ba.W = d.width, ba.nz = p->nz;
   ba.wmat = wmat, ba.wmat_stride = wstride, ba.z0 = d.z_begin;
-  ba.lens = d.propagation == HF_PROP_FRESNEL ? p->lens : nullptr;
+  ba.lens = d.propagation == HF_PROP_FRESNEL && !p->filter2d ? p->lens : nullptr;
   ba.out = p->band, ba.OH = d.height, ba.OW = d.width, ba.oy = 0, ba.ox = 0;
   ba.out_plane = p->P, ba.out_win = win_px, ba.scale = 1.0f;
   int rec = p->timer.begin(s, ST_BAND);
   HF_TRY(launch_band_dft(ba, d.input_dtype, nwin, s));
+  if (p->filter2d) // band planes -> FFT2 x annulus -> IFFT2, in place, before the lens
+    HF_TRY(launch_filter2d(p->f2d, (int64_t)nwin * p->nz, d.height, d.width, 0, p->band, p->band, p->band2, nullptr, s));
   p->timer.end(s, rec);
 
   if (d.propagation == HF_PROP_NONE) {
@@ -235,6 +246,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     rp.in = p->band, rp.in_real = 0, rp.in_win = win_px, rp.in_plane = p->P, rp.in_row = d.width, rp.in_col = 1;
     rp.IH = d.height, rp.IW = d.width, rp.H = d.height, rp.N = d.width, rp.nplanes = p->nz, rp.inverse = 0;
     rp.out = p->fast ? p->band : p->band2, rp.out_win = win_px, rp.out_plane = p->P, rp.out_row = d.width;
+    rp.pre = p->filter2d ? p->lens : nullptr; // the lens, when the band pass could not fuse it
     rec = p->timer.begin(s, ST_ROWS);
     HF_TRY(launch_row_pass(rp, nwin, s));
     p->timer.end(s, rec);
@@ -331,6 +343,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
   p->OW          = OW;
   p->frame_bytes = frame_bytes_of(d.input_dtype, p->P);
   p->fast        = fft_fast_length(OH) && fft_fast_length(OW);
+  p->filter2d    = d.as_filter != 0 && d.propagation != HF_PROP_ANGULAR_SPECTRUM;
   p->mom.nz       = p->nz;
   p->mom.mask     = d.moment_mask;
   p->mom.fftshift = d.fftshift;
@@ -341,10 +354,15 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
   const int     T  = d.frames;
   int           rc = HF_OK;
   do {
+    if (p->filter2d && !(p->fast && d.height <= 1024)) {
+      rc = fail(HF_ERR_UNSUPPORTED, "plan: Filter2D needs frame sides in {64..1536} (height <= 1024)");
+      break;
+    }
     const int64_t plane = (int64_t)p->P, oplane = (int64_t)OH * OW;
     if ((rc = dev_alloc(&p->band, (size_t)(B * p->nz * plane), p->bytes)))
       break;
-    const bool need_band2 = d.propagation == HF_PROP_ANGULAR_SPECTRUM || (d.propagation == HF_PROP_FRESNEL && !p->fast);
+    const bool need_band2 = d.propagation == HF_PROP_ANGULAR_SPECTRUM || (d.propagation == HF_PROP_FRESNEL && !p->fast) ||
+                            p->filter2d;
     if (need_band2 && (rc = dev_alloc(&p->band2, (size_t)(B * p->nz * oplane), p->bytes)))
       break;
     if (d.propagation == HF_PROP_FRESNEL && (rc = dev_alloc(&p->lens, (size_t)plane, p->bytes)))
@@ -381,7 +399,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       break;
     // the tensor-core band pass holds 2 (z1 - z0) real columns per pixel: the one-sided band only
     p->rows_tc = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
-                 d.time_method == HF_TIME_RFFT &&
+                 d.time_method == HF_TIME_RFFT && !p->filter2d &&
                  band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
     if (d.propagation == HF_PROP_FRESNEL && p->fast && col_moments_tma_supported(d.height, d.width)) {
       const uint64_t rows = (uint64_t)B * p->nz * d.height;

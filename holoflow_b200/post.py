@@ -68,6 +68,40 @@ class Flatfield:
             pass
 
 
+class Filter2D:
+    """IFFT2(FFT2(x) x annulus) per [H][W] plane, unnormalized, of complex64 (in place allowed)
+    or float32 planes (filter2d.cu)."""
+
+    def __init__(self, shape: Sequence[int], real: bool, r_inner: int, r_outer: int, s_inner: int, s_outer: int,
+                 stream=None):
+        planes = 1
+        for n in shape[:-2]:
+            planes *= n
+        self.shape, self.real = tuple(shape), real
+        self._f = C.c_void_p()
+        check(lib().hf_filter2d_create(planes, shape[-2], shape[-1], int(real), r_inner, r_outer, s_inner, s_outer,
+                                       _stream(stream), C.byref(self._f)))
+
+    def __call__(self, x: torch.Tensor, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        assert x.is_cuda and tuple(x.shape) == self.shape and x.is_contiguous()
+        assert x.dtype == (torch.float32 if self.real else torch.complex64)
+        if out is None:
+            out = torch.empty_like(x)
+        check(lib().hf_filter2d_exec(self._f, _ptr(x), _ptr(out), _stream(stream)))
+        return out
+
+    def close(self) -> None:
+        if self._f:
+            lib().hf_filter2d_destroy(self._f)
+            self._f = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class PctClip:
     """Clips [D][H][W] to the values at the min_pct / max_pct ranks of the pixels inside `roi`
     (cx, cy, rx, ry normalized to the image, angle in degrees)."""

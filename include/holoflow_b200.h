@@ -312,7 +312,7 @@ int hf_multi_plan(hf_multi *multi, int i, hf_plan **plan);
 /* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
  * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------
  * Kinds: "FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
- * "Conversion", "FFTShiftNp", "Flatfield", "PctClip", "Holofile" (the reference's, with its JSON
+ * "Conversion", "FFTShiftNp", "Flatfield", "Filter2D", "PctClip", "Holofile" (the reference's, with its JSON
  * settings keys) and "DopplerMoments" (the fused per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
  * HF_U16, HF_F32, HF_CF32), strides in BYTES (all zero = C-contiguous), mem_loc 1 = device.
  * infer() failures return HF_ERR_INVALID with "<Factory> inference error: ..." in hf_last_error();
@@ -367,6 +367,17 @@ int hf_flatfield_create(int64_t planes, int height, int width, float sigma_y, fl
 int hf_flatfield_is_fourier(const hf_flatfield *ff, int *fourier);
 int hf_flatfield_exec(hf_flatfield *ff, const float *in, float *out, hf_stream_t s);
 int hf_flatfield_destroy(hf_flatfield *ff);
+
+/* Filter2D (holotask/src/syncs/filter2d.cu): out = IFFT2(FFT2(in) x mask) per [height][width]
+ * plane, unnormalized, mask = the band-pass annulus a (1 - b) of radii r_inner / r_outer with
+ * raised-cosine edges s_inner / s_outer.  real_input = 0: complex64 in and out (in place allowed),
+ * the mask applied as (g, g) like the reference's complex path; real_input = 1: float32 in and
+ * out, the mask (g, 0).  Image sides in {64..1536}, height <= 1024. */
+typedef struct hf_filter2d hf_filter2d;
+int hf_filter2d_create(int64_t planes, int height, int width, int real_input, uint32_t r_inner, uint32_t r_outer,
+                       uint32_t s_inner, uint32_t s_outer, hf_stream_t s, hf_filter2d **f);
+int hf_filter2d_exec(hf_filter2d *f, const void *in, void *out, hf_stream_t s);
+int hf_filter2d_destroy(hf_filter2d *f);
 
 /* PctClip (holotask/src/syncs/pct_clip.cu): clips [depth][height][width] to the values at
  * ranks int(pct / 100 * (count - 1)) of the pixels inside the ellipse (normalized centre, radii

@@ -77,6 +77,10 @@ struct HolofileSettings {
 struct FFTShiftSettings {
   std::vector<int> axes; // empty: every axis
 };
+struct Filter2DSettings { // filter2d.cu:26-40
+  uint32_t r_inner = 0, r_outer = 0, s_inner = 0, s_outer = 0;
+  bool     operator==(const Filter2DSettings &) const = default;
+};
 struct FlatfieldSettings {
   float sigma_y = 0.f, sigma_x = 0.f; // Gaussian sigmas in pixels
 };
@@ -93,6 +97,7 @@ struct PctClipSettings {
 void from_json(const nlohmann::json &j, FresnelDiffractionSettings &s);
 void from_json(const nlohmann::json &j, FFTShiftSettings &s);
 void from_json(const nlohmann::json &j, FlatfieldSettings &s);
+void from_json(const nlohmann::json &j, Filter2DSettings &s);
 void from_json(const nlohmann::json &j, PctClipSettings &s);
 void from_json(const nlohmann::json &j, HolofileSettings::LoadKind &s);
 void from_json(const nlohmann::json &j, HolofileSettings &s);
@@ -134,13 +139,14 @@ HFB_SYNC_FACTORY(ConversionFactory);
 HFB_SYNC_FACTORY(DopplerMomentsFactory);
 HFB_SYNC_FACTORY(FFTShiftFactory);  // kind "FFTShiftNp"
 HFB_SYNC_FACTORY(FlatfieldFactory);
+HFB_SYNC_FACTORY(Filter2DFactory);
 HFB_SYNC_FACTORY(PctClipFactory);
 HFB_SYNC_FACTORY(HolofileFactory); // frames [batch, H, W] (12-bit: packed rows [batch, H, 3W/2] U8)
 #undef HFB_SYNC_FACTORY
 
 // Registers every node above under its kind string: "FresnelDiffraction", "AngularSpectrum",
-// "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion", "FFTShiftNp", "Flatfield", "PctClip",
-// "Holofile" (the reference's) and "DopplerMoments".
+// "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion", "FFTShiftNp", "Flatfield", "Filter2D",
+// "PctClip", "Holofile" (the reference's) and "DopplerMoments".
 void register_path_kinds(core::Registry &registry);
 
 // The process-wide registry the C ABI's hf_node_* functions use.

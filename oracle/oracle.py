@@ -502,6 +502,8 @@ class PathConfig:
     as_padding: Optional[dict] = None
     phase_mode: str = "f32"
     time_method: str = "rfft"      # "rfft" (one-sided band) | "fft" (two-sided, 2 Nz planes)
+    filter2d: Optional[dict] = None  # r_inner/r_outer/s_inner/s_outer: Filter2D on the band planes
+                                     # before Fresnel (graph_builder.cc:124-126)
 
     @property
     def nz(self) -> int:
@@ -531,7 +533,11 @@ def propagate(planes: np.ndarray, cfg: PathConfig) -> np.ndarray:
 
 def reconstruct_window(window: np.ndarray, cfg: PathConfig) -> np.ndarray:
     """One T-frame window -> float64 [3, H', W'] (M0, M1, M2)."""
-    mag = propagate(band_planes(window, cfg), cfg)
+    planes = band_planes(window, cfg)
+    if cfg.filter2d and cfg.propagation != "angular_spectrum":
+        f = cfg.filter2d
+        planes = filter2d(planes, f["r_inner"], f["r_outer"], f["s_inner"], f["s_outer"])
+    mag = propagate(planes, cfg)
     w = freq_weights(cfg.frames, cfg.z0, cfg.z1, cfg.fs, cfg.time_method)
     return moments_from_magnitude(mag, w, cfg.fftshift)
 
@@ -663,3 +669,43 @@ def slide_avg(images: Sequence[np.ndarray], window: int, discard_first: int = 0)
         if k >= window:
             outs.append(avg.copy())
     return outs
+
+
+def filter2d_mask(height: int, width: int, r_inner: int, r_outer: int, s_inner: int, s_outer: int,
+                  real: bool) -> np.ndarray:
+    """The Filter2D annulus a (1 - b) in natural frequency order (filter2d.cu:109-199), float32.
+    Complex input: the centred mask, corners swapped (fftshift for even sides).  Real input: the
+    R2C half spectrum [H][W/2+1], with the `smooth > 0` guards."""
+    f = np.float32
+
+    def annulus(dist, guards):
+        ri, ro, si, so = f(r_inner), f(r_outer), f(s_inner), f(s_outer)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            a = np.where(dist < ro, f(1), np.where((so > 0 if guards else True) & (dist < ro + so),
+                                                   np.cos((dist - ro) / so * f(np.pi) / f(2)), f(0)))
+            b = np.where(dist < ri, f(1), np.where((si > 0 if guards else True) & (dist < ri + si),
+                                                   np.cos((dist - ri) / si * f(np.pi) / f(2)), f(0)))
+        return (a * (f(1) - b)).astype(f)
+
+    if real:
+        x = np.arange(width // 2 + 1, dtype=f)
+        y = np.arange(height)
+        fy = np.where(y <= height // 2, y, y - height).astype(f)
+        return annulus(np.hypot(x[None, :], fy[:, None]), True)
+    x = np.arange(width, dtype=f) - f(width) / f(2)
+    y = np.arange(height, dtype=f) - f(height) / f(2)
+    centred = annulus(np.hypot(x[None, :], y[:, None]), False)
+    return np.fft.ifftshift(centred)
+
+
+def filter2d(x: np.ndarray, r_inner: int, r_outer: int, s_inner: int, s_outer: int) -> np.ndarray:
+    """Filter2D (filter2d.cu:229-244): complex planes -> FFT2 x (g + i g) -> IFFT2, real planes ->
+    RFFT2 x g -> IRFFT2; both unnormalized (cuFFT), per [H][W] plane."""
+    H, W = x.shape[-2:]
+    if np.iscomplexobj(x):
+        g = filter2d_mask(H, W, r_inner, r_outer, s_inner, s_outer, False).astype(np.float64)
+        spec = np.fft.fft2(np.asarray(x, dtype=np.complex128), axes=(-2, -1)) * (g + 1j * g)
+        return np.fft.ifft2(spec, axes=(-2, -1)) * (H * W)
+    g = filter2d_mask(H, W, r_inner, r_outer, s_inner, s_outer, True).astype(np.float64)
+    spec = np.fft.rfft2(np.asarray(x, dtype=np.float64), axes=(-2, -1)) * g
+    return np.fft.irfft2(spec, s=(H, W), axes=(-2, -1)) * (H * W)

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from oracle import synth as S
 
 pytestmark = pytest.mark.gpu
 
@@ -130,3 +131,45 @@ def test_display_chain_nodes_end_to_end(cuda):
     (u8,) = N.run_sync_factory("Conversion", {"target": "U8", "strategy": "Scaled"}, [c])
     u = u8.cpu().numpy()
     assert u.dtype == np.uint8 and u.min() == 0 and u.max() == 255
+
+
+@pytest.mark.parametrize("real,shape,radii", [(False, (3, 256, 256), (4, 60, 6, 10)), (True, (2, 512, 512), (0, 100, 0, 20)),
+                                              (False, (1, 1024, 1024), (10, 300, 20, 40)), (True, (1, 128, 256), (3, 40, 5, 0))])
+def test_filter2d_complex_and_real(cuda, real, shape, radii):
+    """Filter2D against the oracle: the annulus in natural frequency order, (g, g) on complex
+    planes as the reference's complex path, (g, 0) on the real half spectrum; unnormalized."""
+    import torch
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(shape).astype(np.float32)
+    if not real:
+        x = (x + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    f = _post().Filter2D(shape, real, *radii)
+    got = f(torch.from_numpy(x).to(cuda)).cpu().numpy()
+    exp = O.filter2d(x, *radii)
+    assert O.rel_l2(got, exp) < 1e-5
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_pipeline_filter2d_before_fresnel(cuda, form):
+    """With the filter on and Fresnel propagation, the band planes go through Filter2D before
+    the lens (graph_builder.cc:124-126), in both forms, against the oracle."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    H = W = 256
+    nwin, n = 2, 80
+    z0, z1 = O.band_bins(4e3, 33e3, 67e3, 64)
+    frames = S.Interferograms(S.config1(n, height=H, width=W)).frames(0, n)
+    ring = torch.from_numpy(O.pack12(frames.reshape(-1))).to(cuda)
+    flt = dict(r_inner=4, r_outer=90, s_inner=6, s_outer=20)
+    cfg = pl.PipelineConfig(height=H, width=W, frames=64, hop=16, z_begin=z0, z_end=z1, fs=67e3, z=0.25,
+                            clutter_rank=4, form=form, max_batch=nwin, as_filter=1, **flt)
+    p = pl.Pipeline(cfg)
+    got = p.run(ring, n, 0, nwin).cpu().numpy()
+    assert p.status() == 0
+    ocfg = O.PathConfig(H, W, 64, 16, z0, z1, fs=67e3, z=0.25, clutter_rank=4, filter2d=flt)
+    tol = 1e-4 if form == 0 else 1e-3
+    for w in range(nwin):
+        exp = O.reconstruct_window(frames[16 * w:16 * w + 64], ocfg)
+        for m in range(3):
+            assert O.rel_l2(got[w, m], exp[m]) < tol, (w, m)

@@ -39,7 +39,8 @@ def invalid(kind, settings, descs, fragment):
 
 def test_reference_kinds_are_registered():
     assert set(N.kinds()) == {"FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
-                              "Conversion", "Holofile", "FFTShiftNp", "Flatfield", "PctClip", "DopplerMoments"}
+                              "Conversion", "Holofile", "FFTShiftNp", "Flatfield", "Filter2D", "PctClip",
+                              "DopplerMoments"}
 
 
 def test_unknown_kind_and_bad_settings():
@@ -165,3 +166,13 @@ def test_doppler_moments_two_sided_time_method():
             p + "time_method must be rfft or fft")
     invalid("DopplerMoments", {**s, "time_z_begin": 0, "time_z_end": 33}, [desc([1, 64, 64, 64], U16)],
             p + "at most 64 band planes")
+
+
+def test_filter2d_infer():
+    f = {"r_inner": 2, "r_outer": 40, "s_inner": 3, "s_outer": 5}
+    assert out_of("Filter2D", f, [desc([2, 64, 64], CF32)]) == ((2, 64, 64), CF32)
+    assert out_of("Filter2D", f, [desc([64, 64], F32)]) == ((64, 64), F32)
+    p = "Filter2DFactory inference error: "
+    invalid("Filter2D", f, [desc([64, 64], U16)], p + "input must be complex float32 or real float32")
+    invalid("Filter2D", f, [desc([64])], p + "input must be a tensor of rank 2 or higher")
+    invalid("Filter2D", f, [desc([64, 64], CF32, device=False)], p + "input must be in device memory")
