@@ -381,6 +381,9 @@ __global__ void __launch_bounds__(128) cov_tc_i8_kernel(FrameRing ring, int64_t 
 // Operand row r of a window holds frame 8 (r / 16) + r % 8, kind h when (r / 8) is even; the h-row
 // and l-row of a frame sit 8 lanes apart in one warp and are folded with a shuffle before the
 // integer atomics.
+// Warp roles: the producer warps fill the stages and arrive (one arrival per warp) on the stage's
+// `full` barrier; the last warp waits on it, issues the stage's MMAs and commits them to the
+// stage's `free` barrier, so no producer waits for the others between tiles.
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc::smem_u32(dst)), "l"(src) : "memory");
@@ -403,11 +406,29 @@ template <int FMT, int HOP8> struct GroupCov {
   static constexpr int D    = F <= 112 ? 4 : 3;            // raw ring depth (tiles)
   static constexpr int S    = F <= 136 ? 3 : 2;            // operand stages
   static constexpr int STG  = 256 * F;                     // 2F rows x 128 B
-  static constexpr size_t smem = 1024 + (size_t)S * STG + (size_t)D * NT * RB + S * 8 + 16;
+  static constexpr int NTHR = NT + 32;                     // producers + the MMA warp
+  static constexpr size_t smem = 1024 + (size_t)S * STG + (size_t)D * NT * RB + 2 * S * 8 + 16;
 };
 
+// Bounded mbarrier wait that also gives up once another thread has raised `abort`; the first
+// thread to time out records `code` in the status word and raises it.
+__device__ __forceinline__ bool wait_or_abort(uint64_t *mbar, uint32_t parity, volatile int *abort, int *status,
+                                              int code) {
+  const uint64_t t0 = tc::globaltimer_ns();
+  for (uint32_t i = 0; i < tc::kWaitLimit; ++i) {
+    if (tc::mbar_try_wait(mbar, parity))
+      return true;
+    if ((i & 255u) == 255u && (*abort || tc::globaltimer_ns() - t0 > tc::kWaitNs))
+      break;
+  }
+  if (!*abort && status)
+    atomicCAS(status, 0, code);
+  *abort = 1;
+  return false;
+}
+
 template <int FMT, int HOP8>
-__global__ void __launch_bounds__(GroupCov<FMT, HOP8>::NT, 1)
+__global__ void __launch_bounds__(GroupCov<FMT, HOP8>::NTHR, 1)
     cov_tc_group_kernel(FrameRing ring, int64_t P, int nwin, uint32_t ncols, unsigned long long *acc,
                         unsigned long long *sums, int *status) {
   using G                = GroupCov<FMT, HOP8>;
@@ -417,15 +438,22 @@ __global__ void __launch_bounds__(GroupCov<FMT, HOP8>::NT, 1)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t  *raw   = smem + G::S * G::STG;
-  uint64_t *mbar  = reinterpret_cast<uint64_t *>(raw + (size_t)G::D * G::NT * G::RB);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + G::S);
+  uint64_t *mbar  = reinterpret_cast<uint64_t *>(raw + (size_t)G::D * G::NT * G::RB); // [S] free
+  uint64_t *fullb = mbar + G::S;                                                        // [S] full
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(fullb + G::S);
+  int      *abort_flag = reinterpret_cast<int *>(tslot + 1);
+  volatile int *abortv = abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int w0  = 4 * blockIdx.y;
   const int g   = min(4, nwin - w0);   // windows of this group
   const int Fg  = T + (g - 1) * HOP;   // frames of this group
+  const bool producer = tid < G::NT;   // the last warp issues the MMAs
   if (tid == 0) {
-    for (int s = 0; s < G::S; ++s)
-      tc::mbar_init(&mbar[s], 1);
+    for (int s = 0; s < G::S; ++s) {
+      tc::mbar_init(&mbar[s], 1);              // the MMA commit of the stage's tile
+      tc::mbar_init(&fullb[s], G::NT / 32);    // one arrival per producer warp
+    }
+    *abort_flag = 0;
     tc::mbar_fence_init();
   }
   if (warp == 0)
@@ -455,19 +483,19 @@ __global__ void __launch_bounds__(GroupCov<FMT, HOP8>::NT, 1)
     }
     cp_async_commit();
   };
-#pragma unroll
-  for (int d = 0; d < G::D - 1; ++d)
-    issue(blockIdx.x + (int64_t)d * gridDim.x, d);
-
   uint32_t sx = 0u, sl = 0u; // sums of the high and low 6-bit fields
   int      nj = 0;
   bool     ok = true;
+  if (producer) {
+#pragma unroll
+  for (int d = 0; d < G::D - 1; ++d)
+    issue(blockIdx.x + (int64_t)d * gridDim.x, d);
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++nj) {
     const int s = nj % G::S;
     issue(tile + (int64_t)(G::D - 1) * gridDim.x, (nj + G::D - 1) % G::D);
     bool w_ok = true;
-    if (nj >= G::S)
-      w_ok = tc::mbar_wait_bounded(&mbar[s], (uint32_t)((nj / G::S) - 1) & 1u, status, 5);
+    if (nj >= G::S) // the MMAs that read this stage S tiles ago are done
+      w_ok = wait_or_abort(&mbar[s], (uint32_t)((nj / G::S) - 1) & 1u, abortv, status, 5);
     cp_async_wait<G::D - 1>();
     const bool valid = active && tile * kTcPX + grp * 32 < P;
     if (w_ok && active) {
@@ -522,36 +550,51 @@ __global__ void __launch_bounds__(GroupCov<FMT, HOP8>::NT, 1)
             make_uint4(lw[4 * hc], lw[4 * hc + 1], lw[4 * hc + 2], lw[4 * hc + 3]);
       }
     }
-    tc::fence_proxy_async_smem();
-    ok = __syncthreads_and(w_ok) != 0;
-    if (!ok)
+    tc::fence_proxy_async_smem(); // this thread's stage writes before the async proxy reads them
+    __syncwarp();
+    if (lane == 0)
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&fullb[s])) : "memory");
+    if (!w_ok || *abortv) {
+      ok = false;
       break;
-    if (tid == 0) {
-      tc::fence_after_sync();
-      const uint8_t *st = smem + s * G::STG;
-      for (int wl = 0; wl < g; ++wl) {
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-          const uint64_t d = tc::sw128_desc(tc::smem_u32(st + wl * HOP8 * 2048 + ks * 32), 16, 1024);
-          tc::mma_i8(tbase + 128 * wl, d, d, idesc, (nj > 0 || ks > 0) ? 1u : 0u);
-        }
-      }
-      tc::mma_commit(&mbar[s]);
     }
   }
   cp_async_wait<0>(); // no copy may land in shared memory after the CTA has left
-  if (nj > 0 && ok) {
-    const int last = nj - 1;
-    ok = tc::mbar_wait_bounded(&mbar[last % G::S], (uint32_t)(last / G::S) & 1u, status, 6);
+  } else {
+    // MMA warp: issue each stage's MMAs as soon as every producer warp has filled it
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++nj) {
+      const int s = nj % G::S;
+      if (!wait_or_abort(&fullb[s], (uint32_t)(nj / G::S) & 1u, abortv, status, 7)) {
+        ok = false;
+        break;
+      }
+      if (lane == 0) {
+        tc::fence_after_sync();
+        const uint8_t *st = smem + s * G::STG;
+        for (int wl = 0; wl < g; ++wl) {
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint64_t d = tc::sw128_desc(tc::smem_u32(st + wl * HOP8 * 2048 + ks * 32), 16, 1024);
+            tc::mma_i8(tbase + 128 * wl, d, d, idesc, (nj > 0 || ks > 0) ? 1u : 0u);
+          }
+        }
+        tc::mma_commit(&mbar[s]);
+      }
+      __syncwarp();
+    }
+    if (nj > 0 && ok) { // drain: the last commit covers every MMA issued before it
+      const int last = nj - 1;
+      ok = wait_or_abort(&mbar[last % G::S], (uint32_t)(last / G::S) & 1u, abortv, status, 6);
+    }
   }
-  ok = __syncthreads_and(ok) != 0;
+  ok = __syncthreads_and(ok && !*abortv) != 0;
   tc::fence_after_sync();
 
   // frame sums: the four runs of a frame are adjacent lanes; each window holding frame f gets it
   unsigned long long fs = 64ull * sx + sl;
   fs += __shfl_xor_sync(0xFFFFFFFFu, fs, 1);
   fs += __shfl_xor_sync(0xFFFFFFFFu, fs, 2);
-  if (active && grp == 0)
+  if (producer && active && grp == 0)
     for (int wl = 0; wl < g; ++wl) {
       const int t = f - wl * HOP;
       if (t >= 0 && t < T)
@@ -676,8 +719,8 @@ int launch_tc_group(const FrameRing &ring, int64_t P, int nwin, void *ws, double
   HF_CUDA(cudaMemsetAsync(acc, 0, ((size_t)nwin * T * T + (size_t)nwin * T) * sizeof(unsigned long long), s));
   HF_CUDA(cudaFuncSetAttribute(cov_tc_group_kernel<FMT, HOP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)G::smem));
-  cov_tc_group_kernel<FMT, HOP8><<<dim3(ctas, ngroups), G::NT, G::smem, s>>>(ring, P, nwin, ncols, acc, sums,
-                                                                              status);
+  cov_tc_group_kernel<FMT, HOP8><<<dim3(ctas, ngroups), G::NTHR, G::smem, s>>>(ring, P, nwin, ncols, acc, sums,
+                                                                                status);
   note_launch();
   HF_TRY(launch_status("cov_tc_group_kernel"));
   return launch_i8_finalize(acc, sums, T, P, FMT == HF_U8 ? 128 : 2048, nwin, gram, s);
