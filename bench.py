@@ -267,7 +267,7 @@ def run_batched(args, local):
     }), flush=True)
 
 
-def run_serve(args, local, form, seed=1004):
+def run_serve(args, local, form, seed=1004, life=120):
     """Config 4: camera streams arrive by a Poisson process (mean 1.5 per round until 12 have come,
     4 open at the start), each with its own frame size (512^2 .. 1536 x 1024), 12-bit packed input,
     (T, hop) of (64, 16) or (128, 32), z and fs; a stream leaves after 120 windows.  Each round every
@@ -304,7 +304,7 @@ def run_serve(args, local, form, seed=1004):
         return {"cfg": cfg, "pool": pool(H, W), "pos": 0, "done": 0, "out": torch.empty(
             (4, 3, H, W), dtype=torch.float32, pin_memory=True)}
 
-    LIFE = 120  # windows per stream
+    LIFE = life  # windows per stream
     srv = Server(max_streams=24, hbm_reserve_bytes=8 << 30)
     waiting = [new_stream(k) for k in range(12)]
     open_, sids, frames_done, windows_done, refused = {}, {}, 0, 0, 0
@@ -381,6 +381,10 @@ def main():
     if args.workload == "serve":
         if rank != 0:
             return None
+        # untimed warm-up of both forms on the same seeded streams: loads every kernel module and
+        # builds every table once, so neither timed run pays the process's first-use costs
+        for f in (1, 0):
+            run_serve(args, local, f, life=8)
         res = {f: run_serve(args, local, 1 if f == "chosen" else 0) for f in ("chosen", "plain")}
         print(json.dumps({
             "metric": "streaming server: sustained frames/s and p50/p99 frame-to-image latency, chosen vs plain",
