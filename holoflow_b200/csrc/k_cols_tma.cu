@@ -187,7 +187,7 @@ template <int N1> int launch_n1(const CUtensorMap &tmap, const ColMomArgs &a, co
 } // namespace
 
 bool col_moments_tma_supported(int H, int W) {
-  return (H == 64 || H == 128 || H == 256 || H == 512 || H == 1024) && W >= 2 && W % 2 == 0;
+  return (H == 64 || H == 128 || H == 256 || H == 512 || H == 768 || H == 1024) && W >= 2 && W % 2 == 0;
 }
 
 int launch_col_moments_tma(const CUtensorMap &tmap, const ColMomArgs &a, const MomentSpec &m, int nwin,
@@ -199,6 +199,7 @@ int launch_col_moments_tma(const CUtensorMap &tmap, const ColMomArgs &a, const M
   case 4: return launch_n1<4>(tmap, a, m, nwin, s);
   case 8: return launch_n1<8>(tmap, a, m, nwin, s);
   case 16: return launch_n1<16>(tmap, a, m, nwin, s);
+  case 24: return launch_n1<24>(tmap, a, m, nwin, s);
   default: return launch_n1<32>(tmap, a, m, nwin, s);
   }
 }

@@ -111,7 +111,8 @@ template <int FMT, int N1>
 __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArgs a) {
   constexpr int W      = N1 * 32;
   constexpr int NTILE  = W / 128;
-  constexpr int NCOL   = NTILE * 64 < 32 ? 32 : NTILE * 64;
+  // TMEM is allocated in powers of two columns (>= 32): 6 tiles (W = 768) take 512
+  constexpr int NCOL   = NTILE * 64 <= 32 ? 32 : (NTILE * 64 <= 128 ? 128 : (NTILE * 64 <= 256 ? 256 : 512));
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t *sA   = smem;                                  // NTILE x 16 KB
@@ -396,7 +397,7 @@ template <int FMT, int N1> int launch_n1(const BandRowsArgs &a, cudaStream_t s) 
 } // namespace
 
 bool band_rows_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes) {
-  return (fmt == HF_MONO12P || fmt == HF_U16) && T == 64 && (W == 256 || W == 512 || W == 1024) && nz >= 1 &&
+  return (fmt == HF_MONO12P || fmt == HF_U16) && T == 64 && (W == 256 || W == 512 || W == 768 || W == 1024) && nz >= 1 &&
          nz <= 32 && frame_bytes % 16 == 0;
 }
 
@@ -406,6 +407,7 @@ int launch_band_rows_tc(const BandRowsArgs &a, int fmt, cudaStream_t s) {
   switch (a.W) {
   case 256: return fmt == HF_MONO12P ? launch_n1<HF_MONO12P, 8>(a, s) : launch_n1<HF_U16, 8>(a, s);
   case 512: return fmt == HF_MONO12P ? launch_n1<HF_MONO12P, 16>(a, s) : launch_n1<HF_U16, 16>(a, s);
+  case 768: return fmt == HF_MONO12P ? launch_n1<HF_MONO12P, 24>(a, s) : launch_n1<HF_U16, 24>(a, s);
   default: return fmt == HF_MONO12P ? launch_n1<HF_MONO12P, 32>(a, s) : launch_n1<HF_U16, 32>(a, s);
   }
 }

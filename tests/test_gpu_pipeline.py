@@ -166,7 +166,7 @@ def test_chosen_form_grouped_gram(cuda, hop, nwin, dtype, first, H):
         assert np.array_equal(gram.cpu().numpy(), X @ X.T), w
 
 
-@pytest.mark.parametrize("H,W,nwin", [(256, 256, 3), (512, 512, 2), (1024, 1024, 2)])
+@pytest.mark.parametrize("H,W,nwin", [(256, 256, 3), (512, 512, 2), (768, 768, 2), (1024, 1024, 2)])
 def test_chosen_form_fresnel_vs_oracle(cuda, H, W, nwin):
     """Chosen form (int8 tensor-core Gram, f16 tensor-core band DFT fused with lens + row FFT):
     M0/M1/M2 within the 1e-3 relative-L2 target of the float64 oracle, and the device status word
