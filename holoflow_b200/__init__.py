@@ -24,6 +24,8 @@ HF_NORM_BACKWARD, HF_NORM_FORWARD, HF_NORM_ORTHO = 0, 1, 2
 HF_PROP_NONE, HF_PROP_FRESNEL, HF_PROP_ANGULAR_SPECTRUM = 0, 1, 2
 HF_M0, HF_M1, HF_M2 = 1, 2, 4
 HF_FORM_PLAIN, HF_FORM_CHOSEN = 0, 1
+HF_STFD_LOCAL, HF_STFD_GLOBAL = 0, 1
+HF_STFD_COMPLEX, HF_STFD_MAGNITUDE, HF_STFD_MEAN_MAGNITUDE = 0, 1, 2
 
 
 class HfError(RuntimeError):
@@ -166,6 +168,35 @@ _PROTOS = {
     "hf_holo_finish": (C.c_int, [_vp]),
     "hf_plan_stage_times": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
+    "hf_stfd_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                 C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                                 C.POINTER(_vp)]),
+    "hf_stfd_grid": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hf_stfd_set_z": (C.c_int, [_vp, C.c_float, _vp]),
+    "hf_stfd_exec": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "hf_stfd_destroy": (C.c_int, [_vp]),
+    "hf_shslopes_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                     C.POINTER(HfEllipse), C.c_int, _vp, C.POINTER(_vp)]),
+    "hf_shslopes_active": (C.c_int, [_vp, _vp]),
+    "hf_shslopes_exec": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "hf_shslopes_destroy": (C.c_int, [_vp]),
+    "hf_zernike_fit_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                        C.c_float, C.c_int, C.POINTER(C.c_int), C.c_int, C.POINTER(_vp)]),
+    "hf_zernike_fit_pupil_radius": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "hf_zernike_fit_exec": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "hf_zernike_fit_host": (C.c_int, [_vp, _vp, _vp]),
+    "hf_zernike_fit_destroy": (C.c_int, [_vp]),
+    "hf_zernike_phase": (C.c_int, [_vp, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "hf_correct_phase": (C.c_int, [_vp, C.c_int, _vp, _i64, C.c_int, C.c_int, _vp, _vp]),
+    "hf_wrap2pi": (C.c_int, [_vp, _vp, _i64, _vp]),
+    "hf_defocus_z": (C.c_int, [C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_double),
+                               C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "hf_autofocus_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                      C.c_float, C.c_int, C.POINTER(C.c_int), C.c_int, _vp, C.POINTER(_vp)]),
+    "hf_autofocus_pupil_radius": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "hf_autofocus_exec": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "hf_autofocus_outputs": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "hf_autofocus_destroy": (C.c_int, [_vp]),
 }
 
 _lib = None

@@ -440,6 +440,91 @@ int hf_holo_write(hf_holo_writer *writer, const void *src, int64_t count);
 /* Appends the footer and closes the file. */
 int hf_holo_finish(hf_holo_writer *writer);
 
+/* ---- Shack-Hartmann autofocus (graph_builder.cc:307-501) --------------------------------------
+ * Sub-aperture and correlation transforms take any side 2..1024 (HF_ERR_UNSUPPORTED beyond).
+ * Validation failures return HF_ERR_INVALID with the reference factory's message.
+ *
+ * ShortTimeFresnelDiffraction (holotask/include/holotask/syncs/short_time_fresnel_diffraction.hh:
+ * 40-56): `planes` fields [planes][H][W] (complex64, or float32 when real_input), windows of
+ * win_h x win_w every stride_y / stride_x pixels, each times the quadratic input lens (the whole
+ * field's frame for HF_STFD_GLOBAL, the window's for HF_STFD_LOCAL), unnormalised 2D forward FFT.
+ * Outputs: HF_STFD_COMPLEX [planes][ny][nx][win_h][win_w] complex64 (times the window lens unless
+ * skip_phase_shift); HF_STFD_MAGNITUDE the same shape in float32 (output_magnitude); and
+ * HF_STFD_MEAN_MAGNITUDE [ny][nx][win_h][win_w] float32, the mean of |.| over the planes (the
+ * reference's following Mean over the band axis), each window fftshifted when fftshift_windows.
+ * hf_stfd_set_z replaces the distance (the factory's z-only update). */
+#define HF_STFD_LOCAL 0
+#define HF_STFD_GLOBAL 1
+#define HF_STFD_COMPLEX 0
+#define HF_STFD_MAGNITUDE 1
+#define HF_STFD_MEAN_MAGNITUDE 2
+typedef struct hf_stfd hf_stfd;
+int hf_stfd_create(int64_t planes, int height, int width, int real_input, int win_h, int win_w, int stride_y,
+                   int stride_x, float lambda, float dx, float dy, float z, int phase_ref, int output,
+                   int skip_phase_shift, int fftshift_windows, hf_stream_t s, hf_stfd **f);
+int hf_stfd_grid(const hf_stfd *f, int *ny, int *nx);
+int hf_stfd_set_z(hf_stfd *f, float z, hf_stream_t s);
+int hf_stfd_exec(hf_stfd *f, const void *in, void *out, hf_stream_t s);
+int hf_stfd_destroy(hf_stfd *f);
+
+/* ShackHartmannSlopes, single-reference mode (holotask/include/holotask/syncs/
+ * shack_hartmann_slopes.hh:28-61): images [sy][sx][h][w] float32 (sy, sx odd) -> slopes
+ * [sy][sx][2] float32: each image phase-correlated with the centre one inside the ROI ellipse
+ * (mean removed, cosine taper), peak offset with parabolic refinement, times lambda / (n d),
+ * centre offset and the mean over the active sub-apertures removed (inactive ones 0).  `maps`
+ * (optional, [sy][sx][h][w]) receives the correlation maps.  hf_shslopes_active writes the
+ * active flags (1 byte per sub-aperture). */
+typedef struct hf_shslopes hf_shslopes;
+int hf_shslopes_create(int sy, int sx, int height, int width, float lambda, float dx, float dy, float z,
+                       const hf_ellipse *roi, int skip_outside_pupil, hf_stream_t s, hf_shslopes **p);
+int hf_shslopes_active(const hf_shslopes *p, uint8_t *active);
+int hf_shslopes_exec(hf_shslopes *p, const float *images, float *slopes, float *maps, hf_stream_t s);
+int hf_shslopes_destroy(hf_shslopes *p);
+
+/* ZernikeFromSlopes (holotask/include/holotask/syncs/zernike_from_slopes.hh:27-45): Noll indexes
+ * 2..10 (unique, at most 9); tip and tilt stay 0; the other coefficients (radians) are the
+ * least-squares fit of the zero-mean slopes.  hf_zernike_fit_exec runs on the device (device
+ * slopes [sy*sx*2] -> device coefficients; `cumulative`, optional, accumulates them) with the
+ * reference's float32 sequence; hf_zernike_fit_host runs the same on host arrays. */
+typedef struct hf_zernike_fit hf_zernike_fit;
+int hf_zernike_fit_create(int sy, int sx, int sub_h, int sub_w, int stride_y, int stride_x, float lambda, float dx,
+                          float dy, int skip_outside_pupil, const int *indexes, int n_indexes, hf_zernike_fit **f);
+int hf_zernike_fit_pupil_radius(const hf_zernike_fit *f, float *radius);
+int hf_zernike_fit_exec(hf_zernike_fit *f, const float *slopes, float *coeffs, float *cumulative, hf_stream_t s);
+int hf_zernike_fit_host(const hf_zernike_fit *f, const float *slopes, float *coeffs);
+int hf_zernike_fit_destroy(hf_zernike_fit *f);
+
+/* ZernikePhase (zernike_phase.hh): device coefficients -> device phase [ny][nx] (optional
+ * `cumulative` += phase).  CorrectPhase (correct_phase.cu): out = in exp(-i phase), the [H][W]
+ * phase broadcast over `planes`, complex64 or float32 input, complex64 output (in place allowed
+ * for complex input).  Wrap2Pi (wrap2pi.cu): fmod by 2 pi into [0, 2 pi).  hf_defocus_z is
+ * ZernikeDefocusZProp's estimate (zernike_defocus_z_prop.cc:84-97) from the defocus coefficient. */
+int hf_zernike_phase(const float *coeffs, const int *indexes, int n_indexes, int ny, int nx, float *phase,
+                     float *cumulative, hf_stream_t s);
+int hf_correct_phase(const void *in, int complex_input, const float *phase, int64_t planes, int height, int width,
+                     void *out, hf_stream_t s);
+int hf_wrap2pi(const float *in, float *out, int64_t n, hf_stream_t s);
+int hf_defocus_z(float a4, float lambda, float z_curr, float pupil_radius, double *delta_inv_z, double *z_new,
+                 double *delta_z_mm);
+
+/* One autofocus pass chain on one spectrum (build_shack_hartmann, graph_builder.cc:307-501, with
+ * pp_accumulation 1 and no flatfield): sub-apertures of W / nb x H / nb (nb odd), short-time
+ * Fresnel with the global phase, mean |.| over the nz planes, fftshift, single-reference slopes
+ * in the ROI circle of radius roi_radius, device Zernike fit, phase map over H x W, and
+ * corrected = delayed exp(-i phase) (delayed NULL: the planes themselves).  n_iter passes chain
+ * as the reference's (each later pass measures and corrects the previous output);
+ * hf_autofocus_outputs copies (on stream s, into device buffers; NULL skips one) the last exec's
+ * M0 [nb][nb][sh][sw], slopes [nb][nb][2], and the coefficients [n_indexes] and phase [H][W]
+ * summed over the passes.  With n_indexes 0 the planes pass through. */
+typedef struct hf_autofocus hf_autofocus;
+int hf_autofocus_create(int nz, int height, int width, int nb_subaps, int n_iter, float lambda, float dx, float z,
+                        float roi_radius, int skip_outside_pupil, const int *indexes, int n_indexes, hf_stream_t s,
+                        hf_autofocus **a);
+int hf_autofocus_pupil_radius(const hf_autofocus *a, float *radius);
+int hf_autofocus_exec(hf_autofocus *a, const void *planes, const void *delayed, void *corrected, hf_stream_t s);
+int hf_autofocus_outputs(const hf_autofocus *a, float *m0, float *slopes, float *coeffs, float *phase, hf_stream_t s);
+int hf_autofocus_destroy(hf_autofocus *a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,11 +66,13 @@ def stfd_input_lens(field_h, field_w, win_h, win_w, lam, z, dx, dy, phase_ref="g
 
 def stfd_window_lens(win_h: int, win_w: int, lam: float, z: float, dx: float) -> np.ndarray:
     """stft_win_lens_kernel (short_time_fresnel_diffraction.cu:405-420): output-plane quadratic
-    phase of one window, pixel pitch dx on both axes."""
+    phase of one window, pixel pitch dx on both axes, the phase argument in float32."""
     size = max(win_w, win_h)
-    x = ((np.arange(win_w) + (size - win_w) // 2) - size / 2.0) * dx
-    y = ((np.arange(win_h) + (size - win_h) // 2) - size / 2.0) * dx
-    return np.exp(1j * math.pi / (lam * z) * (x[None, :] ** 2 + y[:, None] ** 2))
+    x = (np.arange(win_w) + (size - win_w) // 2 - size / 2.0).astype(F32) * F32(dx)
+    y = (np.arange(win_h) + (size - win_h) // 2 - size / 2.0).astype(F32) * F32(dx)
+    k = PI_F32 / (F32(lam) * F32(z))
+    ph = (k * ((x * x)[None, :] + (y * y)[:, None])).astype(F32)
+    return np.exp(1j * ph.astype(np.float64))
 
 
 def stfd_grid(H: int, W: int, win_h: int, win_w: int, stride_y: int, stride_x: int):

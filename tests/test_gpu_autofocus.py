@@ -1,0 +1,253 @@
+"""Shack-Hartmann autofocus on the GPU against the oracle (oracle/shack.py), which restates
+short_time_fresnel_diffraction.cu, cross_correlation2.cu, shack_hartmann_slopes.cu,
+zernike_from_slopes.cc, zernike_phase.cu, correct_phase.cu and wrap2pi.cu.
+
+Tolerances: the short-time Fresnel transforms are float32 FFTs of lengths up to 1024 against
+float64 (relative L2 1e-5); correlation maps 2e-5 absolute on textured images (the cross power
+is unit-magnitude in every bin, so bins at rounding level would carry noise phases); peak offsets
+2e-3 pixel; the device Zernike fit equals the host fit bit for bit and the float64
+fit to 2e-5 (the reference's bound); the autofocus chain's coefficients to 1e-3 relative."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import shack as SH
+
+pytestmark = pytest.mark.gpu
+
+LAM, DX, Z = 852e-9, 20e-6, 0.25
+
+
+def _af():
+    from holoflow_b200 import autofocus
+    return autofocus
+
+
+def cfield(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+@pytest.mark.parametrize("shape,win,stride,ref,output", [
+    ((2, 510, 510), (102, 102), (102, 102), "global", "magnitude"),   # nb = 5: 2 x 3 x 17
+    ((1, 512, 512), (170, 170), (170, 170), "global", "complex"),     # nb = 3: 2 x 5 x 17
+    ((3, 219, 219), (73, 73), (73, 73), "local", "complex"),          # prime side
+    ((1, 256, 320), (64, 80), (32, 40), "local", "magnitude"),        # overlapping, non-square
+    ((2, 1024, 1024), (204, 204), (204, 204), "global", "magnitude"),  # 4 x 3 x 17
+    ((1, 96, 1024), (96, 1024), (96, 1024), "global", "complex"),     # one window, longest rows
+])
+def test_stfd_matches_oracle(cuda, shape, win, stride, ref, output):
+    import torch
+    rng = np.random.default_rng(1)
+    x = cfield(rng, shape)
+    op = _af().ShortTimeFresnel(shape, win, stride, LAM, DX, DX, Z, phase_ref=ref, output=output)
+    got = op(torch.from_numpy(x).to(cuda)).cpu().numpy()
+    exp = SH.stfd(x, win[0], win[1], stride[0], stride[1], LAM, DX, DX, Z, ref, output == "magnitude")
+    assert got.shape == exp.shape
+    assert O.rel_l2(got, exp) < 1e-5
+
+
+def test_stfd_real_input_window_lens_and_set_z(cuda):
+    import torch
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((2, 120, 150)).astype(np.float32)
+    op = _af().ShortTimeFresnel(x.shape, (40, 50), (40, 50), LAM, DX, DX, Z, phase_ref="local", output="complex",
+                                skip_phase_shift=False, real_input=True)
+    exp = SH.stfd(x, 40, 50, 40, 50, LAM, DX, DX, Z, "local", False, skip_phase_shift=False)
+    assert O.rel_l2(op(torch.from_numpy(x).to(cuda)).cpu().numpy(), exp) < 1e-5
+    op.set_z(0.4)
+    exp = SH.stfd(x, 40, 50, 40, 50, LAM, DX, DX, 0.4, "local", False, skip_phase_shift=False)
+    assert O.rel_l2(op(torch.from_numpy(x).to(cuda)).cpu().numpy(), exp) < 1e-5
+
+
+@pytest.mark.parametrize("nb,side,nz", [(5, 510, 8), (3, 512, 4), (7, 511, 2)])
+def test_subaperture_mean_magnitude_with_shift(cuda, nb, side, nz):
+    """The fused Mean over the band and the per-sub-aperture fftshift (graph_builder.cc:345-347)."""
+    import torch
+    rng = np.random.default_rng(3)
+    x = cfield(rng, (nz, side, side))
+    s = side // nb
+    op = _af().ShortTimeFresnel(x.shape, (s, s), (s, s), LAM, DX, DX, Z, phase_ref="global",
+                                output="mean_magnitude", fftshift_windows=True)
+    got = op(torch.from_numpy(x).to(cuda)).cpu().numpy()
+    exp = SH.subaperture_m0(x, nb, LAM, DX, Z)
+    assert O.rel_l2(got, exp) < 1e-5
+
+
+def translated(sy, sx, h, w, shifts):
+    def pattern(x, y):
+        def g(cx, cy, s, a):
+            return a * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * s * s))
+        return g(0.43 * w, 0.48 * h, 3.4, 1.0) + g(0.62 * w, 0.36 * h, 2.1, 0.55) + g(0.31 * w, 0.66 * h, 1.7, 0.27)
+    y, x = np.mgrid[0:h, 0:w].astype(np.float64)
+    return np.stack([pattern(x - dx, y - dy) for dx, dy in shifts]).reshape(sy, sx, h, w).astype(np.float32)
+
+
+@pytest.mark.parametrize("case", ["integer", "subpixel"])
+def test_slopes_known_answers(cuda, case):
+    """The reference's slope tests (shack_hartmann_test.cu:563-654) on the device, and the offsets
+    against the oracle.  (The maps of these smooth images are not compared: the unit-magnitude
+    cross power gives every spectral bin the same weight, and the bins where the Gaussians' spectra
+    have decayed to float32 rounding carry phases that are rounding noise in any float32
+    implementation; test_correlation_maps_textured compares maps where the spectrum is not.)"""
+    import torch
+    if case == "integer":
+        shifts = [(-2, 1), (-1, 0), (0, -1), (-1, 1), (0, 0), (1, -1), (0, 1), (1, 0), (2, -1)]
+        sy = sx = 3
+        h = w = 32
+        skip = False
+    else:
+        shifts = [(0.0, 0.0)] * 25
+        shifts[6], shifts[18], shifts[2], shifts[22] = (0.35, -0.42), (-0.35, 0.42), (-0.60, -0.25), (0.60, 0.25)
+        sy = sx = 5
+        h = w = 48
+        skip = True
+    img = translated(sy, sx, h, w, shifts)
+    kw = dict(lam=float(w), dx=1.0, dy=w / h, z=2.0)
+    roi = (0.5, 0.5, 10.0, 10.0, 0.0)
+    op = _af().ShackHartmannSlopes(sy, sx, h, w, roi=roi, skip_outside_pupil=skip, **kw)
+    got = op(torch.from_numpy(img).to(cuda)).cpu().numpy().reshape(-1, 2)
+    exp = SH.shack_hartmann_slopes(img, roi=roi, skip_outside=skip, **kw)
+    # the noise-phase bins move each map by ~1e-2 of its peak, the parabolic refinement by ~3e-3 px
+    assert np.abs(got - exp.reshape(-1, 2)).max() < 1e-2
+    act = op.active()
+    if case == "integer":
+        assert all(act)
+        assert np.abs(got - np.array(shifts, float)).max() < 0.03
+    else:
+        assert abs(got[np.array(act), 0].sum()) < 2e-6 and abs(got[np.array(act), 1].sum()) < 2e-6
+        assert all(got[i, 0] == 0.0 and got[i, 1] == 0.0 for i in range(25) if not act[i])
+        assert abs(got[6, 0] - 0.35) < 0.13 and abs(got[6, 1] + 0.42) < 0.13
+
+
+@pytest.mark.parametrize("sy,h,w", [(3, 32, 32), (5, 34, 51), (3, 17, 40)])
+def test_correlation_maps_textured(cuda, sy, h, w):
+    """Maps and offsets on textured images (every spectral bin well above rounding): sample i is
+    the centre image rolled by an integer offset, so each map is one sharp peak there."""
+    import torch
+    rng = np.random.default_rng(6)
+    base = rng.standard_normal((h, w)).astype(np.float32)
+    offs = [(int(rng.integers(-3, 4)), int(rng.integers(-3, 4))) for _ in range(sy * sy)]
+    offs[(sy // 2) * sy + sy // 2] = (0, 0)
+    img = np.stack([np.roll(base, (dy, dx), axis=(0, 1)) for dx, dy in offs]).reshape(sy, sy, h, w)
+    kw = dict(lam=float(w), dx=1.0, dy=w / h, z=2.0)
+    roi = (0.5, 0.5, 10.0, 10.0, 0.0)
+    op = _af().ShackHartmannSlopes(sy, sy, h, w, roi=roi, skip_outside_pupil=False, **kw)
+    maps = torch.empty((sy, sy, h, w), dtype=torch.float32, device=cuda)
+    got = op(torch.from_numpy(img).to(cuda), maps=maps).cpu().numpy().reshape(-1, 2)
+    exp, emaps = SH.shack_hartmann_slopes(img, roi=roi, skip_outside=False, return_maps=True, **kw)
+    assert np.abs(maps.cpu().numpy() - emaps).max() < 2e-5
+    assert np.abs(got - exp.reshape(-1, 2)).max() < 2e-3
+
+
+def test_zernike_fit_device_equals_host_and_oracle(cuda):
+    import torch
+    from tests.test_shack_oracle import FIT_GEO, ideal_slopes
+    inj = [0.18, -0.11, 0.07, 0.04, -0.03, 0.05, -0.02]
+    s = sum(ideal_slopes(m, inj[m - 4]) for m in range(4, 11)).astype(np.float32)
+    idx = list(range(2, 11))
+    fit = _af().ZernikeFit(5, 5, (10, 10), (10, 10), 0.5, 1.0, 1.0, idx)
+    assert fit.pupil_radius == 25.0
+    dev = fit(torch.from_numpy(s.reshape(-1)).to(cuda)).cpu().numpy()
+    host = np.array(fit.host(s.reshape(-1)), np.float32)
+    assert np.array_equal(dev, host)
+    exp = SH.zernike_from_slopes(s, idx, 0.5, SH.geometry(**FIT_GEO))
+    assert np.abs(dev - exp).max() < 2e-5
+    assert dev[0] == 0.0 and dev[1] == 0.0
+
+
+def test_zernike_phase_correct_phase_wrap(cuda):
+    import torch
+    af = _af()
+    idx = [2, 4, 5, 7, 10]
+    c = np.array([0.3, -1.2, 0.4, 0.25, -0.6], np.float32)
+    ph = af.zernike_phase(torch.from_numpy(c).to(cuda), idx, 96, 130)
+    exp = SH.zernike_phase(c.astype(np.float64), idx, 96, 130)
+    assert np.abs(ph.cpu().numpy() - exp).max() < 1e-5
+    rng = np.random.default_rng(4)
+    x = cfield(rng, (3, 96, 130))
+    got = af.correct_phase(torch.from_numpy(x).to(cuda), ph).cpu().numpy()
+    assert O.rel_l2(got, SH.correct_phase(x, ph.cpu().numpy().astype(np.float64))) < 1e-6
+    xr = rng.standard_normal((2, 96, 130)).astype(np.float32)
+    got = af.correct_phase(torch.from_numpy(xr).to(cuda), ph).cpu().numpy()
+    assert O.rel_l2(got, SH.correct_phase(xr, ph.cpu().numpy().astype(np.float64))) < 1e-6
+    v = (rng.standard_normal(10000) * 20).astype(np.float32)
+    assert np.array_equal(af.wrap2pi(torch.from_numpy(v).to(cuda)).cpu().numpy(), SH.wrap2pi(v))
+
+
+def aberrated_planes(nz, side, a4, seed=5):
+    """Band planes whose one-FFT Fresnel image is a few point scatterers seen through a defocus
+    aberration a4 Z4 (radians) over the pupil: planes = conj(lens) IFFT(points) exp(i a4 Z4)."""
+    rng = np.random.default_rng(seed)
+    lens = SH.stfd_input_lens(side, side, side, side, LAM, Z, DX, DX, "global")
+    y, x = (np.mgrid[0:side, 0:side] - (side - 1) / 2.0) / (side / 2.0)
+    ab = np.exp(1j * a4 * SH.zernike_value(4, x, y))
+    out = np.empty((nz, side, side), np.complex64)
+    for k in range(nz):
+        pts = np.zeros((side, side), np.complex128)
+        for _ in range(6):
+            pts[rng.integers(side // 4, 3 * side // 4), rng.integers(side // 4, 3 * side // 4)] = np.exp(
+                2j * math.pi * rng.random()) * (1.0 + rng.random())
+        out[k] = np.conj(lens) * np.fft.ifft2(pts) * ab * side
+    return out
+
+
+@pytest.mark.parametrize("nb,side,n_iter", [(5, 510, 1), (3, 512, 2)])
+def test_autofocus_chain_matches_oracle_and_recovers_defocus(cuda, nb, side, n_iter):
+    """The whole pass chain against the oracle; the injected defocus comes back as A4 and a second
+    measurement of the corrected planes finds almost none left."""
+    import torch
+    af = _af()
+    a4 = 4.0
+    planes = aberrated_planes(4, side, a4)
+    idx = [4, 5, 6]
+    cfg = SH.AutofocusConfig(nb, LAM, DX, Z, idx)
+    op = af.Autofocus(4, side, side, nb, LAM, DX, Z, indexes=idx, n_iter=n_iter)
+    dev = torch.from_numpy(planes).to(cuda)
+    corrected = op(dev)
+    m0, sl, coeff = op.m0().cpu().numpy(), op.slopes().cpu().numpy(), op.coefficients().cpu().numpy()
+    cur, total_c, total_ph = planes.astype(np.complex128), np.zeros(len(idx)), 0.0
+    for _ in range(n_iter):
+        em0, esl, ec, eph, cur = SH.autofocus(cur, cfg)
+        total_c, total_ph = total_c + ec, total_ph + eph
+    assert O.rel_l2(m0, em0) < 1e-4
+    spp = LAM / ((side // nb) * DX)
+    assert np.abs(sl - esl).max() / spp < 2e-3
+    assert np.abs(coeff - total_c).max() < 1e-3 * max(1.0, np.abs(total_c).max())
+    assert O.rel_l2(op.phase().cpu().numpy(), total_ph) < 1e-3
+    assert O.rel_l2(corrected.cpu().numpy(), cur) < 1e-3
+    # physics: the fit sees the injected defocus, and the corrected planes carry little of it
+    assert abs(coeff[0] - a4) < 0.35 * a4
+    again = af.Autofocus(4, side, side, nb, LAM, DX, Z, indexes=idx)
+    again(corrected)
+    assert abs(again.coefficients().cpu().numpy()[0]) < 0.35 * abs(coeff[0])
+
+
+def test_autofocus_without_orders_passes_planes_through(cuda):
+    import torch
+    planes = aberrated_planes(2, 255, 2.0)
+    op = _af().Autofocus(2, 255, 255, 5, LAM, DX, Z, indexes=[])
+    dev = torch.from_numpy(planes).to(cuda)
+    out = op(dev)
+    assert torch.equal(out, dev)
+    assert op.slopes().shape == (5, 5, 2)
+
+
+def test_validation_messages(cuda):
+    import holoflow_b200 as hf
+    af = _af()
+    with pytest.raises(hf.HfError, match="autofocus_nb_subaps must be odd"):
+        af.Autofocus(2, 64, 64, 4, LAM, DX, Z)
+    with pytest.raises(hf.HfError, match="too large for the current frame size"):
+        af.Autofocus(2, 64, 64, 65, LAM, DX, Z)
+    with pytest.raises(hf.HfError, match="only Noll indexes 2..10"):
+        af.ZernikeFit(5, 5, (10, 10), (10, 10), 0.5, 1.0, 1.0, [11])
+    with pytest.raises(hf.HfError, match="indexes must be unique"):
+        af.ZernikeFit(5, 5, (10, 10), (10, 10), 0.5, 1.0, 1.0, [4, 4])
+    with pytest.raises(hf.HfError, match="dx must equal dy"):
+        af.ShortTimeFresnel((1, 64, 64), (32, 32), (32, 32), LAM, DX, 2 * DX, Z)
+    with pytest.raises(hf.HfError, match="must be odd for an unambiguous center"):
+        af.ShackHartmannSlopes(4, 5, 32, 32, LAM, DX, DX, Z)
+    with pytest.raises(hf.HfError, match="window sides must be in 2..1024"):
+        af.ShortTimeFresnel((1, 2048, 2048), (2048, 2048), (2048, 2048), LAM, DX, DX, Z)
