@@ -44,6 +44,9 @@ class HfDesc(C.Structure):
         ("pad_w", C.c_int32), ("pad_h", C.c_int32), ("as_filter", C.c_int32),
         ("r_inner", C.c_uint32), ("r_outer", C.c_uint32), ("s_inner", C.c_uint32),
         ("s_outer", C.c_uint32), ("time_method", C.c_int32),
+        ("autofocus_nb_subaps", C.c_int32), ("autofocus_n_iter", C.c_int32), ("autofocus_n_orders", C.c_int32),
+        ("autofocus_orders", C.c_int32 * 9), ("autofocus_roi_radius", C.c_float),
+        ("autofocus_keep_outside", C.c_int32),
     ]
 
 
@@ -166,6 +169,7 @@ _PROTOS = {
                                  C.POINTER(_vp)]),
     "hf_holo_write": (C.c_int, [_vp, _vp, _i64]),
     "hf_holo_finish": (C.c_int, [_vp]),
+    "hf_plan_autofocus_coefficients": (C.c_int, [_vp, C.c_int, _vp, _vp]),
     "hf_plan_stage_times": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
     "hf_stfd_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
@@ -175,8 +179,9 @@ _PROTOS = {
     "hf_stfd_set_z": (C.c_int, [_vp, C.c_float, _vp]),
     "hf_stfd_exec": (C.c_int, [_vp, _vp, _vp, _vp]),
     "hf_stfd_destroy": (C.c_int, [_vp]),
-    "hf_shslopes_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
-                                     C.POINTER(HfEllipse), C.c_int, _vp, C.POINTER(_vp)]),
+    "hf_shslopes_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(HfEllipse), C.c_int, _vp,
+                                     C.POINTER(_vp)]),
     "hf_shslopes_active": (C.c_int, [_vp, _vp]),
     "hf_shslopes_exec": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "hf_shslopes_destroy": (C.c_int, [_vp]),

@@ -86,12 +86,13 @@ class ShackHartmannSlopes(_Handle):
     _destroy = "hf_shslopes_destroy"
 
     def __init__(self, sy: int, sx: int, height: int, width: int, lam: float, dx: float, dy: float, z: float,
-                 roi: Sequence[float] = (0.5, 0.5, 0.5, 0.5, 0.0), skip_outside_pupil: bool = True, stream=None):
+                 roi: Sequence[float] = (0.5, 0.5, 0.5, 0.5, 0.0), skip_outside_pupil: bool = True,
+                 sub: Tuple[int, int] = (0, 0), stride: Tuple[int, int] = (0, 0), stream=None):
         super().__init__()
         self.shape = (sy, sx, height, width)
         e = HfEllipse(*[float(v) for v in roi])
-        check(lib().hf_shslopes_create(sy, sx, height, width, lam, dx, dy, z, C.byref(e), int(skip_outside_pupil),
-                                       _stream(stream), C.byref(self._h)))
+        check(lib().hf_shslopes_create(sy, sx, height, width, sub[0], sub[1], stride[0], stride[1], lam, dx, dy, z,
+                                       C.byref(e), int(skip_outside_pupil), _stream(stream), C.byref(self._h)))
 
     def active(self) -> list:
         buf = (C.c_uint8 * (self.shape[0] * self.shape[1]))()

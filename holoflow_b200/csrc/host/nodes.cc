@@ -1166,6 +1166,631 @@ std::unique_ptr<ISyncTask> PctClipFactory::update(std::unique_ptr<ISyncTask> old
 }
 
 // ================================================================================================
+// Shack-Hartmann autofocus: ShortTimeFresnelDiffraction (short_time_fresnel_diffraction.cu:604-840),
+// ShackHartmannSlopes (shack_hartmann_slopes.cu:326-440), ZernikeFromSlopes
+// (zernike_from_slopes.cc:283-377), ZernikePhase (zernike_phase.cu:270-363), CorrectPhase
+// (correct_phase.cu:160-226), Wrap2Pi (wrap2pi.cu), ZernikeDefocusZProp (zernike_defocus_z_prop.cc)
+// ================================================================================================
+namespace {
+void read_indexes(const nlohmann::json &j, std::vector<int> &v) {
+  v.clear();
+  if (j.contains("indexes"))
+    j.at("indexes").get_to(v);
+  else if (j.contains("indices"))
+    j.at("indices").get_to(v);
+}
+void read_ellipse(const nlohmann::json &j, PctClipSettings::Ellipse &e) {
+  if (j.contains("cx"))
+    j.at("cx").get_to(e.cx);
+  if (j.contains("cy"))
+    j.at("cy").get_to(e.cy);
+  if (j.contains("rx"))
+    j.at("rx").get_to(e.rx);
+  if (j.contains("ry"))
+    j.at("ry").get_to(e.ry);
+  if (j.contains("angle"))
+    j.at("angle").get_to(e.angle);
+}
+core::MemLoc read_memloc(const nlohmann::json &j) {
+  const std::string v = j.get<std::string>();
+  if (v == "Host")
+    return core::MemLoc::Host;
+  if (v == "Device")
+    return core::MemLoc::Device;
+  throw std::invalid_argument("invalid MemLoc string");
+}
+} // namespace
+
+void from_json(const nlohmann::json &j, ShortTimeFresnelDiffractionSettings &s) {
+  j.at("lambda").get_to(s.lambda);
+  j.at("dx").get_to(s.dx);
+  j.at("dy").get_to(s.dy);
+  j.at("z").get_to(s.z);
+  j.at("win_h").get_to(s.win_h);
+  j.at("win_w").get_to(s.win_w);
+  j.at("stride_y").get_to(s.stride_y);
+  j.at("stride_x").get_to(s.stride_x);
+  if (j.contains("phase_ref"))
+    j.at("phase_ref").get_to(s.phase_ref);
+  if (s.phase_ref != "LOCAL" && s.phase_ref != "GLOBAL")
+    throw std::invalid_argument("ShortTimeFresnelDiffraction: unknown phase_ref " + s.phase_ref);
+  if (j.contains("skip_phase_shift"))
+    j.at("skip_phase_shift").get_to(s.skip_phase_shift);
+  if (j.contains("output_magnitude"))
+    j.at("output_magnitude").get_to(s.output_magnitude);
+  if (j.contains("axes"))
+    j.at("axes").get_to(s.axes);
+}
+void from_json(const nlohmann::json &j, ShackHartmannSlopeSettings &s) {
+  s.mode = j.value("mode", std::string("single_reference"));
+  if (s.mode != "single_reference" && s.mode != "full_pairwise")
+    throw std::invalid_argument("Unknown Shack-Hartmann slope mode: " + s.mode);
+  j.at("lambda").get_to(s.lambda);
+  j.at("dx").get_to(s.dx);
+  j.at("dy").get_to(s.dy);
+  j.at("z").get_to(s.z);
+  j.at("subaperture_height").get_to(s.subaperture_height);
+  j.at("subaperture_width").get_to(s.subaperture_width);
+  j.at("stride_y").get_to(s.stride_y);
+  j.at("stride_x").get_to(s.stride_x);
+  if (j.contains("correlation_roi"))
+    read_ellipse(j.at("correlation_roi"), s.correlation_roi);
+  s.skip_subapertures_outside_pupil = j.value("skip_subapertures_outside_pupil", true);
+  s.output_xcorr_maps               = j.value("output_xcorr_maps", false);
+  s.pair_batch_size                 = j.value("pair_batch_size", size_t{256});
+}
+void from_json(const nlohmann::json &j, ZernikeFromSlopesSettings &s) {
+  read_indexes(j, s.indexes);
+  j.at("lambda").get_to(s.lambda);
+  j.at("dx").get_to(s.dx);
+  j.at("dy").get_to(s.dy);
+  j.at("subaperture_height").get_to(s.subaperture_height);
+  j.at("subaperture_width").get_to(s.subaperture_width);
+  j.at("stride_y").get_to(s.stride_y);
+  j.at("stride_x").get_to(s.stride_x);
+  s.ny                              = j.value("ny", size_t{1});
+  s.nx                              = j.value("nx", size_t{1});
+  s.skip_subapertures_outside_pupil = j.value("skip_subapertures_outside_pupil", true);
+}
+void from_json(const nlohmann::json &j, ZernikePhaseSettings &s) {
+  read_indexes(j, s.indexes);
+  j.at("ny").get_to(s.ny);
+  j.at("nx").get_to(s.nx);
+  if (j.contains("output"))
+    s.output = read_memloc(j.at("output"));
+  else if (j.contains("device"))
+    s.output = read_memloc(j.at("device"));
+  else
+    s.output = core::MemLoc::Host;
+}
+void from_json(const nlohmann::json &j, ZernikeDefocusZPropSettings &s) {
+  read_indexes(j, s.indexes);
+  j.at("lambda").get_to(s.lambda);
+  j.at("z_curr").get_to(s.z_curr);
+  j.at("pupil_radius").get_to(s.pupil_radius);
+}
+
+namespace {
+void check_noll(const Check &check, const std::vector<int> &idx) {
+  check(!idx.empty(), "indexes must not be empty");
+  check(idx.size() <= 9, "too many requested Zernike modes");
+  for (int v : idx)
+    check(v >= 2 && v <= 10, "only Noll indexes 2..10 are supported");
+  auto u = idx;
+  std::sort(u.begin(), u.end());
+  check(std::adjacent_find(u.begin(), u.end()) == u.end(), "indexes must be unique");
+}
+
+class ShortTimeFresnelTask final : public ISyncTask {
+public:
+  hf_stfd                            *f = nullptr;
+  ShortTimeFresnelDiffractionSettings settings;
+  TDesc                               idesc;
+  cudaStream_t                        stream{};
+  ~ShortTimeFresnelTask() override { hf_stfd_destroy(f); }
+  OpResult execute(SyncCtx &ctx) override {
+    hf_ok(hf_stfd_exec(f, ctx.inputs[0].data(), ctx.outputs[0].data(), stream), "ShortTimeFresnelDiffraction");
+    return OpResult::Ok;
+  }
+};
+
+class ShackHartmannSlopesTask final : public ISyncTask {
+public:
+  hf_shslopes               *p = nullptr;
+  ShackHartmannSlopeSettings settings;
+  TDesc                      idesc;
+  cudaStream_t               stream{};
+  ~ShackHartmannSlopesTask() override { hf_shslopes_destroy(p); }
+  OpResult execute(SyncCtx &ctx) override {
+    float *maps = settings.output_xcorr_maps ? reinterpret_cast<float *>(ctx.outputs[1].data()) : nullptr;
+    hf_ok(hf_shslopes_exec(p, reinterpret_cast<const float *>(ctx.inputs[0].data()),
+                           reinterpret_cast<float *>(ctx.outputs[0].data()), maps, stream),
+          "ShackHartmannSlopes");
+    return OpResult::Ok;
+  }
+};
+
+class ZernikeFromSlopesTask final : public ISyncTask {
+public:
+  hf_zernike_fit           *f = nullptr;
+  ZernikeFromSlopesSettings settings;
+  TDesc                     idesc;
+  cudaStream_t              stream{};
+  ~ZernikeFromSlopesTask() override { hf_zernike_fit_destroy(f); }
+  OpResult execute(SyncCtx &ctx) override {
+    const auto *in  = reinterpret_cast<const float *>(ctx.inputs[0].data());
+    auto       *out = reinterpret_cast<float *>(ctx.outputs[0].data());
+    if (idesc.mem_loc == MemLoc::Host) { // the reference's host fit, after the producer's stream
+      if (cudaStreamSynchronize(stream) != cudaSuccess)
+        throw std::runtime_error("ZernikeFromSlopes: stream synchronisation failed");
+      hf_ok(hf_zernike_fit_host(f, in, out), "ZernikeFromSlopes");
+    } else {
+      hf_ok(hf_zernike_fit_exec(f, in, out, nullptr, stream), "ZernikeFromSlopes");
+    }
+    return OpResult::Ok;
+  }
+};
+
+float zernike_value_host(int noll, float x, float y) { // eval_zernike_noll_value (zernike_phase.cu:88-113)
+  const float s3 = std::sqrt(3.0f), s6 = std::sqrt(6.0f), s8 = std::sqrt(8.0f);
+  switch (noll) {
+  case 2: return 2.0f * x;
+  case 3: return 2.0f * y;
+  case 4: return s3 * (2.0f * (x * x + y * y) - 1.0f);
+  case 5: return 2.0f * s6 * x * y;
+  case 6: return s6 * (x * x - y * y);
+  case 7: return s8 * y * (3.0f * x * x - y * y);
+  case 8: return s8 * y * (3.0f * x * x + 3.0f * y * y - 2.0f);
+  case 9: return s8 * x * (3.0f * x * x + 3.0f * y * y - 2.0f);
+  default: return s8 * x * (x * x - 3.0f * y * y);
+  }
+}
+
+class ZernikePhaseTask final : public ISyncTask {
+public:
+  ZernikePhaseSettings settings;
+  cudaStream_t         stream{};
+  OpResult             execute(SyncCtx &ctx) override {
+    const auto *c   = reinterpret_cast<const float *>(ctx.inputs[0].data());
+    auto       *out = reinterpret_cast<float *>(ctx.outputs[0].data());
+    const int   ny = settings.ny, nx = settings.nx;
+    if (settings.output == MemLoc::Device) {
+      hf_ok(hf_zernike_phase(c, settings.indexes.data(), (int)settings.indexes.size(), ny, nx, out, nullptr, stream),
+            "ZernikePhase");
+      return OpResult::Ok;
+    }
+    const float cy = ((float)ny - 1.0f) * 0.5f, cx = ((float)nx - 1.0f) * 0.5f;
+    const float r  = 0.5f * (float)std::min(ny, nx);
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const float xn = ((float)x - cx) / r, yn = ((float)y - cy) / r;
+        float       ph = 0.f;
+        for (size_t i = 0; i < settings.indexes.size(); ++i)
+          ph += c[i] * zernike_value_host(settings.indexes[i], xn, yn);
+        out[(size_t)y * nx + x] = ph;
+      }
+    return OpResult::Ok;
+  }
+};
+
+class CorrectPhaseTask final : public ISyncTask {
+public:
+  TDesc        idesc;
+  cudaStream_t stream{};
+  OpResult     execute(SyncCtx &ctx) override {
+    const size_t r      = idesc.rank();
+    int64_t      planes = 1;
+    for (size_t i = 0; i + 2 < r; ++i)
+      planes *= (int64_t)idesc.shape[i];
+    hf_ok(hf_correct_phase(ctx.inputs[0].data(), idesc.dtype == DType::CF32 ? 1 : 0,
+                           reinterpret_cast<const float *>(ctx.inputs[1].data()), planes, (int)idesc.shape[r - 2],
+                           (int)idesc.shape[r - 1], ctx.outputs[0].data(), stream),
+          "CorrectPhase");
+    return OpResult::Ok;
+  }
+};
+
+class Wrap2PiTask final : public ISyncTask {
+public:
+  TDesc        idesc;
+  cudaStream_t stream{};
+  OpResult     execute(SyncCtx &ctx) override {
+    hf_ok(hf_wrap2pi(reinterpret_cast<const float *>(ctx.inputs[0].data()), reinterpret_cast<float *>(ctx.outputs[0].data()),
+                     (int64_t)idesc.num_elements(), stream),
+          "Wrap2Pi");
+    return OpResult::Ok;
+  }
+};
+
+class ZernikeDefocusZPropTask final : public ISyncTask {
+public:
+  ZernikeDefocusZPropSettings settings;
+  TDesc                       idesc;
+  cudaStream_t                stream{};
+  double                      estimate[3] = {0.0, 0.0, 0.0}; // delta 1/z, new z, delta z (mm)
+  bool                        valid       = false;
+  OpResult                    execute(SyncCtx &ctx) override {
+    const size_t pos = (size_t)(std::find(settings.indexes.begin(), settings.indexes.end(), 4) - settings.indexes.begin());
+    const float *src = reinterpret_cast<const float *>(ctx.inputs[0].data()) + pos;
+    float        a4  = 0.f;
+    if (idesc.mem_loc == MemLoc::Device) {
+      if (cudaMemcpyAsync(&a4, src, sizeof(float), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+          cudaStreamSynchronize(stream) != cudaSuccess)
+        throw std::runtime_error("ZernikeDefocusZProp: copy of the defocus coefficient failed");
+    } else {
+      a4 = *src;
+    }
+    // an undefined estimate leaves the previous one in place (the reference only logs it)
+    valid = hf_defocus_z(a4, settings.lambda, settings.z_curr, settings.pupil_radius, &estimate[0], &estimate[1],
+                         &estimate[2]) == HF_OK;
+    return OpResult::Ok;
+  }
+};
+
+int64_t leading_planes(const TDesc &d) {
+  int64_t p = 1;
+  for (size_t i = 0; i + 2 < d.rank(); ++i)
+    p *= (int64_t)d.shape[i];
+  return p;
+}
+} // namespace
+
+InferResult ShortTimeFresnelDiffractionFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"ShortTimeFresnelDiffractionFactory"};
+  const auto  s = j.get<ShortTimeFresnelDiffractionSettings>();
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &id = input_descs[0];
+  check(id.rank() >= 2, "input must be rank >= 2");
+  check(id.dtype == DType::CF32 || id.dtype == DType::F32, "input must be CF32 or F32");
+  check(id.mem_loc == MemLoc::Device, "input must be on device");
+  check(id.is_contiguous(), "input must be C-contiguous");
+  check(s.lambda > 0.f, "lambda must be positive");
+  check(s.dx > 0.f, "dx must be positive");
+  check(s.dy > 0.f, "dy must be positive");
+  check(s.dx == s.dy, "dx must equal dy");
+  check(s.z != 0.f, "z must be non-zero");
+  check(s.win_h >= 1 && s.win_w >= 1, "window dimensions must be >= 1");
+  check(s.stride_y >= 1 && s.stride_x >= 1, "strides must be >= 1");
+  const int rank = (int)id.rank();
+  check(s.axes.size() == 2 || s.axes.empty(), "axes must contain exactly two elements");
+  if (s.axes.size() == 2) {
+    const int a0 = s.axes[0] < 0 ? s.axes[0] + rank : s.axes[0], a1 = s.axes[1] < 0 ? s.axes[1] + rank : s.axes[1];
+    check(a0 >= 0 && a0 < rank && a1 >= 0 && a1 < rank, "axes out of bounds");
+    check(a0 != a1, "axes must be distinct");
+    check(a0 == rank - 2 && a1 == rank - 1, "only trailing axes (-2, -1) are supported");
+  }
+  const size_t H = id.shape[rank - 2], W = id.shape[rank - 1];
+  check(s.win_h <= H && s.win_w <= W, "window dimensions exceed field size");
+  std::vector<size_t> shape(id.shape.begin(), id.shape.end() - 2);
+  shape.push_back((H - s.win_h) / s.stride_y + 1);
+  shape.push_back((W - s.win_w) / s.stride_x + 1);
+  shape.push_back(s.win_h);
+  shape.push_back(s.win_w);
+  return sync_result(id, TDesc(shape, s.output_magnitude ? DType::F32 : DType::CF32, MemLoc::Device));
+}
+
+std::unique_ptr<ISyncTask> ShortTimeFresnelDiffractionFactory::create(std::span<const TDesc> input_descs,
+                                                                      const nlohmann::json &j,
+                                                                      const SyncCreateCtx  &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<ShortTimeFresnelTask>();
+  t->settings = j.get<ShortTimeFresnelDiffractionSettings>();
+  t->idesc    = input_descs[0];
+  t->stream   = ctx.stream;
+  const auto  &s = t->settings;
+  const size_t r = t->idesc.rank();
+  hf_ok(hf_stfd_create(leading_planes(t->idesc), (int)t->idesc.shape[r - 2], (int)t->idesc.shape[r - 1],
+                       t->idesc.dtype == DType::F32 ? 1 : 0, (int)s.win_h, (int)s.win_w, (int)s.stride_y,
+                       (int)s.stride_x, s.lambda, s.dx, s.dy, s.z, s.phase_ref == "GLOBAL" ? HF_STFD_GLOBAL : HF_STFD_LOCAL,
+                       s.output_magnitude ? HF_STFD_MAGNITUDE : HF_STFD_COMPLEX, s.skip_phase_shift ? 1 : 0, 0,
+                       ctx.stream, &t->f),
+        "ShortTimeFresnelDiffraction");
+  return t;
+}
+
+// update: the same task for the same settings, the lenses rebuilt when only z changed (:780-840)
+std::unique_ptr<ISyncTask> ShortTimeFresnelDiffractionFactory::update(std::unique_ptr<ISyncTask> old,
+                                                                      std::span<const TDesc> input_descs,
+                                                                      const nlohmann::json &j,
+                                                                      const SyncCreateCtx  &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<ShortTimeFresnelTask *>(old.get());
+  if (t && same_desc(t->idesc, input_descs[0])) {
+    auto s = j.get<ShortTimeFresnelDiffractionSettings>();
+    if (s == t->settings) {
+      t->stream = ctx.stream;
+      return old;
+    }
+    auto z_only = s;
+    z_only.z    = t->settings.z;
+    if (z_only == t->settings) {
+      hf_ok(hf_stfd_set_z(t->f, s.z, ctx.stream), "ShortTimeFresnelDiffraction");
+      t->settings = s, t->stream = ctx.stream;
+      return old;
+    }
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult ShackHartmannSlopesFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"ShackHartmannSlopesFactory"};
+  const auto  s = j.get<ShackHartmannSlopeSettings>();
+  check(input_descs.size() == 1, "task must have exactly one input");
+  const auto &in = input_descs[0];
+  check(in.mem_loc == MemLoc::Device, "input memory location must be Device");
+  check(in.dtype == DType::F32, "input dtype must be F32");
+  check(in.rank() == 5, "input rank must be 5");
+  check(in.shape[0] == 1, "only batch size 1 is supported");
+  check(in.shape[1] > 0 && in.shape[2] > 0, "subaperture grid dimensions must be positive");
+  if (s.mode == "single_reference")
+    check(in.shape[1] % 2 == 1 && in.shape[2] % 2 == 1,
+          "subaperture grid dimensions must be odd for an unambiguous center reference");
+  check(in.shape[3] >= 2 && in.shape[4] >= 2, "reconstruction dimensions must be at least 2");
+  check(s.lambda > 0.f, "wavelength must be > 0");
+  check(s.dx > 0.f && s.dy > 0.f, "pixel pitches must be > 0");
+  check(s.z > 0.f, "propagation distance must be > 0");
+  check(s.subaperture_height > 0 && s.subaperture_width > 0, "subaperture dimensions must be positive");
+  check(s.stride_y > 0 && s.stride_x > 0, "strides must be positive");
+  check(s.correlation_roi.rx > 0.f && s.correlation_roi.ry > 0.f, "correlation ROI radii must be positive");
+  check(s.pair_batch_size > 0, "pair_batch_size must be positive");
+  check(!(s.mode == "full_pairwise" && s.output_xcorr_maps), "FullPairwise correlation-map output is not supported");
+  if (s.mode == "full_pairwise")
+    throw std::logic_error("ShackHartmannSlopes: FullPairwise mode is not built (single_reference only)");
+  std::vector<TDesc> outs{TDesc({1, in.shape[1], in.shape[2], 2}, DType::F32, MemLoc::Device)};
+  if (s.output_xcorr_maps)
+    outs.emplace_back(in.shape, DType::F32, MemLoc::Device);
+  InferResult r = sync_result(in, outs[0]);
+  r.output_descs  = outs;
+  r.owned_outputs = std::vector<bool>(outs.size(), false);
+  return r;
+}
+
+std::unique_ptr<ISyncTask> ShackHartmannSlopesFactory::create(std::span<const TDesc> input_descs,
+                                                              const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<ShackHartmannSlopesTask>();
+  t->settings = j.get<ShackHartmannSlopeSettings>();
+  t->idesc    = input_descs[0];
+  t->stream   = ctx.stream;
+  const auto      &s = t->settings;
+  const hf_ellipse roi{s.correlation_roi.cx, s.correlation_roi.cy, s.correlation_roi.rx, s.correlation_roi.ry,
+                       s.correlation_roi.angle};
+  hf_ok(hf_shslopes_create((int)t->idesc.shape[1], (int)t->idesc.shape[2], (int)t->idesc.shape[3],
+                           (int)t->idesc.shape[4], (int)s.subaperture_height, (int)s.subaperture_width, (int)s.stride_y,
+                           (int)s.stride_x, s.lambda, s.dx, s.dy, s.z, &roi, s.skip_subapertures_outside_pupil ? 1 : 0,
+                           ctx.stream, &t->p),
+        "ShackHartmannSlopes");
+  return t;
+}
+
+std::unique_ptr<ISyncTask> ShackHartmannSlopesFactory::update(std::unique_ptr<ISyncTask> old,
+                                                              std::span<const TDesc> input_descs,
+                                                              const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<ShackHartmannSlopesTask *>(old.get());
+  if (t && t->settings == j.get<ShackHartmannSlopeSettings>() && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult ZernikeFromSlopesFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"ZernikeFromSlopesFactory"};
+  const auto  s = j.get<ZernikeFromSlopesSettings>();
+  check(input_descs.size() == 1, "task must have exactly one input");
+  const auto &in = input_descs[0];
+  check(in.dtype == DType::F32, "input dtype must be F32");
+  check(in.rank() == 4, "input rank must be 4");
+  check(in.shape[0] == 1, "only batch size 1 is supported");
+  check(in.shape[1] > 0 && in.shape[2] > 0, "subaperture grid dimensions must be positive");
+  check(in.shape[3] == 2, "last input dimension must contain [dW/dx, dW/dy]");
+  check(in.is_contiguous(), "input must be C-contiguous");
+  check(s.lambda > 0.f, "wavelength must be > 0");
+  check(s.dx > 0.f && s.dy > 0.f, "pixel pitches must be > 0");
+  check(s.subaperture_height > 0 && s.subaperture_width > 0, "subaperture dimensions must be positive");
+  check(s.stride_y > 0 && s.stride_x > 0, "strides must be positive");
+  check(s.ny == 1 && s.nx == 1, "only global fitting with ny = nx = 1 is supported for zero-mean slopes");
+  check_noll(check, s.indexes);
+  return sync_result(in, TDesc({1, 1, s.indexes.size()}, DType::F32, in.mem_loc));
+}
+
+std::unique_ptr<ISyncTask> ZernikeFromSlopesFactory::create(std::span<const TDesc> input_descs,
+                                                            const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<ZernikeFromSlopesTask>();
+  t->settings = j.get<ZernikeFromSlopesSettings>();
+  t->idesc    = input_descs[0];
+  t->stream   = ctx.stream;
+  const auto &s = t->settings;
+  hf_ok(hf_zernike_fit_create((int)t->idesc.shape[1], (int)t->idesc.shape[2], (int)s.subaperture_height,
+                              (int)s.subaperture_width, (int)s.stride_y, (int)s.stride_x, s.lambda, s.dx, s.dy,
+                              s.skip_subapertures_outside_pupil ? 1 : 0, s.indexes.data(), (int)s.indexes.size(), &t->f),
+        "ZernikeFromSlopesFactory");
+  return t;
+}
+
+std::unique_ptr<ISyncTask> ZernikeFromSlopesFactory::update(std::unique_ptr<ISyncTask> old,
+                                                            std::span<const TDesc> input_descs,
+                                                            const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<ZernikeFromSlopesTask *>(old.get());
+  if (t && t->settings == j.get<ZernikeFromSlopesSettings>() && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult ZernikePhaseFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"ZernikePhaseFactory"};
+  const auto  s = j.get<ZernikePhaseSettings>();
+  check(input_descs.size() == 1, "ZernikePhase task must have exactly one input");
+  const auto &in = input_descs[0];
+  check(in.mem_loc == s.output, "Input coefficients must be in the output memory location");
+  check(in.dtype == DType::F32, "Input coefficients dtype must be F32");
+  check(in.rank() == 1, "Input coefficients rank must be 1");
+  check(in.is_contiguous(), "Input coefficients must be C-contiguous");
+  check(!s.indexes.empty(), "indexes must not be empty");
+  check(s.indexes.size() <= 9, "Too many requested Zernike modes");
+  for (int v : s.indexes)
+    check(v >= 2 && v <= 10, "Only zernike Noll indexes 2..10 are supported");
+  auto u = s.indexes;
+  std::sort(u.begin(), u.end());
+  check(std::adjacent_find(u.begin(), u.end()) == u.end(), "indexes must be unique");
+  check(s.ny > 0 && s.nx > 0, "Resolution ny and nx must be greater than 0");
+  check(in.shape[0] == s.indexes.size(), "Input coefficient count must match settings.indexes size");
+  return sync_result(in, TDesc({(size_t)s.ny, (size_t)s.nx}, DType::F32, s.output));
+}
+
+std::unique_ptr<ISyncTask> ZernikePhaseFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                       const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<ZernikePhaseTask>();
+  t->settings = j.get<ZernikePhaseSettings>();
+  t->stream   = ctx.stream;
+  return t;
+}
+
+std::unique_ptr<ISyncTask> ZernikePhaseFactory::update(std::unique_ptr<ISyncTask> old,
+                                                       std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                       const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<ZernikePhaseTask *>(old.get());
+  if (t && t->settings == j.get<ZernikePhaseSettings>()) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult CorrectPhaseFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &) const {
+  const Check check{"CorrectPhaseFactory"};
+  check(input_descs.size() == 2, "expected exactly two inputs");
+  const auto &id = input_descs[0], &md = input_descs[1];
+  check(id.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(md.mem_loc == MemLoc::Device, "phase mask must be in device memory");
+  check(id.dtype == DType::F32 || id.dtype == DType::CF32, "input dtype must be F32 or CF32");
+  check(md.dtype == DType::F32, "phase mask dtype must be F32");
+  check(id.rank() >= 2, "input rank must be at least 2");
+  check(md.rank() >= 2, "phase mask rank must be at least 2");
+  check(id.shape[id.rank() - 2] == md.shape[md.rank() - 2], "phase mask height must match the input");
+  check(id.shape[id.rank() - 1] == md.shape[md.rank() - 1], "phase mask width must match the input");
+  check(id.is_contiguous() && md.is_contiguous(), "inputs must be C-contiguous");
+  size_t mask_planes = 1;
+  for (size_t i = 0; i + 2 < md.rank(); ++i)
+    mask_planes *= md.shape[i];
+  check(mask_planes == 1, "the phase mask must be one [H, W] plane");
+  InferResult r = sync_result(id, TDesc(id.shape, DType::CF32, MemLoc::Device));
+  r.input_descs  = {id, md};
+  r.owned_inputs = {false, false};
+  return r;
+}
+
+std::unique_ptr<ISyncTask> CorrectPhaseFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                       const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t    = std::make_unique<CorrectPhaseTask>();
+  t->idesc  = input_descs[0];
+  t->stream = ctx.stream;
+  return t;
+}
+
+std::unique_ptr<ISyncTask> CorrectPhaseFactory::update(std::unique_ptr<ISyncTask> old,
+                                                       std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                       const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<CorrectPhaseTask *>(old.get());
+  if (t && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult Wrap2PiFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &) const {
+  const Check check{"Wrap2PiFactory"};
+  check(input_descs.size() == 1, "expected exactly one input");
+  const auto &id = input_descs[0];
+  check(id.mem_loc == MemLoc::Device, "input must be in device memory");
+  check(id.dtype == DType::F32, "input dtype must be F32");
+  check(id.is_contiguous(), "input must be C-contiguous");
+  return sync_result(id, id, {{0, 0}});
+}
+
+std::unique_ptr<ISyncTask> Wrap2PiFactory::create(std::span<const TDesc> input_descs, const nlohmann::json &j,
+                                                  const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t    = std::make_unique<Wrap2PiTask>();
+  t->idesc  = input_descs[0];
+  t->stream = ctx.stream;
+  return t;
+}
+
+std::unique_ptr<ISyncTask> Wrap2PiFactory::update(std::unique_ptr<ISyncTask> old, std::span<const TDesc> input_descs,
+                                                  const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<Wrap2PiTask *>(old.get());
+  if (t && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+InferResult ZernikeDefocusZPropFactory::infer(std::span<const TDesc> input_descs, const nlohmann::json &j) const {
+  const Check check{"ZernikeDefocusZPropFactory"};
+  const auto  s = j.get<ZernikeDefocusZPropSettings>();
+  check(s.lambda > 0.f, "lambda must be positive");
+  check(s.z_curr != 0.f, "z_curr must be non-zero");
+  check(s.pupil_radius > 0.f, "pupil_radius must be positive");
+  check(!s.indexes.empty(), "indexes must not be empty");
+  check(std::find(s.indexes.begin(), s.indexes.end(), 4) != s.indexes.end(), "indexes must contain Z4 defocus");
+  auto u = s.indexes;
+  std::sort(u.begin(), u.end());
+  check(std::adjacent_find(u.begin(), u.end()) == u.end(), "indexes must be unique");
+  check(input_descs.size() == 1, "ZernikeDefocusZProp task must have exactly one input");
+  const auto &id = input_descs[0];
+  check(id.dtype == DType::F32, "Input coefficients dtype must be F32");
+  check(id.rank() == 1, "Input coefficients rank must be 1");
+  check(id.is_contiguous(), "Input coefficients must be C-contiguous");
+  check(id.shape[0] == s.indexes.size(), "Input coefficient count must match settings.indexes size");
+  InferResult r = sync_result(id, id);
+  r.output_descs.clear();
+  r.owned_outputs.clear();
+  return r;
+}
+
+std::unique_ptr<ISyncTask> ZernikeDefocusZPropFactory::create(std::span<const TDesc> input_descs,
+                                                              const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto t      = std::make_unique<ZernikeDefocusZPropTask>();
+  t->settings = j.get<ZernikeDefocusZPropSettings>();
+  t->idesc    = input_descs[0];
+  t->stream   = ctx.stream;
+  return t;
+}
+
+std::unique_ptr<ISyncTask> ZernikeDefocusZPropFactory::update(std::unique_ptr<ISyncTask> old,
+                                                              std::span<const TDesc> input_descs,
+                                                              const nlohmann::json &j, const SyncCreateCtx &ctx) const {
+  (void)infer(input_descs, j);
+  auto *t = dynamic_cast<ZernikeDefocusZPropTask *>(old.get());
+  if (t && t->settings == j.get<ZernikeDefocusZPropSettings>() && same_desc(t->idesc, input_descs[0])) {
+    t->stream = ctx.stream;
+    return old;
+  }
+  old.reset();
+  return create(input_descs, j, ctx);
+}
+
+// ================================================================================================
 // registry
 // ================================================================================================
 void register_path_kinds(core::Registry &r) {
@@ -1183,6 +1808,13 @@ void register_path_kinds(core::Registry &r) {
   r.register_sync("Flatfield", std::make_unique<FlatfieldFactory>());
   r.register_sync("Filter2D", std::make_unique<Filter2DFactory>());
   r.register_sync("PctClip", std::make_unique<PctClipFactory>());
+  r.register_sync("ShortTimeFresnelDiffraction", std::make_unique<ShortTimeFresnelDiffractionFactory>());
+  r.register_sync("ShackHartmannSlopes", std::make_unique<ShackHartmannSlopesFactory>());
+  r.register_sync("ZernikeFromSlopes", std::make_unique<ZernikeFromSlopesFactory>());
+  r.register_sync("ZernikePhase", std::make_unique<ZernikePhaseFactory>());
+  r.register_sync("CorrectPhase", std::make_unique<CorrectPhaseFactory>());
+  r.register_sync("Wrap2Pi", std::make_unique<Wrap2PiFactory>());
+  r.register_sync("ZernikeDefocusZProp", std::make_unique<ZernikeDefocusZPropFactory>());
 }
 
 core::Registry &default_registry() {

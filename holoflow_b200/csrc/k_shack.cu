@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "hf_common.cuh"
+#include "k_shack.cuh"
 
 namespace hf {
 namespace {
@@ -889,8 +890,9 @@ void release(hf_shslopes *p) {
 
 extern "C" {
 
-int hf_shslopes_create(int sy, int sx, int height, int width, float lambda, float dx, float dy, float z,
-                       const hf_ellipse *roi, int skip_outside, hf_stream_t s, hf_shslopes **out) {
+int hf_shslopes_create(int sy, int sx, int height, int width, int sub_h, int sub_w, int stride_y, int stride_x,
+                       float lambda, float dx, float dy, float z, const hf_ellipse *roi, int skip_outside, hf_stream_t s,
+                       hf_shslopes **out) {
   clear_error();
   HF_CHECK_ARG(out != nullptr, "ShackHartmannSlopesFactory inference error: null argument");
   *out = nullptr;
@@ -903,8 +905,12 @@ int hf_shslopes_create(int sy, int sx, int height, int width, float lambda, floa
   HF_CHECK_ARG(z > 0.f, "ShackHartmannSlopesFactory inference error: propagation distance must be > 0");
   const hf_ellipse e = roi ? *roi : hf_ellipse{0.5f, 0.5f, 0.5f, 0.5f, 0.f};
   HF_CHECK_ARG(e.rx > 0.f && e.ry > 0.f, "ShackHartmannSlopesFactory inference error: correlation ROI radii must be positive");
+  if (sub_h <= 0 && sub_w <= 0 && stride_y <= 0 && stride_x <= 0) // 0: the image size, stride = size
+    sub_h = stride_y = height, sub_w = stride_x = width;
+  HF_CHECK_ARG(sub_h > 0 && sub_w > 0, "ShackHartmannSlopesFactory inference error: subaperture dimensions must be positive");
+  HF_CHECK_ARG(stride_y > 0 && stride_x > 0, "ShackHartmannSlopesFactory inference error: strides must be positive");
   std::vector<Sample> geo;
-  const float r = geometry(sy, sx, height, width, height, width, dy, dx, skip_outside != 0, geo);
+  const float r = geometry(sy, sx, sub_h, sub_w, stride_y, stride_x, dy, dx, skip_outside != 0, geo);
   HF_CHECK_ARG(r > 0.f, "ShackHartmannSlopesFactory inference error: pupil radius must be positive");
   HF_CHECK_ARG(std::any_of(geo.begin(), geo.end(), [](const Sample &g) { return g.active; }),
                "ShackHartmannSlopesFactory inference error: at least one subaperture must be active");
@@ -1301,7 +1307,8 @@ int hf_autofocus_create(int nz, int height, int width, int nb_subaps, int n_iter
   int rc = hf_stfd_create(nz, height, width, 0, a->sh, a->sw, a->sh, a->sw, lambda, dx, dx, z, HF_STFD_GLOBAL,
                           HF_STFD_MEAN_MAGNITUDE, 1, 1, s, &a->stfd);
   if (rc == HF_OK)
-    rc = hf_shslopes_create(nb_subaps, nb_subaps, a->sh, a->sw, lambda, dx, dx, z, &roi, skip_outside, s, &a->sl);
+    rc = hf_shslopes_create(nb_subaps, nb_subaps, a->sh, a->sw, a->sh, a->sw, a->sh, a->sw, lambda, dx, dx, z, &roi,
+                            skip_outside, s, &a->sl);
   if (rc == HF_OK && n_indexes > 0)
     rc = hf_zernike_fit_create(nb_subaps, nb_subaps, a->sh, a->sw, a->sh, a->sw, lambda, dx, dx, skip_outside, indexes,
                                n_indexes, &a->fit);
@@ -1335,23 +1342,18 @@ int hf_autofocus_pupil_radius(const hf_autofocus *a, float *r) {
 int hf_autofocus_exec(hf_autofocus *a, const void *planes, const void *delayed, void *corrected, hf_stream_t s) {
   clear_error();
   HF_CHECK_ARG(a != nullptr && planes != nullptr && corrected != nullptr, "Autofocus: null argument");
-  const int64_t plane = (int64_t)a->H * a->W, total = (int64_t)a->nz * plane;
-  HF_CUDA(cudaMemsetAsync(a->cum_coeffs, 0, kShkMaxModes * sizeof(float), s));
-  HF_CUDA(cudaMemsetAsync(a->cum_phase, 0, (size_t)plane * sizeof(float), s));
+  const int64_t total = (int64_t)a->nz * a->H * a->W;
+  HF_TRY(hf::autofocus_begin(a, s));
   for (int pass = 0; pass < a->n_iter; ++pass) {
     // pass 0 measures the current spectrum and corrects the delayed one; later passes measure and
     // correct their predecessor's output (graph_builder.cc:149-153)
     const void *cur = pass == 0 ? planes : corrected;
     const void *del = pass == 0 ? (delayed ? delayed : planes) : corrected;
-    HF_TRY(hf_stfd_exec(a->stfd, cur, a->m0, s));
-    HF_TRY(hf_shslopes_exec(a->sl, a->m0, a->slopes, nullptr, s));
-    if (a->nidx > 0) {
-      HF_TRY(hf_zernike_fit_exec(a->fit, a->slopes, a->coeffs, a->cum_coeffs, s));
-      HF_TRY(hf_zernike_phase(a->coeffs, a->idx, a->nidx, a->H, a->W, a->phase, a->cum_phase, s));
+    HF_TRY(hf::autofocus_measure(a, cur, s));
+    if (a->nidx > 0)
       HF_TRY(hf_correct_phase(del, 1, a->phase, a->nz, a->H, a->W, corrected, s));
-    } else if (del != corrected) { // no Zernike orders: a zero phase map, E exp(-i 0) = E
+    else if (del != corrected) // no Zernike orders: a zero phase map, E exp(-i 0) = E
       HF_CUDA(cudaMemcpyAsync(corrected, del, (size_t)total * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-    }
   }
   return HF_OK;
 }
@@ -1381,3 +1383,52 @@ int hf_autofocus_destroy(hf_autofocus *a) {
 }
 
 } // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Internal entry points of the fused pipeline (k_shack.cuh)
+// ------------------------------------------------------------------------------------------------
+namespace hf {
+namespace {
+// lens exp(-i phase): the correction folded into the Fresnel lens that the row pass multiplies by
+__global__ void shk_fold_lens_kernel(const float2 *lens, const float *phase, float2 *out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float sv, cv;
+    sincosf(phase[i], &sv, &cv);
+    const float2 l = lens[i];
+    out[i]         = make_float2(l.x * cv + l.y * sv, l.y * cv - l.x * sv);
+  }
+}
+} // namespace
+
+int autofocus_begin(hf_autofocus *a, cudaStream_t s) {
+  HF_CUDA(cudaMemsetAsync(a->cum_coeffs, 0, kShkMaxModes * sizeof(float), s));
+  HF_CUDA(cudaMemsetAsync(a->cum_phase, 0, (size_t)a->H * a->W * sizeof(float), s));
+  return HF_OK;
+}
+
+int autofocus_measure(hf_autofocus *a, const void *planes, cudaStream_t s) {
+  HF_TRY(hf_stfd_exec(a->stfd, planes, a->m0, s));
+  HF_TRY(hf_shslopes_exec(a->sl, a->m0, a->slopes, nullptr, s));
+  if (a->nidx > 0) {
+    HF_TRY(hf_zernike_fit_exec(a->fit, a->slopes, a->coeffs, a->cum_coeffs, s));
+    HF_TRY(hf_zernike_phase(a->coeffs, a->idx, a->nidx, a->H, a->W, a->phase, a->cum_phase, s));
+  }
+  return HF_OK;
+}
+
+int autofocus_correct(hf_autofocus *a, const void *planes, void *out, cudaStream_t s) {
+  return hf_correct_phase(planes, 1, a->phase, a->nz, a->H, a->W, out, s);
+}
+
+int autofocus_fold_lens(hf_autofocus *a, const float2 *lens, float2 *out, cudaStream_t s) {
+  const int64_t n = (int64_t)a->H * a->W;
+  shk_fold_lens_kernel<<<grid_1d(n), 256, 0, s>>>(lens, a->phase, out, n);
+  note_launch();
+  return launch_status("shk_fold_lens_kernel");
+}
+
+int autofocus_passes(const hf_autofocus *a) { return a->n_iter; }
+int autofocus_orders(const hf_autofocus *a) { return a->nidx; }
+const float *autofocus_cumulative_coeffs(const hf_autofocus *a) { return a->cum_coeffs; }
+
+} // namespace hf

@@ -22,6 +22,7 @@
 #include "k_misc.cuh"
 #include "k_pca.cuh"
 #include "k_post.cuh"
+#include "k_shack.cuh"
 #include "k_tc_band.cuh"
 #include "tma_host.cuh"
 
@@ -39,10 +40,12 @@ enum Stage {
   ST_COLS_MOM,
   ST_COLS_TF,
   ST_ROWS_MOM,
+  ST_AUTOFOCUS,
   ST_COUNT
 };
-const char *kStageName[ST_COUNT] = {"covariance", "eigen_filter", "band_dft", "fft_rows",
-                                    "band_dft_rows", "fft_cols_moments", "fft_cols_tf", "fft_rows_moments"};
+const char *kStageName[ST_COUNT] = {"covariance",       "eigen_filter", "band_dft",         "fft_rows",
+                                    "band_dft_rows",    "fft_cols_moments", "fft_cols_tf", "fft_rows_moments",
+                                    "autofocus"};
 static_assert(ST_COUNT <= HF_MAX_STAGES, "stage table");
 
 struct StageTimer {
@@ -103,9 +106,17 @@ struct hf_plan {
   // Filter2D on the band planes before the Fresnel lens (graph_builder.cc:124-126, 568-576)
   bool    filter2d = false;
   float2 *f2d      = nullptr; // [H][W] annulus mask in natural frequency order
+  // Shack-Hartmann autofocus on every window's band planes before the lens (graph_builder.cc:139-153)
+  hf_autofocus *af       = nullptr;
+  float2       *lens_af  = nullptr; // [H][W] lens with the window's correction folded in
+  float        *af_coeff = nullptr; // [max_batch][9] coefficients of the last exec
 };
 
 static void plan_free(hf_plan *p) {
+  hf_autofocus_destroy(p->af);
+  p->af = nullptr;
+  dev_free(p->lens_af);
+  dev_free(p->af_coeff);
   dev_free(p->f2d);
   dev_free(p->lens);
   dev_free(p->tf);
@@ -221,7 +232,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
   BandArgs ba{};
   ba.ring = fr, ba.T = d.frames, ba.P = p->P, ba.H = d.height, ba.W = d.width, ba.nz = p->nz;
   ba.wmat = wmat, ba.wmat_stride = wstride, ba.z0 = d.z_begin;
-  ba.lens = d.propagation == HF_PROP_FRESNEL && !p->filter2d ? p->lens : nullptr;
+  ba.lens = d.propagation == HF_PROP_FRESNEL && !p->filter2d && !p->af ? p->lens : nullptr;
   ba.out = p->band, ba.OH = d.height, ba.OW = d.width, ba.oy = 0, ba.ox = 0;
   ba.out_plane = p->P, ba.out_win = win_px, ba.scale = 1.0f;
   int rec = p->timer.begin(s, ST_BAND);
@@ -247,9 +258,37 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     rp.IH = d.height, rp.IW = d.width, rp.H = d.height, rp.N = d.width, rp.nplanes = p->nz, rp.inverse = 0;
     rp.out = p->fast ? p->band : p->band2, rp.out_win = win_px, rp.out_plane = p->P, rp.out_row = d.width;
     rp.pre = p->filter2d ? p->lens : nullptr; // the lens, when the band pass could not fuse it
-    rec = p->timer.begin(s, ST_ROWS);
-    HF_TRY(launch_row_pass(rp, nwin, s));
-    p->timer.end(s, rec);
+    if (p->af) {
+      // per window: passes 1..n-1 correct the planes in place, the last pass's correction is
+      // folded into the lens of the window's row pass (no extra read and write of the planes)
+      rec = p->timer.begin(s, ST_AUTOFOCUS);
+      for (int w = 0; w < nwin; ++w) {
+        float2 *planes = p->band + w * win_px;
+        HF_TRY(autofocus_begin(p->af, s));
+        for (int pass = 0; pass < autofocus_passes(p->af); ++pass) {
+          HF_TRY(autofocus_measure(p->af, planes, s));
+          if (pass + 1 < autofocus_passes(p->af))
+            HF_TRY(autofocus_correct(p->af, planes, planes, s));
+        }
+        HF_TRY(autofocus_fold_lens(p->af, p->lens, p->lens_af + (int64_t)w * p->P, s));
+        HF_CUDA(cudaMemcpyAsync(p->af_coeff + 9 * w, autofocus_cumulative_coeffs(p->af), 9 * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+      }
+      p->timer.end(s, rec);
+      rec = p->timer.begin(s, ST_ROWS);
+      for (int w = 0; w < nwin; ++w) { // one row pass per window, each with its own lens
+        RowPass rw = rp;
+        rw.in      = p->band + w * win_px;
+        rw.out     = rp.out + w * win_px;
+        rw.pre     = p->lens_af + (int64_t)w * p->P;
+        HF_TRY(launch_row_pass(rw, 1, s));
+      }
+      p->timer.end(s, rec);
+    } else {
+      rec = p->timer.begin(s, ST_ROWS);
+      HF_TRY(launch_row_pass(rp, nwin, s));
+      p->timer.end(s, rec);
+    }
     if (p->fast)
       return cols_moments(p, nwin, out, s);
     ColPass cp{};
@@ -344,6 +383,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
   p->frame_bytes = frame_bytes_of(d.input_dtype, p->P);
   p->fast        = fft_fast_length(OH) && fft_fast_length(OW);
   p->filter2d    = d.as_filter != 0 && d.propagation != HF_PROP_ANGULAR_SPECTRUM;
+  const bool autofocus = d.autofocus_nb_subaps > 0 && d.autofocus_n_orders > 0;
   p->mom.nz       = p->nz;
   p->mom.mask     = d.moment_mask;
   p->mom.fftshift = d.fftshift;
@@ -357,6 +397,29 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
     if (p->filter2d && !(p->fast && d.height <= 1024)) {
       rc = fail(HF_ERR_UNSUPPORTED, "plan: Filter2D needs frame sides in {64..1536} (height <= 1024)");
       break;
+    }
+    if (autofocus) {
+      if (d.propagation == HF_PROP_ANGULAR_SPECTRUM) { // graph_builder.cc:535-537
+        rc = fail(HF_ERR_INVALID, "Angular Spectrum is not supported with Shack-Hartmann autofocus");
+        break;
+      }
+      if (d.propagation != HF_PROP_FRESNEL || !p->fast) {
+        rc = fail(HF_ERR_UNSUPPORTED, "plan: autofocus needs Fresnel propagation on frame sides in {64..1536}");
+        break;
+      }
+      if (d.autofocus_n_orders > 9) {
+        rc = fail(HF_ERR_INVALID, "plan: at most 9 autofocus orders");
+        break;
+      }
+      if ((rc = hf_autofocus_create(p->nz, d.height, d.width, d.autofocus_nb_subaps, std::max(1, d.autofocus_n_iter),
+                                    d.lambda, d.pitch, d.z,
+                                    d.autofocus_roi_radius > 0.f ? d.autofocus_roi_radius : 0.5f,
+                                    d.autofocus_keep_outside ? 0 : 1, d.autofocus_orders, d.autofocus_n_orders, stream,
+                                    &p->af)))
+        break;
+      if ((rc = dev_alloc(&p->lens_af, (size_t)(B * p->P), p->bytes)) ||
+          (rc = dev_alloc(&p->af_coeff, (size_t)(9 * B), p->bytes)))
+        break;
     }
     const int64_t plane = (int64_t)p->P, oplane = (int64_t)OH * OW;
     if ((rc = dev_alloc(&p->band, (size_t)(B * p->nz * plane), p->bytes)))
@@ -399,7 +462,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       break;
     // the tensor-core band pass holds 2 (z1 - z0) real columns per pixel: the one-sided band only
     p->rows_tc = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
-                 d.time_method == HF_TIME_RFFT && !p->filter2d &&
+                 d.time_method == HF_TIME_RFFT && !p->filter2d && !p->af &&
                  band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
     if (d.propagation == HF_PROP_FRESNEL && p->fast && col_moments_tma_supported(d.height, d.width)) {
       const uint64_t rows = (uint64_t)B * p->nz * d.height;
@@ -484,6 +547,16 @@ int hf_plan_timing(hf_plan *p, int enable) {
   p->timer.on    = enable != 0;
   p->timer.n     = 0;
   p->timer.nexec = 0;
+  return HF_OK;
+}
+
+int hf_plan_autofocus_coefficients(hf_plan *p, int w, float *coeffs, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr && coeffs != nullptr, "hf_plan_autofocus_coefficients: null argument");
+  HF_CHECK_ARG(p->af != nullptr, "hf_plan_autofocus_coefficients: the plan has no autofocus");
+  HF_CHECK_ARG(w >= 0 && w < p->d.max_batch, "hf_plan_autofocus_coefficients: window out of range");
+  HF_CUDA(cudaMemcpyAsync(coeffs, p->af_coeff + 9 * w, (size_t)p->d.autofocus_n_orders * sizeof(float),
+                          cudaMemcpyDeviceToDevice, s));
   return HF_OK;
 }
 

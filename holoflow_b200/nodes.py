@@ -123,7 +123,10 @@ def run_sync_factory(kind: str, settings: dict[str, Any], inputs: Sequence[torch
     node = Node(kind, settings, descs)
     try:
         n_out = len(infer(kind, settings, descs))
-        outs = [empty_like_desc(node.output_desc(i), inputs[0].device) for i in range(n_out)]
+        outs = []
+        for i in range(n_out):
+            d = node.output_desc(i)
+            outs.append(empty_like_desc(d, inputs[0].device if d.mem_loc == 1 else "cpu"))
         r = node.execute(inputs, outs)
         if r != 0:
             raise HfError(r, f"{kind}: execute returned OpResult {r}")

@@ -4,7 +4,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import Optional
+from typing import Optional, Sequence
 
 import torch
 
@@ -98,13 +98,21 @@ class PipelineConfig:
     s_inner: int = 0
     s_outer: int = 0
     time_method: int = 0  # HF_TIME_RFFT; HF_TIME_FFT = two-sided band, 2 (z_end - z_begin) planes
+    autofocus_nb_subaps: int = 0  # Shack-Hartmann autofocus before the lens (odd; 0 = off)
+    autofocus_n_iter: int = 1
+    autofocus_orders: Sequence[int] = ()  # Noll indexes 2..10 (empty = off)
+    autofocus_roi_radius: float = 0.5
+    autofocus_keep_outside: int = 0
 
     def desc(self) -> HfDesc:
+        orders = list(self.autofocus_orders)
         return HfDesc(self.height, self.width, self.frames, self.hop, self.z_begin, self.z_end,
                       self.input_dtype, self.propagation, self.clutter_rank, self.moment_mask,
                       self.fftshift, self.form, self.max_batch, self.lam, self.pitch, self.z, self.fs,
                       self.pad_w, self.pad_h, self.as_filter, self.r_inner, self.r_outer,
-                      self.s_inner, self.s_outer, self.time_method)
+                      self.s_inner, self.s_outer, self.time_method, self.autofocus_nb_subaps,
+                      self.autofocus_n_iter, len(orders), (C.c_int32 * 9)(*orders), self.autofocus_roi_radius,
+                      self.autofocus_keep_outside)
 
     @property
     def frame_bytes(self) -> int:
@@ -157,11 +165,17 @@ class Pipeline:
 
     def stage_times(self):
         """{stage: (total ms, execs)} of the execs recorded since timing(True)."""
-        ms = (C.c_float * 8)()
-        names = (C.c_char_p * 8)()
+        ms = (C.c_float * 16)()  # HF_MAX_STAGES
+        names = (C.c_char_p * 16)()
         ns, ne = C.c_int(), C.c_int()
         check(lib().hf_plan_stage_times(self._plan, ms, names, C.byref(ns), C.byref(ne)))
         return {names[k].decode(): (ms[k], ne.value) for k in range(ns.value)}
+
+    def autofocus_coefficients(self, w: int = 0) -> torch.Tensor:
+        """Window w's Zernike coefficients (radians, autofocus_orders order) of the last run."""
+        out = torch.empty(len(self.cfg.autofocus_orders), dtype=torch.float32, device="cuda")
+        check(lib().hf_plan_autofocus_coefficients(self._plan, w, _ptr(out), _stream()))
+        return out
 
     def close(self) -> None:
         if self._plan:

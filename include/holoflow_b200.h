@@ -200,6 +200,15 @@ typedef struct hf_desc {
   int32_t time_method;       /* HF_TIME_RFFT (0): the band [z0, z1); HF_TIME_FFT: the two-sided
                                 method, [z0, z1) then [T - z1, T - z0), 2 (z1 - z0) planes
                                 (graph_builder.cc:270-287, weights 590-594)                   */
+  /* Shack-Hartmann autofocus before the Fresnel propagation (graph_builder.cc:139-153, 307-501):
+   * each window's band planes are measured on nb x nb sub-apertures and corrected by the fitted
+   * Zernike phase.  0 sub-apertures or 0 orders: off.  Fresnel propagation only.             */
+  int32_t autofocus_nb_subaps;   /* odd                                                        */
+  int32_t autofocus_n_iter;      /* passes (0 reads as 1)                                      */
+  int32_t autofocus_n_orders;    /* entries of autofocus_orders in use                         */
+  int32_t autofocus_orders[9];   /* Noll indexes 2..10                                         */
+  float   autofocus_roi_radius;  /* correlation ROI radius (pp_pctclip_radius; 0 reads as 0.5) */
+  int32_t autofocus_keep_outside; /* 1: keep sub-apertures outside the pupil                   */
 } hf_desc;
 #define HF_TIME_RFFT 0
 #define HF_TIME_FFT 1
@@ -225,13 +234,18 @@ int hf_pipeline_exec(hf_plan *plan, const void *ring, int64_t ring_frames, int64
  * stream between stages (up to 128 execs after hf_plan_timing(plan, 1), which also resets the
  * record).  hf_plan_stage_times sums, per stage, the elapsed milliseconds over the recorded execs
  * (call after synchronising the stream); names[k] (optional) receives static stage names. */
-#define HF_MAX_STAGES 8
+#define HF_MAX_STAGES 16
 int hf_plan_timing(hf_plan *plan, int enable);
 int hf_plan_stage_times(hf_plan *plan, float *ms, const char **names, int *nstages, int *nexec);
 
 /* Device status word of the plan (synchronises the device): 0, or the code of the first bounded
  * device-side wait (tensor-core pipeline mbarriers) that expired; `reset` clears it. */
 int hf_plan_status(hf_plan *plan, int *status, int reset);
+
+/* With autofocus on: window w's Zernike coefficients (radians, summed over the passes, in
+ * autofocus_orders order) of the last hf_pipeline_exec, copied into the device buffer `coeffs`
+ * (autofocus_n_orders floats) on stream s. */
+int hf_plan_autofocus_coefficients(hf_plan *plan, int w, float *coeffs, hf_stream_t s);
 
 /* Debug/inspection: after hf_pipeline_exec, copy window `w`'s T x T Gram matrix (float64) and
  * its filter+DFT matrix W (complex64 [T][Nz]) to device buffers (either may be NULL). */
@@ -471,12 +485,15 @@ int hf_stfd_destroy(hf_stfd *f);
  * shack_hartmann_slopes.hh:28-61): images [sy][sx][h][w] float32 (sy, sx odd) -> slopes
  * [sy][sx][2] float32: each image phase-correlated with the centre one inside the ROI ellipse
  * (mean removed, cosine taper), peak offset with parabolic refinement, times lambda / (n d),
- * centre offset and the mean over the active sub-apertures removed (inactive ones 0).  `maps`
+ * centre offset and the mean over the active sub-apertures removed (inactive ones 0).  The
+ * active set comes from the sub-aperture geometry (sub_h x sub_w every stride_y / stride_x
+ * pixels; all four 0: the image size).  `maps`
  * (optional, [sy][sx][h][w]) receives the correlation maps.  hf_shslopes_active writes the
  * active flags (1 byte per sub-aperture). */
 typedef struct hf_shslopes hf_shslopes;
-int hf_shslopes_create(int sy, int sx, int height, int width, float lambda, float dx, float dy, float z,
-                       const hf_ellipse *roi, int skip_outside_pupil, hf_stream_t s, hf_shslopes **p);
+int hf_shslopes_create(int sy, int sx, int height, int width, int sub_h, int sub_w, int stride_y, int stride_x,
+                       float lambda, float dx, float dy, float z, const hf_ellipse *roi, int skip_outside_pupil,
+                       hf_stream_t s, hf_shslopes **p);
 int hf_shslopes_active(const hf_shslopes *p, uint8_t *active);
 int hf_shslopes_exec(hf_shslopes *p, const float *images, float *slopes, float *maps, hf_stream_t s);
 int hf_shslopes_destroy(hf_shslopes *p);

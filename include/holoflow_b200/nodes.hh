@@ -94,6 +94,50 @@ struct PctClipSettings {
   bool    operator==(const PctClipSettings &) const = default;
 };
 
+// Shack-Hartmann autofocus (holotask/include/holotask/syncs/short_time_fresnel_diffraction.hh,
+// shack_hartmann_slopes.hh, zernike_from_slopes.hh, zernike_phase.hh, zernike_defocus_z_prop.hh):
+// the same keys and defaults.
+struct ShortTimeFresnelDiffractionSettings {
+  float            lambda = 0.f, dx = 0.f, dy = 0.f, z = 0.f;
+  size_t           win_h = 0, win_w = 0, stride_y = 0, stride_x = 0;
+  std::string      phase_ref        = "LOCAL"; // LOCAL | GLOBAL
+  bool             skip_phase_shift = true, output_magnitude = false;
+  std::vector<int> axes             = {-2, -1};
+  bool             operator==(const ShortTimeFresnelDiffractionSettings &) const = default;
+};
+struct ShackHartmannSlopeSettings {
+  std::string             mode   = "single_reference"; // single_reference (full_pairwise: not built)
+  float                   lambda = 0.f, dx = 0.f, dy = 0.f, z = 0.f;
+  size_t                  subaperture_height = 0, subaperture_width = 0, stride_y = 0, stride_x = 0;
+  PctClipSettings::Ellipse correlation_roi;
+  bool                    skip_subapertures_outside_pupil = true, output_xcorr_maps = false;
+  size_t                  pair_batch_size                 = 256;
+  bool                    operator==(const ShackHartmannSlopeSettings &) const = default;
+};
+struct ZernikeFromSlopesSettings {
+  std::vector<int> indexes;
+  float            lambda = 0.f, dx = 0.f, dy = 0.f;
+  size_t           subaperture_height = 0, subaperture_width = 0, stride_y = 0, stride_x = 0, ny = 1, nx = 1;
+  bool             skip_subapertures_outside_pupil = true;
+  bool             operator==(const ZernikeFromSlopesSettings &) const = default;
+};
+struct ZernikePhaseSettings {
+  std::vector<int> indexes;
+  int              ny = 0, nx = 0;
+  core::MemLoc     output = core::MemLoc::Host;
+  bool             operator==(const ZernikePhaseSettings &) const = default;
+};
+struct ZernikeDefocusZPropSettings {
+  std::vector<int> indexes;
+  float            lambda = 0.f, z_curr = 0.f, pupil_radius = 0.f;
+  bool             operator==(const ZernikeDefocusZPropSettings &) const = default;
+};
+
+void from_json(const nlohmann::json &j, ShortTimeFresnelDiffractionSettings &s);
+void from_json(const nlohmann::json &j, ShackHartmannSlopeSettings &s);
+void from_json(const nlohmann::json &j, ZernikeFromSlopesSettings &s);
+void from_json(const nlohmann::json &j, ZernikePhaseSettings &s);
+void from_json(const nlohmann::json &j, ZernikeDefocusZPropSettings &s);
 void from_json(const nlohmann::json &j, FresnelDiffractionSettings &s);
 void from_json(const nlohmann::json &j, FFTShiftSettings &s);
 void from_json(const nlohmann::json &j, FlatfieldSettings &s);
@@ -141,6 +185,13 @@ HFB_SYNC_FACTORY(FFTShiftFactory);  // kind "FFTShiftNp"
 HFB_SYNC_FACTORY(FlatfieldFactory);
 HFB_SYNC_FACTORY(Filter2DFactory);
 HFB_SYNC_FACTORY(PctClipFactory);
+HFB_SYNC_FACTORY(ShortTimeFresnelDiffractionFactory);
+HFB_SYNC_FACTORY(ShackHartmannSlopesFactory); // [1, sy, sx, h, w] -> slopes [1, sy, sx, 2] (+ maps)
+HFB_SYNC_FACTORY(ZernikeFromSlopesFactory);   // Host input as the reference; Device input runs the device fit
+HFB_SYNC_FACTORY(ZernikePhaseFactory);
+HFB_SYNC_FACTORY(CorrectPhaseFactory);
+HFB_SYNC_FACTORY(Wrap2PiFactory);
+HFB_SYNC_FACTORY(ZernikeDefocusZPropFactory); // sink: no outputs; the task keeps the last estimate
 HFB_SYNC_FACTORY(HolofileFactory); // frames [batch, H, W] (12-bit: packed rows [batch, H, 3W/2] U8)
 #undef HFB_SYNC_FACTORY
 

@@ -504,6 +504,8 @@ class PathConfig:
     time_method: str = "rfft"      # "rfft" (one-sided band) | "fft" (two-sided, 2 Nz planes)
     filter2d: Optional[dict] = None  # r_inner/r_outer/s_inner/s_outer: Filter2D on the band planes
                                      # before Fresnel (graph_builder.cc:124-126)
+    autofocus: Optional[dict] = None  # nb, orders, n_iter, roi_radius, keep_outside: Shack-Hartmann
+                                      # autofocus before Fresnel (graph_builder.cc:139-153)
 
     @property
     def nz(self) -> int:
@@ -537,9 +539,26 @@ def reconstruct_window(window: np.ndarray, cfg: PathConfig) -> np.ndarray:
     if cfg.filter2d and cfg.propagation != "angular_spectrum":
         f = cfg.filter2d
         planes = filter2d(planes, f["r_inner"], f["r_outer"], f["s_inner"], f["s_outer"])
+    if cfg.autofocus and cfg.autofocus.get("orders"):
+        planes = autofocus_planes(planes, cfg)[0]
     mag = propagate(planes, cfg)
     w = freq_weights(cfg.frames, cfg.z0, cfg.z1, cfg.fs, cfg.time_method)
     return moments_from_magnitude(mag, w, cfg.fftshift)
+
+
+def autofocus_planes(planes: np.ndarray, cfg: PathConfig):
+    """The autofocus passes on one window's band planes (oracle/shack.py); returns the corrected
+    planes and the coefficients summed over the passes."""
+    from . import shack as SH
+    a = cfg.autofocus
+    acfg = SH.AutofocusConfig(a["nb"], cfg.lam, cfg.pitch, cfg.z, list(a["orders"]), a.get("roi_radius", 0.5),
+                              not a.get("keep_outside", False))
+    total = np.zeros(len(acfg.indexes))
+    cur = np.asarray(planes, np.complex128)
+    for _ in range(a.get("n_iter", 1)):
+        r = SH.autofocus(cur, acfg)
+        cur, total = r[4], total + r[2]
+    return cur, total
 
 
 def band_bins(f_lo: float, f_hi: float, fs: float, T: int) -> tuple[int, int]:

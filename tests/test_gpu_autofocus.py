@@ -251,3 +251,94 @@ def test_validation_messages(cuda):
         af.ShackHartmannSlopes(4, 5, 32, 32, LAM, DX, DX, Z)
     with pytest.raises(hf.HfError, match="window sides must be in 2..1024"):
         af.ShortTimeFresnel((1, 2048, 2048), (2048, 2048), (2048, 2048), LAM, DX, DX, Z)
+
+
+def test_autofocus_as_nodes(cuda):
+    """ShortTimeFresnelDiffraction -> Mean -> FFTShiftNp -> ShackHartmannSlopes -> (host)
+    ZernikeFromSlopes -> ZernikePhase -> CorrectPhase, driven as the reference's graph wires them
+    (graph_builder.cc:336-451), against the oracle chain."""
+    import torch
+    from holoflow_b200 import nodes as N
+    nb, side, nz = 5, 510, 4
+    s = side // nb
+    planes = aberrated_planes(nz, side, 3.0, seed=8)
+    dev = torch.from_numpy(planes).to(cuda)
+    stfd = {"lambda": LAM, "dx": DX, "dy": DX, "z": Z, "win_h": s, "win_w": s, "stride_y": s, "stride_x": s,
+            "phase_ref": "GLOBAL", "output_magnitude": True}
+    (mag,) = N.run_sync_factory("ShortTimeFresnelDiffraction", stfd, [dev.reshape(1, nz, side, side)])
+    assert tuple(mag.shape) == (1, nz, nb, nb, s, s)
+    (m0,) = N.run_sync_factory("Mean", {"axes": [1], "keepdims": False}, [mag])
+    (m0,) = N.run_sync_factory("FFTShiftNp", {"axes": [-2, -1]}, [m0])
+    assert O.rel_l2(m0.cpu().numpy()[0], SH.subaperture_m0(planes, nb, LAM, DX, Z)) < 1e-5
+    sl = {"lambda": LAM, "dx": DX, "dy": DX, "z": Z, "subaperture_height": s, "subaperture_width": s, "stride_y": s,
+          "stride_x": s, "correlation_roi": {"cx": 0.5, "cy": 0.5, "rx": 0.5, "ry": 0.5, "angle": 0.0}}
+    (slopes,) = N.run_sync_factory("ShackHartmannSlopes", sl, [m0])
+    idx = [4, 5, 6]
+    fit = {"indexes": idx, "lambda": LAM, "dx": DX, "dy": DX, "subaperture_height": s, "subaperture_width": s,
+           "stride_y": s, "stride_x": s}
+    (coeffs,) = N.run_sync_factory("ZernikeFromSlopes", fit, [slopes.cpu()])
+    (dcoeffs,) = N.run_sync_factory("ZernikeFromSlopes", fit, [slopes])
+    assert torch.equal(coeffs, dcoeffs.cpu())  # host and device fits agree bit for bit
+    _, esl, ec, eph, ecor = SH.autofocus(planes.astype(np.complex128), SH.AutofocusConfig(nb, LAM, DX, Z, idx))
+    spp = LAM / (s * DX)
+    assert np.abs(slopes.cpu().numpy()[0] - esl).max() / spp < 2e-3
+    assert np.abs(coeffs.numpy().reshape(-1) - ec).max() < 1e-3 * max(1.0, np.abs(ec).max())
+    zp = {"indexes": idx, "ny": side, "nx": side, "output": "Device"}
+    (phase,) = N.run_sync_factory("ZernikePhase", zp, [dcoeffs.reshape(-1)])
+    (host_phase,) = N.run_sync_factory("ZernikePhase", dict(zp, output="Host"), [coeffs.reshape(-1)])
+    assert np.abs(phase.cpu().numpy() - host_phase.numpy()).max() < 1e-5
+    (cor,) = N.run_sync_factory("CorrectPhase", {}, [dev, phase])
+    assert O.rel_l2(cor.cpu().numpy(), ecor) < 1e-3
+    (w,) = N.run_sync_factory("Wrap2Pi", {}, [phase])
+    assert np.array_equal(w.cpu().numpy(), SH.wrap2pi(phase.cpu().numpy()))
+
+
+def doppler_frames(T, side, k0, a4, seed=9):
+    """float32 frames x_t = Re(A exp(2 pi i k0 t / T)): the band DFT at bin k0 is (T / 2) A, with
+    A = conj(Fresnel lens) IFFT(point scatterers) exp(i a4 Z4), so the Fresnel image of the band
+    is the scatterers seen through a defocus aberration."""
+    rng = np.random.default_rng(seed)
+    lens = O.fresnel_lens(side, side, LAM, Z, DX)
+    y, x = (np.mgrid[0:side, 0:side] - (side - 1) / 2.0) / (side / 2.0)
+    pts = np.zeros((side, side), np.complex128)
+    for _ in range(8):
+        pts[rng.integers(side // 4, 3 * side // 4), rng.integers(side // 4, 3 * side // 4)] = np.exp(
+            2j * math.pi * rng.random()) * (1.0 + rng.random())
+    A = np.conj(lens) * np.fft.ifft2(pts) * np.exp(1j * a4 * SH.zernike_value(4, x, y)) * side * 100.0
+    t = np.arange(T)[:, None, None]
+    return np.real(A[None] * np.exp(2j * math.pi * k0 * t / T)).astype(np.float32)
+
+
+@pytest.mark.parametrize("form,n_iter", [(0, 1), (1, 1), (1, 2)])
+def test_pipeline_with_autofocus(cuda, form, n_iter):
+    """The fused pipeline with autofocus on (graph_builder.cc:139-153): each window's band planes
+    are measured and corrected before the Fresnel lens; moments and coefficients against the
+    oracle, and the correction sharpens the image."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    T, side, k0, a4, nb = 32, 256, 5, 4.0, 5
+    frames = doppler_frames(T, side, k0, a4)
+    ring = torch.from_numpy(frames).to(cuda)
+    base = dict(height=side, width=side, frames=T, hop=T, z_begin=3, z_end=9, input_dtype=hf.HF_F32, lam=LAM,
+                pitch=DX, z=Z, form=form, max_batch=1)
+    af = dict(autofocus_nb_subaps=nb, autofocus_orders=(4, 5, 6), autofocus_n_iter=n_iter)
+    p = pl.Pipeline(pl.PipelineConfig(**base, **af))
+    got = p.run(ring, T, 0, 1).cpu().numpy()[0]
+    assert p.status() == 0
+    coeff = p.autofocus_coefficients(0).cpu().numpy()
+    ocfg = O.PathConfig(side, side, T, T, 3, 9, lam=LAM, pitch=DX, z=Z,
+                        autofocus=dict(nb=nb, orders=[4, 5, 6], n_iter=n_iter))
+    exp = O.reconstruct_window(frames.astype(np.float64), ocfg)
+    _, ecoeff = O.autofocus_planes(O.band_planes(frames.astype(np.float64), ocfg), ocfg)
+    assert np.abs(coeff - ecoeff).max() < 1e-3 * max(1.0, np.abs(ecoeff).max())
+    tol = 1e-4 if form == 0 else 1e-3
+    for m in range(3):
+        assert O.rel_l2(got[m], exp[m]) < tol, m
+    assert abs(coeff[0] - a4) < 0.35 * a4
+    # the corrected image is sharper: more of M0's energy in its brightest pixels
+    plain = pl.Pipeline(pl.PipelineConfig(**base)).run(ring, T, 0, 1).cpu().numpy()[0, 0]
+    def peak_share(img):
+        v = np.sort(img.ravel())[::-1]
+        return v[:64].sum() / v.sum()
+    assert peak_share(got[0]) > 1.2 * peak_share(plain)

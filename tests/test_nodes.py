@@ -40,7 +40,8 @@ def invalid(kind, settings, descs, fragment):
 def test_reference_kinds_are_registered():
     assert set(N.kinds()) == {"FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
                               "Conversion", "Holofile", "FFTShiftNp", "Flatfield", "Filter2D", "PctClip",
-                              "DopplerMoments"}
+                              "DopplerMoments", "ShortTimeFresnelDiffraction", "ShackHartmannSlopes",
+                              "ZernikeFromSlopes", "ZernikePhase", "CorrectPhase", "Wrap2Pi", "ZernikeDefocusZProp"}
 
 
 def test_unknown_kind_and_bad_settings():
@@ -176,3 +177,62 @@ def test_filter2d_infer():
     invalid("Filter2D", f, [desc([64, 64], U16)], p + "input must be complex float32 or real float32")
     invalid("Filter2D", f, [desc([64])], p + "input must be a tensor of rank 2 or higher")
     invalid("Filter2D", f, [desc([64, 64], CF32, device=False)], p + "input must be in device memory")
+
+
+STFD = {"lambda": 852e-9, "dx": 20e-6, "dy": 20e-6, "z": 0.25, "win_h": 102, "win_w": 102, "stride_y": 102,
+        "stride_x": 102, "phase_ref": "GLOBAL"}
+SLOPES = {"lambda": 852e-9, "dx": 20e-6, "dy": 20e-6, "z": 0.25, "subaperture_height": 102, "subaperture_width": 102,
+          "stride_y": 102, "stride_x": 102, "correlation_roi": {"rx": 0.5, "ry": 0.5}}
+FIT = {"indexes": [4, 5, 6], "lambda": 852e-9, "dx": 20e-6, "dy": 20e-6, "subaperture_height": 102,
+       "subaperture_width": 102, "stride_y": 102, "stride_x": 102}
+
+
+def test_autofocus_kinds_infer():
+    """ShortTimeFresnelDiffraction (short_time_fresnel_diffraction.cu:604-649), ShackHartmannSlopes
+    (shack_hartmann_slopes.cu:326-388), ZernikeFromSlopes (zernike_from_slopes.cc:283-323),
+    ZernikePhase (zernike_phase.cu:290-334), CorrectPhase (correct_phase.cu:160-190), Wrap2Pi,
+    ZernikeDefocusZProp (zernike_defocus_z_prop.cc:173-211): output descriptors and messages."""
+    assert out_of("ShortTimeFresnelDiffraction", STFD, [desc([2, 510, 510], CF32)]) == ((2, 5, 5, 102, 102), CF32)
+    mag = dict(STFD, output_magnitude=True, stride_y=51, stride_x=34)
+    assert out_of("ShortTimeFresnelDiffraction", mag, [desc([512, 520], F32)]) == ((9, 13, 102, 102), F32)
+    p = "ShortTimeFresnelDiffractionFactory inference error: "
+    invalid("ShortTimeFresnelDiffraction", dict(STFD, dy=1e-5), [desc([1, 64, 64], CF32)], p + "dx must equal dy")
+    invalid("ShortTimeFresnelDiffraction", STFD, [desc([1, 64, 64], CF32)], p + "window dimensions exceed field size")
+    invalid("ShortTimeFresnelDiffraction", STFD, [desc([1, 512, 512], U16)], p + "input must be CF32 or F32")
+    invalid("ShortTimeFresnelDiffraction", dict(STFD, axes=[0, 1]), [desc([4, 512, 512], CF32)],
+            p + "only trailing axes (-2, -1) are supported")
+
+    assert out_of("ShackHartmannSlopes", SLOPES, [desc([1, 5, 5, 102, 102])]) == ((1, 5, 5, 2), F32)
+    outs = N.infer("ShackHartmannSlopes", dict(SLOPES, output_xcorr_maps=True), [desc([1, 5, 5, 102, 102])])
+    assert [N.shape_of(o) for o in outs] == [(1, 5, 5, 2), (1, 5, 5, 102, 102)]
+    p = "ShackHartmannSlopesFactory inference error: "
+    invalid("ShackHartmannSlopes", SLOPES, [desc([1, 4, 5, 102, 102])],
+            p + "subaperture grid dimensions must be odd for an unambiguous center reference")
+    invalid("ShackHartmannSlopes", SLOPES, [desc([5, 5, 102, 102])], p + "input rank must be 5")
+    invalid("ShackHartmannSlopes", dict(SLOPES, z=-1.0), [desc([1, 5, 5, 102, 102])],
+            p + "propagation distance must be > 0")
+    invalid("ShackHartmannSlopes", dict(SLOPES, correlation_roi={"rx": 0.0}), [desc([1, 5, 5, 102, 102])],
+            p + "correlation ROI radii must be positive")
+
+    assert out_of("ZernikeFromSlopes", FIT, [desc([1, 5, 5, 2], device=False)]) == ((1, 1, 3), F32)
+    p = "ZernikeFromSlopesFactory inference error: "
+    invalid("ZernikeFromSlopes", dict(FIT, indexes=[4, 11]), [desc([1, 5, 5, 2])], p + "only Noll indexes 2..10")
+    invalid("ZernikeFromSlopes", dict(FIT, indexes=[4, 4]), [desc([1, 5, 5, 2])], p + "indexes must be unique")
+    invalid("ZernikeFromSlopes", dict(FIT, ny=2), [desc([1, 5, 5, 2])], p + "only global fitting with ny = nx = 1")
+    invalid("ZernikeFromSlopes", FIT, [desc([1, 5, 5, 3])], p + "last input dimension must contain [dW/dx, dW/dy]")
+
+    zp = {"indexes": [4, 5], "ny": 96, "nx": 130, "output": "Device"}
+    assert out_of("ZernikePhase", zp, [desc([2])]) == ((96, 130), F32)
+    p = "ZernikePhaseFactory inference error: "
+    invalid("ZernikePhase", zp, [desc([2], device=False)], p + "Input coefficients must be in the output memory location")
+    invalid("ZernikePhase", zp, [desc([3])], p + "Input coefficient count must match settings.indexes size")
+
+    (o,) = N.infer("CorrectPhase", {}, [desc([4, 64, 48], CF32), desc([64, 48])])
+    assert (N.shape_of(o), o.dtype) == ((4, 64, 48), CF32)
+    invalid("CorrectPhase", {}, [desc([4, 64, 48], CF32), desc([64, 40])],
+            "CorrectPhaseFactory inference error: phase mask width must match the input")
+    assert out_of("Wrap2Pi", {}, [desc([7, 9])]) == ((7, 9), F32)
+    zd = {"indexes": [4, 5], "lambda": 852e-9, "z_curr": 0.25, "pupil_radius": 5e-3}
+    assert N.infer("ZernikeDefocusZProp", zd, [desc([2])]) == []
+    invalid("ZernikeDefocusZProp", dict(zd, indexes=[5, 6]), [desc([2])],
+            "ZernikeDefocusZPropFactory inference error: indexes must contain Z4 defocus")
