@@ -47,9 +47,10 @@ def parse():
     ap.add_argument("--batch", type=int, default=8, help="windows per step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="config1", choices=["config1", "batched", "serve"],
+    ap.add_argument("--workload", default="config1", choices=["config1", "batched", "serve", "autofocus"],
                     help="config1: the headline line; batched: 16 uneven acquisitions in one graph launch; "
-                         "serve: Poisson-arriving camera streams on the streaming server")
+                         "serve: Poisson-arriving camera streams on the streaming server; autofocus: the "
+                         "Shack-Hartmann pass on one config-1 spectrum and its cost inside the pipeline")
     return ap.parse_args()
 
 
@@ -369,6 +370,142 @@ def run_serve(args, local, form, seed=1004, life=120):
             "windows": int(windows_done), "rounds": rnd, "admission_deferrals": refused, "seconds": round(secs, 3)}
 
 
+AF_NB, AF_ORDERS = 5, (4, 5, 6, 7, 8, 9, 10)
+AF_LAM, AF_DX, AF_Z = 852e-9, 12e-6, 0.25
+
+
+def autofocus_planes(nz, side, device, seed=11):
+    """Band planes of one spectrum seen through an aberration: per plane, seeded point scatterers
+    in the Fresnel image plane, conj(lens) IFFT(points) exp(i (3 Z4 + 1.5 Z5 - Z6)), complex64 on
+    the device."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    k = math.pi / (AF_LAM * AF_Z)
+    c = (torch.arange(side, dtype=torch.float64) - side / 2.0) * AF_DX
+    lens = torch.polar(torch.ones(side, side, dtype=torch.float64), k * (c[None, :] ** 2 + c[:, None] ** 2))
+    u = (torch.arange(side, dtype=torch.float64) - (side - 1) / 2.0) / (side / 2.0)
+    x, y = u[None, :], u[:, None]
+    phi = 3.0 * math.sqrt(3.0) * (2.0 * (x * x + y * y) - 1.0) + 1.5 * 2.0 * math.sqrt(6.0) * x * y \
+        - math.sqrt(6.0) * (x * x - y * y)
+    ab = torch.conj(lens) * torch.polar(torch.ones_like(phi), phi)
+    out = torch.empty((nz, side, side), dtype=torch.complex64, device=device)
+    for i in range(nz):
+        pts = torch.zeros(side, side, dtype=torch.complex128)
+        idx = torch.randint(side // 4, 3 * side // 4, (12, 2), generator=g)
+        pts[idx[:, 0], idx[:, 1]] = torch.polar(1.0 + torch.rand(12, generator=g, dtype=torch.float64),
+                                                2 * math.pi * torch.rand(12, generator=g, dtype=torch.float64))
+        out[i] = (ab * torch.fft.ifft2(pts) * side).to(torch.complex64).to(device)
+    return out
+
+
+def run_autofocus(args, local):
+    """One Shack-Hartmann pass (measure + correct) on one config-1 spectrum, its per-call split and
+    the roofline of its dominant kernel, the oracle on the host beside it, and the pipeline's
+    windows/s with autofocus on and off."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import autofocus as af
+    from holoflow_b200 import pipeline as pl
+    from holoflow_b200 import synth as sy
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nz, side, s = Z1 - Z0, H, H // AF_NB
+    planes = autofocus_planes(nz, side, dev)
+    out = torch.empty_like(planes)
+    op = af.Autofocus(nz, side, side, AF_NB, AF_LAM, AF_DX, AF_Z, indexes=AF_ORDERS)
+    stfd = af.ShortTimeFresnel(planes.shape, (s, s), (s, s), AF_LAM, AF_DX, AF_DX, AF_Z, phase_ref="global",
+                               output="mean_magnitude", fftshift_windows=True)
+    slopes = af.ShackHartmannSlopes(AF_NB, AF_NB, s, s, AF_LAM, AF_DX, AF_DX, AF_Z)
+    m0 = stfd(planes)
+    sl = slopes(m0)
+    phase = torch.zeros((side, side), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / k
+
+    lib = hf.lib()
+    lib.hf_reset_launch_count()
+    with ClockSampler(local) as clk:
+        ms = timed(lambda: op(planes, out=out), args.steps)
+        launches = lib.hf_launch_count() // (args.warmup + args.steps)
+        split = {"short_time_fresnel_mean": timed(lambda: stfd(planes, out=m0), args.steps),
+                 "slopes": timed(lambda: slopes(m0), args.steps),
+                 "correct_phase": timed(lambda: af.correct_phase(planes, phase, out=out), args.steps)}
+    split["zernike_fit_and_phase"] = max(0.0, ms - sum(split.values()))
+    P, Pw = side * side, AF_NB * AF_NB * s * s
+    algo = {"short_time_fresnel_mean": 8 * nz * P + 2 * 8 * nz * Pw + 4 * Pw,
+            "correct_phase": 2 * 8 * nz * P + 4 * P}
+    dom = max(("short_time_fresnel_mean", "correct_phase"), key=lambda k: split[k])
+    peak, peak_kind = peaks()
+    achieved = algo[dom] / (split[dom] / 1000.0) / 1e9
+    roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "algorithmic_bytes_per_launch": algo[dom], "ms_per_launch": round(split[dom], 4),
+            "calls_ms": {k: round(v, 4) for k, v in split.items()}}
+
+    # the pipeline on config-1 windows with the pass on every window (chosen form), and without
+    def pipeline_rate(orders):
+        B = 8
+        cfg = pl.PipelineConfig(height=H, width=W, frames=T, hop=HOP, z_begin=Z0, z_end=Z1, fs=FS, z=AF_Z,
+                                lam=AF_LAM, pitch=AF_DX, clutter_rank=RANK_CLUTTER, max_batch=B,
+                                form=hf.HF_FORM_CHOSEN, autofocus_nb_subaps=AF_NB if orders else 0,
+                                autofocus_orders=orders)
+        gen = sy.DeviceInterferograms(sy.config1_scene(acquisition=0), device=dev)
+        packed = pl.pack12(gen.frames(0, 64).reshape(-1)).view(64, cfg.frame_bytes)
+        ring = torch.cat([packed] * (RING_FRAMES // 64)).reshape(-1).contiguous()
+        pipe = pl.Pipeline(cfg)
+        res = torch.empty((B, *pipe.out_shape), dtype=torch.float32, device=dev)
+        step = [0]
+
+        def run():
+            pipe.run(ring, RING_FRAMES, (step[0] * B * HOP) % RING_FRAMES, B, out=res)
+            step[0] += 1
+        t = timed(run, max(4, args.steps // 2))
+        pipe.close()
+        return B / (t / 1000.0), t
+
+    on, on_ms = pipeline_rate(AF_ORDERS)
+    off, off_ms = pipeline_rate(())
+
+    cpu = None
+    if not args.no_cpu:
+        from oracle import shack as SH
+        host = planes.cpu().numpy()
+        cfg = SH.AutofocusConfig(AF_NB, AF_LAM, AF_DX, AF_Z, list(AF_ORDERS))
+        SH.autofocus(host[:2], cfg)  # warm-up (imports, FFT plans) on a 2-plane sample
+        t0 = time.perf_counter()
+        SH.autofocus(host, cfg)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(1.0 / dt, 4), "unit": "passes/s", "cores": 1, "kind": "port",
+               "sample": f"one full pass over the same {nz} x {side}^2 spectrum (oracle/shack.py, NumPy)"}
+
+    print(json.dumps({
+        "metric": "Shack-Hartmann autofocus passes/s on one spectrum", "value": round(1000.0 / ms, 2),
+        "unit": "passes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded point scatterers behind a defocus + astigmatism aberration)",
+        "config": {"workload": f"config1 spectrum: {nz} x {side}x{side} complex64 band planes, nb_subaps={AF_NB} "
+                               f"({s}x{s} sub-apertures), Noll {list(AF_ORDERS)}, lambda 852 nm, 12 um, z 0.25 m; "
+                               "measure (short-time Fresnel + band mean, slopes, fit, phase) + correct",
+                   "l2": "inputs (1.9 GB of planes per pass) larger than L2"},
+        "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+        "pipeline_config1_chosen": {"autofocus_on_windows_per_s": round(on, 1), "ms_per_8_windows_on": round(on_ms, 3),
+                                    "autofocus_off_windows_per_s": round(off, 1),
+                                    "ms_per_8_windows_off": round(off_ms, 3)},
+        "clocks": clk.summary()}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -378,6 +515,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "batched":
         return run_batched(args, local) if rank == 0 else None
+    if args.workload == "autofocus":
+        return run_autofocus(args, local) if rank == 0 else None
     if args.workload == "serve":
         if rank != 0:
             return None
