@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=8, help="windows per step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--af-nz", type=int, default=Z1 - Z0, help="autofocus workload: band planes of the spectrum")
+    ap.add_argument("--af-no-pipeline", action="store_true", help="autofocus workload: skip the pipeline leg")
     ap.add_argument("--workload", default="config1", choices=["config1", "batched", "serve", "autofocus"],
                     help="config1: the headline line; batched: 16 uneven acquisitions in one graph launch; "
                          "serve: Poisson-arriving camera streams on the streaming server; autofocus: the "
@@ -410,7 +412,7 @@ def run_autofocus(args, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    nz, side, s = Z1 - Z0, H, H // AF_NB
+    nz, side, s = args.af_nz, H, H // AF_NB
     planes = autofocus_planes(nz, side, dev)
     out = torch.empty_like(planes)
     op = af.Autofocus(nz, side, side, AF_NB, AF_LAM, AF_DX, AF_Z, indexes=AF_ORDERS)
@@ -475,8 +477,8 @@ def run_autofocus(args, local):
         pipe.close()
         return B / (t / 1000.0), t
 
-    on, on_ms = pipeline_rate(AF_ORDERS)
-    off, off_ms = pipeline_rate(())
+    on, on_ms = pipeline_rate(AF_ORDERS) if not args.af_no_pipeline else (0.0, 0.0)
+    off, off_ms = pipeline_rate(()) if not args.af_no_pipeline else (0.0, 0.0)
 
     cpu = None
     if not args.no_cpu:

@@ -42,30 +42,62 @@ namespace {
 constexpr int kShkMaxN     = 1024; // longest transform side
 constexpr int kShkStages   = 16;
 constexpr int kShkThreads  = 256;
+constexpr int kRedThreads  = 1024; // one CTA per correlation map for the ROI mean and the peak
+constexpr int kShkMaxRows  = 16;   // rows per CTA of the row pass
+constexpr int kMeanPlanes  = 4;    // planes per transform in the band-mean column pass
 constexpr int kShkMaxModes = 9; // Noll 2..10
 
+// Division by a run-time invariant d as a multiply-high and a shift (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", 1994, round-up variant): with
+// l = ceil(log2 d), m = ceil(2^(31+l) / d) < 2^32 and x < 2^31, x / d = umulhi(x, m) >> (l - 1).
+struct FastDiv {
+  uint32_t d, m;
+  int      s;
+};
+
+FastDiv make_div(uint32_t d) {
+  if (d <= 1)
+    return {1u, 0u, 0};
+  int l = 0;
+  while ((1u << l) < d)
+    ++l;
+  const uint64_t p = 31 + (uint64_t)l;
+  return {d, (uint32_t)(((1ull << p) + d - 1) / d), (int)(p - 32)};
+}
+
+__device__ __forceinline__ int fdiv(int x, const FastDiv &f) {
+  return f.d == 1 ? x : (int)(__umulhi((uint32_t)x, f.m) >> f.s);
+}
+
+struct Stage {
+  int     p, Ns, m, nb; // radix, span of the sub-transforms before the stage, n / (Ns p), n / p
+  FastDiv by_nb, by_Ns, by_p;
+};
+
 struct GPlan {
-  int n, nst;
-  int p[kShkStages];
+  int     n, nst;
+  FastDiv by_n;
+  Stage   st[kShkStages];
 };
 
 bool make_plan(int n, GPlan &pl) {
   if (n < 2 || n > kShkMaxN)
     return false;
-  pl.n = n, pl.nst = 0;
-  int rem = n;
-  for (int p : {4, 2, 3, 5}) {
-    while (rem % p == 0) {
-      pl.p[pl.nst++] = p;
-      rem /= p;
-    }
-  }
-  for (int p = 7; rem > 1; p += 2) {
-    while (rem % p == 0) {
-      pl.p[pl.nst++] = p;
-      rem /= p;
-    }
-  }
+  std::memset(&pl, 0, sizeof(pl));
+  pl.n = n, pl.nst = 0, pl.by_n = make_div((uint32_t)n);
+  int rem = n, Ns = 1;
+  auto push = [&](int p) {
+    Stage &st = pl.st[pl.nst++];
+    st.p = p, st.Ns = Ns, st.m = n / (Ns * p), st.nb = n / p;
+    st.by_nb = make_div((uint32_t)st.nb), st.by_Ns = make_div((uint32_t)Ns), st.by_p = make_div((uint32_t)p);
+    Ns *= p;
+  };
+  for (int p : {4, 2, 3, 5, 7, 11, 13, 17})
+    while (rem % p == 0)
+      push(p), rem /= p;
+  for (int p = 19; rem > 1; p += 2)
+    while (rem % p == 0)
+      push(p), rem /= p;
   return true;
 }
 
@@ -78,6 +110,32 @@ std::vector<float2> twiddle_table(int n) {
   return t;
 }
 
+// A transform length's plan and twiddle table in device memory (the kernels copy both into
+// shared memory).
+struct DevPlan {
+  int     n   = 0;
+  GPlan  *pl  = nullptr;
+  float2 *tw  = nullptr;
+};
+
+void release(DevPlan &d) {
+  cudaFree(d.pl), cudaFree(d.tw);
+  d.pl = nullptr, d.tw = nullptr;
+}
+
+int dev_plan_init(DevPlan &d, int n) {
+  GPlan pl;
+  if (!make_plan(n, pl))
+    return fail(HF_ERR_UNSUPPORTED, "autofocus: transform sides must be in 2..1024");
+  d.n                         = n;
+  const std::vector<float2> t = twiddle_table(n);
+  HF_TRY(cuda_status(cudaMalloc(&d.pl, sizeof(GPlan)), "autofocus: plan"));
+  HF_TRY(cuda_status(cudaMalloc(&d.tw, t.size() * sizeof(float2)), "autofocus: twiddles"));
+  HF_TRY(cuda_status(cudaMemcpy(d.pl, &pl, sizeof(GPlan), cudaMemcpyHostToDevice), "autofocus: plan"));
+  return cuda_status(cudaMemcpy(d.tw, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice),
+                     "autofocus: twiddles");
+}
+
 __device__ __forceinline__ float2 twid(const float2 *tw, int e, bool inv) {
   const float2 w = tw[e];
   return inv ? make_float2(w.x, -w.y) : w;
@@ -87,63 +145,176 @@ __device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
   return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
 }
 
-template <int P> __device__ __forceinline__ void dft_small(float2 (&v)[P], bool inv, const float2 *tw, int n) {
+// P-point DFT in registers.  2 and 4 take the exact butterflies; an odd P takes the symmetric form
+// Y[q] = v0 + sum_r (v_r + v_{P-r}) cos(2 pi q r / P) - i sum_r (v_r - v_{P-r}) sin(2 pi q r / P),
+// r = 1 .. (P-1)/2, with Y[P-q] the same with +i: ((P-1)/2)^2 complex-by-real products for both.
+// cos and sin of 2 pi m / P come from the length-n table at m n / P.
+template <int P> __device__ __forceinline__ void dft_small(float2 (&v)[P], bool inv, const float2 *tw, int step) {
   if constexpr (P == 2) {
     const float2 a = v[0], b = v[1];
     v[0] = cadd(a, b), v[1] = csub(a, b);
   } else if constexpr (P == 4) {
     const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
     const float2 a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
-    // forward: (-i) a3; inverse: (+i) a3
-    const float2 r = inv ? make_float2(-a3.y, a3.x) : make_float2(a3.y, -a3.x);
+    const float2 r = inv ? make_float2(-a3.y, a3.x) : make_float2(a3.y, -a3.x); // (+i or -i) a3
     v[0] = cadd(a0, a2), v[2] = csub(a0, a2);
     v[1] = cadd(a1, r), v[3] = csub(a1, r);
-  } else { // 3, 5: p-term sums with w_p^(q r) = w_n^((q r mod p) n / p)
-    float2 y[P];
-    const int  step = n / P;
+  } else {
+    constexpr int H = (P - 1) / 2;
+    float2        a[H + 1], b[H + 1];
+    float         cs[H + 1], sn[H + 1];
+    float2        y0 = v[0];
 #pragma unroll
-    for (int q = 0; q < P; ++q) {
-      float2 acc = v[0];
+    for (int r = 1; r <= H; ++r) {
+      a[r] = cadd(v[r], v[P - r]), b[r] = csub(v[r], v[P - r]);
+      y0   = cadd(y0, a[r]);
+      const float2 w = tw[r * step]; // (cos, -sin) of 2 pi r / P
+      cs[r] = w.x, sn[r] = -w.y;
+    }
+    float2 out[P];
+    out[0] = y0;
 #pragma unroll
-      for (int r = 1; r < P; ++r)
-        acc = cfma(v[r], twid(tw, ((q * r) % P) * step, inv), acc);
-      y[q] = acc;
+    for (int q = 1; q <= H; ++q) {
+      float2 sc = v[0], ss = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        const int   mm = (q * r) % P;
+        const float c  = mm <= H ? cs[mm] : cs[P - mm];
+        const float sv = mm <= H ? sn[mm] : -sn[P - mm];
+        sc.x = fmaf(a[r].x, c, sc.x), sc.y = fmaf(a[r].y, c, sc.y);
+        ss.x = fmaf(b[r].x, sv, ss.x), ss.y = fmaf(b[r].y, sv, ss.y);
+      }
+      const float2 yq = make_float2(sc.x + ss.y, sc.y - ss.x); // sc - i ss
+      const float2 yp = make_float2(sc.x - ss.y, sc.y + ss.x); // sc + i ss
+      out[q]     = inv ? yp : yq;
+      out[P - q] = inv ? yq : yp;
     }
 #pragma unroll
     for (int q = 0; q < P; ++q)
-      v[q] = y[q];
+      v[q] = out[q];
+  }
+}
+
+// Odd P: the symmetric form of dft_small, with the inputs folded into a_r = v_r + v_(P-r) and
+// b_r = v_r - v_(P-r) as they are loaded (the twiddle of input P - r is w^P conj(w^r)) and each
+// output pair stored as soon as it is formed, so no P-element array stays live.
+template <int P>
+__device__ void stage_bfly_odd(const float2 *x, float2 *y, int pitch, int rows, const Stage &st, const float2 *tw,
+                               int n, bool inv) {
+  constexpr int H  = (P - 1) / 2;
+  const int     nb = st.nb, Ns = st.Ns, total = rows * nb, step = n / P;
+  float         cs[H + 1], sn[H + 1];
+#pragma unroll
+  for (int r = 1; r <= H; ++r) {
+    const float2 w = tw[r * step]; // (cos, -sin) of 2 pi r / P
+    cs[r] = w.x, sn[r] = -w.y;
+  }
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int     row = fdiv(t, st.by_nb), j = t - row * nb;
+    const int     jb = fdiv(j, st.by_Ns), k = j - jb * Ns;
+    const int     e  = st.m * k;
+    const float2 *xr = x + row * pitch;
+    float2       *yr = y + row * pitch;
+    const float2  v0 = xr[j];
+    float2        a[H + 1], b[H + 1];
+    float2        y0 = v0;
+    if (e > 0) {
+      const float2 w1 = twid(tw, e, inv);
+      float2       wr = w1, wh = w1;
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        if (r > 1)
+          wr = cmul(wr, w1);
+        if (r == H)
+          wh = wr;
+        a[r] = cmul(xr[j + r * nb], wr);
+      }
+      const float2 wp = cmul(cmul(wh, wh), w1); // w^P
+      wr              = w1;
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        if (r > 1)
+          wr = cmul(wr, w1);
+        const float2 u = cmul(xr[j + (P - r) * nb], cmul(wp, make_float2(wr.x, -wr.y)));
+        b[r]           = csub(a[r], u);
+        a[r]           = cadd(a[r], u);
+        y0             = cadd(y0, a[r]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        const float2 vr = xr[j + r * nb], vp = xr[j + (P - r) * nb];
+        a[r] = cadd(vr, vp), b[r] = csub(vr, vp);
+        y0   = cadd(y0, a[r]);
+      }
+    }
+    const int base = jb * Ns * P + k;
+    yr[base]       = y0;
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      float2 sc = v0, ss = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        const int   mm = (q * r) % P;
+        const float c  = mm <= H ? cs[mm] : cs[P - mm];
+        const float sv = mm <= H ? sn[mm] : -sn[P - mm];
+        sc.x = fmaf(a[r].x, c, sc.x), sc.y = fmaf(a[r].y, c, sc.y);
+        ss.x = fmaf(b[r].x, sv, ss.x), ss.y = fmaf(b[r].y, sv, ss.y);
+      }
+      const float2 yq = make_float2(sc.x + ss.y, sc.y - ss.x); // sc - i ss
+      const float2 yp = make_float2(sc.x - ss.y, sc.y + ss.x); // sc + i ss
+      yr[base + q * Ns]       = inv ? yp : yq;
+      yr[base + (P - q) * Ns] = inv ? yq : yp;
+    }
   }
 }
 
 template <int P>
-__device__ void stage_bfly(const float2 *x, float2 *y, int pitch, int rows, int n, int Ns, const float2 *tw, bool inv) {
-  const int nb = n / P, m = n / (Ns * P);
-  for (int t = threadIdx.x; t < rows * nb; t += blockDim.x) {
-    const int     row = t / nb, j = t - row * nb, k = j % Ns;
-    const float2 *xr  = x + row * pitch;
-    float2       *yr  = y + row * pitch;
+__device__ void stage_bfly(const float2 *x, float2 *y, int pitch, int rows, const Stage &st, const float2 *tw, int n,
+                           bool inv) {
+  if constexpr (P % 2 == 1) {
+    stage_bfly_odd<P>(x, y, pitch, rows, st, tw, n, inv);
+    return;
+  }
+  const int nb = st.nb, Ns = st.Ns, total = rows * nb, step = n / P;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int     row = fdiv(t, st.by_nb), j = t - row * nb;
+    const int     jb = fdiv(j, st.by_Ns), k = j - jb * Ns;
+    const int     e  = st.m * k; // twiddle of input r: w_n^(r m k) = (w_n^(m k))^r
+    const float2 *xr = x + row * pitch;
+    float2       *yr = y + row * pitch;
     float2        v[P];
 #pragma unroll
-    for (int r = 0; r < P; ++r) {
+    for (int r = 0; r < P; ++r)
       v[r] = xr[j + r * nb];
-      if (r > 0)
-        v[r] = cmul(v[r], twid(tw, r * m * k, inv)); // r m k < m Ns p = n
+    if (e > 0) {
+      const float2 w1 = twid(tw, e, inv);
+      float2       wr = w1;
+#pragma unroll
+      for (int r = 1; r < P; ++r) {
+        v[r] = cmul(v[r], wr);
+        if (r + 1 < P)
+          wr = cmul(wr, w1);
+      }
     }
-    dft_small<P>(v, inv, tw, n);
-    const int base = (j / Ns) * Ns * P + k;
+    dft_small<P>(v, inv, tw, step);
+    const int base = jb * Ns * P + k;
 #pragma unroll
     for (int q = 0; q < P; ++q)
       yr[base + q * Ns] = v[q];
   }
 }
 
-__device__ void stage_generic(const float2 *x, float2 *y, int pitch, int rows, int n, int Ns, int p, const float2 *tw,
-                              bool inv) {
-  const int nb = n / p, m = n / (Ns * p);
+// Any radix: one p-term sum per output, the exponent stepped by s = m (k + q Ns) modulo n.
+__device__ void stage_generic(const float2 *x, float2 *y, int pitch, int rows, const Stage &st, const FastDiv &by_n,
+                              const float2 *tw, int n, bool inv) {
+  const int p = st.p, nb = st.nb, Ns = st.Ns;
   for (int t = threadIdx.x; t < rows * n; t += blockDim.x) {
-    const int     row = t / n, o = t - row * n;
-    const int     k = o % Ns, q = (o / Ns) % p, j = (o / (Ns * p)) * Ns + k;
-    const int     s  = m * (k + q * Ns); // < n
+    const int     row = fdiv(t, by_n), o = t - row * n;
+    const int     on = fdiv(o, st.by_Ns), k = o - on * Ns;
+    const int     jb = fdiv(on, st.by_p), q = on - jb * p;
+    const int     j  = jb * Ns + k;
+    const int     s  = st.m * (k + q * Ns); // < n
     const float2 *xr = x + row * pitch;
     float2        acc = make_float2(0.f, 0.f);
     int           e   = 0;
@@ -157,23 +328,25 @@ __device__ void stage_generic(const float2 *x, float2 *y, int pitch, int rows, i
   }
 }
 
-// Transforms `rows` rows of a (pitch `pitch`) in place of a/b; returns the buffer holding the result.
-// Every thread of the CTA calls it; the rows must be in `a` and visible (synchronised) on entry.
+// Transforms `rows` rows of `a` (pitch `pitch`), ping-ponging with `b`; returns the buffer that
+// holds the result.  Every thread of the CTA calls it; the rows must be in `a` and visible.
 __device__ float2 *fft_rows_smem(float2 *a, float2 *b, int pitch, int rows, const GPlan &pl, const float2 *tw, bool inv) {
-  int Ns = 1;
   for (int s = 0; s < pl.nst; ++s) {
-    const int p = pl.p[s];
-    switch (p) {
-    case 2: stage_bfly<2>(a, b, pitch, rows, pl.n, Ns, tw, inv); break;
-    case 3: stage_bfly<3>(a, b, pitch, rows, pl.n, Ns, tw, inv); break;
-    case 4: stage_bfly<4>(a, b, pitch, rows, pl.n, Ns, tw, inv); break;
-    case 5: stage_bfly<5>(a, b, pitch, rows, pl.n, Ns, tw, inv); break;
-    default: stage_generic(a, b, pitch, rows, pl.n, Ns, p, tw, inv); break;
+    const Stage &st = pl.st[s];
+    switch (st.p) {
+    case 2: stage_bfly<2>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 3: stage_bfly<3>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 4: stage_bfly<4>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 5: stage_bfly<5>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 7: stage_bfly<7>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 11: stage_bfly<11>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 13: stage_bfly<13>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 17: stage_bfly<17>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    default: stage_generic(a, b, pitch, rows, st, pl.by_n, tw, pl.n, inv); break;
     }
     __syncthreads();
     float2 *t = a;
     a = b, b = t;
-    Ns *= p;
   }
   return a;
 }
@@ -195,7 +368,8 @@ __device__ __forceinline__ float roi_sq_distance(int x, int y, int w, int h, con
 }
 
 struct RowArgs {
-  GPlan         pl;       // transform along the row (length n)
+  const GPlan  *pl;       // device copy of the transform plan along the row
+  int           n;        // row length
   const float2 *tw;       // [n]
   int           R;        // rows per CTA
   int64_t       n_rows;   // rows in all
@@ -214,18 +388,22 @@ struct RowArgs {
   int           ref_img;
 };
 
-template <int MODE> __global__ void __launch_bounds__(kShkThreads) shk_rows_kernel(RowArgs a) {
+template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_rows_kernel(RowArgs a) {
   extern __shared__ __align__(16) float2 sm[];
-  const int n  = a.pl.n;
-  float2   *tw = sm, *b0 = sm + n, *b1 = b0 + (size_t)a.R * n;
+  __shared__ GPlan spl;
+  const int        n  = a.n;
+  float2          *tw = sm, *b0 = sm + n, *b1 = b0 + (size_t)a.R * n;
   for (int e = threadIdx.x; e < n; e += blockDim.x)
     tw[e] = a.tw[e];
+  for (int i = threadIdx.x; i < (int)(sizeof(GPlan) / 4); i += blockDim.x)
+    reinterpret_cast<int *>(&spl)[i] = reinterpret_cast<const int *>(a.pl)[i];
   const int64_t row0 = (int64_t)blockIdx.x * a.R;
   const int     rows = (int)min((int64_t)a.R, a.n_rows - row0);
-  for (int t = threadIdx.x; t < rows * n; t += blockDim.x) {
-    const int     r = t / n, i = t - r * n;
+  // per-row decode once (64-bit divisions), then per element only the row / column split
+  __shared__ int64_t s_off[kShkMaxRows], s_aux[kShkMaxRows];
+  __shared__ int     s_y[kShkMaxRows];
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
     const int64_t row = row0 + r;
-    float2        v;
     if constexpr (MODE == ROW_STFD) {
       int64_t   rem = row;
       const int j   = (int)(rem % a.win_h);
@@ -234,30 +412,64 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads) shk_rows_kern
       rem /= a.nwx;
       const int     gy = (int)(rem % a.nwy);
       const int64_t pl = rem / a.nwy;
-      const int     fy = gy * a.stride_y + j, fx = gx * a.stride_x + i;
-      const int64_t src = (pl * a.H + fy) * (int64_t)a.W + fx;
-      v = a.real_in ? make_float2(static_cast<const float *>(a.field)[src], 0.f) : static_cast<const float2 *>(a.field)[src];
-      v = cmul(v, a.global_lens ? a.lens[(int64_t)fy * a.W + fx] : a.lens[(int64_t)j * n + i]);
-    } else if constexpr (MODE == ROW_XPACK) {
+      const int     fy = gy * a.stride_y + j, fx = gx * a.stride_x;
+      s_off[r] = (pl * a.H + fy) * (int64_t)a.W + fx;                                  // field row start
+      s_aux[r] = a.global_lens ? (int64_t)fy * a.W + fx : (int64_t)j * n;              // lens row start
+    } else {
       const int64_t im = row / a.h;
-      const int     y  = (int)(row - im * a.h);
-      const float   d  = roi_sq_distance(i, y, n, a.h, a.roi);
-      const float   x  = a.img[row * n + i];
-      // (v - mean) * 0.5 (1 + cos(pi sqrt(d))) inside the ellipse, 0 outside
-      v = make_float2(d <= 1.0f ? (x - a.means[im]) * (0.5f * (1.0f + cospif(sqrtf(d)))) : 0.f, 0.f);
-    } else { // ROW_CROSS: unit-magnitude cross power against the reference image's spectrum
-      const int64_t im  = row / a.h;
-      const int     y   = (int)(row - im * a.h);
-      const float2  mv  = a.spec[row * n + i];
-      const float2  rf  = a.spec[((int64_t)a.ref_img * a.h + y) * n + i];
-      const float2  p   = make_float2(mv.x * rf.x + mv.y * rf.y, mv.y * rf.x - mv.x * rf.y);
-      const float   mag = sqrtf(p.x * p.x + p.y * p.y);
-      v                 = mag <= 1e-12f ? make_float2(0.f, 0.f) : make_float2(p.x / mag, p.y / mag);
+      s_y[r]   = (int)(row - im * a.h);
+      s_off[r] = im;
+      s_aux[r] = ((int64_t)a.ref_img * a.h + s_y[r]) * n; // ROW_CROSS: the reference's row
     }
-    b0[t] = v;
   }
   __syncthreads();
-  const float2 *res = fft_rows_smem(b0, b1, n, rows, a.pl, tw, a.inv);
+  // U independent global loads in flight per thread before any is used
+  constexpr int U = 8;
+  for (int t0 = threadIdx.x; t0 < rows * n; t0 += U * blockDim.x) {
+    float2 ld[U], aux[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= rows * n)
+        break;
+      const int     r = fdiv(t, spl.by_n), i = t - r * n;
+      const int64_t row = row0 + r;
+      if constexpr (MODE == ROW_STFD) {
+        const int64_t src = s_off[r] + i;
+        ld[u]  = a.real_in ? make_float2(static_cast<const float *>(a.field)[src], 0.f)
+                           : static_cast<const float2 *>(a.field)[src];
+        aux[u] = a.lens[s_aux[r] + i];
+      } else if constexpr (MODE == ROW_XPACK) {
+        ld[u] = make_float2(a.img[row * n + i], 0.f);
+      } else {
+        ld[u]  = a.spec[row * n + i];
+        aux[u] = a.spec[s_aux[r] + i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= rows * n)
+        break;
+      float2 v;
+      if constexpr (MODE == ROW_STFD) {
+        v = cmul(ld[u], aux[u]);
+      } else if constexpr (MODE == ROW_XPACK) {
+        const int   r = fdiv(t, spl.by_n), i = t - r * n;
+        const float d = roi_sq_distance(i, s_y[r], n, a.h, a.roi);
+        // (v - mean) * 0.5 (1 + cos(pi sqrt(d))) inside the ellipse, 0 outside
+        v = make_float2(d <= 1.0f ? (ld[u].x - a.means[s_off[r]]) * (0.5f * (1.0f + cospif(sqrtf(d)))) : 0.f, 0.f);
+      } else { // ROW_CROSS: unit-magnitude cross power against the reference image's spectrum
+        const float2 mv = ld[u], rf = aux[u];
+        const float2 p   = make_float2(mv.x * rf.x + mv.y * rf.y, mv.y * rf.x - mv.x * rf.y);
+        const float  mag = sqrtf(p.x * p.x + p.y * p.y);
+        v                = mag <= 1e-12f ? make_float2(0.f, 0.f) : make_float2(p.x / mag, p.y / mag);
+      }
+      b0[t] = v;
+    }
+  }
+  __syncthreads();
+  const float2 *res = fft_rows_smem(b0, b1, n, rows, spl, tw, a.inv);
   for (int t = threadIdx.x; t < rows * n; t += blockDim.x)
     a.out[row0 * n + t] = res[t];
 }
@@ -268,7 +480,8 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads) shk_rows_kern
 enum ColMode { COL_COMPLEX = 0, COL_MAG = 1, COL_MEAN_MAG = 2, COL_REAL = 3 };
 
 struct ColArgs {
-  GPlan         pl; // transform along the column (length h)
+  const GPlan  *pl; // device copy of the transform plan along the column
+  int           h;  // column length
   const float2 *tw; // [h]
   int           C, pitch, nstrip, w;
   bool          inv;
@@ -280,34 +493,59 @@ struct ColArgs {
   int64_t       nwin;
   int           shift;   // COL_MEAN_MAG: fftshift of every image on store
   float         scale;   // COL_REAL
+  FastDiv       by_hc;   // h C (plane index of a strip element)
 };
 
-template <int MODE> __global__ void __launch_bounds__(kShkThreads) shk_cols_kernel(ColArgs a) {
+template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_cols_kernel(ColArgs a) {
   extern __shared__ __align__(16) float2 sm[];
-  const int h = a.pl.n, C = a.C, P = a.pitch;
-  float2   *tw = sm, *b0 = sm + h, *b1 = b0 + (size_t)C * P;
-  float    *acc = reinterpret_cast<float *>(b1 + (size_t)C * P); // COL_MEAN_MAG: [h * C]
+  __shared__ GPlan spl;
+  const int        h = a.h, C = a.C, P = a.pitch;
+  constexpr int    GB = MODE == COL_MEAN_MAG ? kMeanPlanes : 1; // planes held per buffer
+  float2          *tw = sm, *b0 = sm + h, *b1 = b0 + (size_t)GB * C * P;
+  float           *acc = reinterpret_cast<float *>(b1 + (size_t)GB * C * P); // COL_MEAN_MAG: [h * C]
   for (int e = threadIdx.x; e < h; e += blockDim.x)
     tw[e] = a.tw[e];
+  for (int i = threadIdx.x; i < (int)(sizeof(GPlan) / 4); i += blockDim.x)
+    reinterpret_cast<int *>(&spl)[i] = reinterpret_cast<const int *>(a.pl)[i];
   const int     strip = (int)(blockIdx.x % a.nstrip);
   const int64_t img   = blockIdx.x / a.nstrip;
   const int     x0 = strip * C, cw = min(C, a.w - x0);
   const int     planes = MODE == COL_MEAN_MAG ? a.planes : 1;
+  const int     lc     = 31 - __clz(C); // C is a power of two
   if constexpr (MODE == COL_MEAN_MAG)
     for (int t = threadIdx.x; t < h * C; t += blockDim.x)
       acc[t] = 0.f;
-  for (int pl = 0; pl < planes; ++pl) {
-    const int64_t src = MODE == COL_MEAN_MAG ? (int64_t)pl * a.nwin + img : img;
-    const float2 *in  = a.in + src * h * (int64_t)a.w;
-    __syncthreads(); // the previous plane's reads of b0/b1 are done
-    for (int t = threadIdx.x; t < h * C; t += blockDim.x) {
-      const int y = t / C, c = t - y * C;
-      b0[c * P + y] = c < cw ? in[(int64_t)y * a.w + x0 + c] : make_float2(0.f, 0.f);
+  // COL_MEAN_MAG transforms G = 4 planes per call (more work between barriers, narrower strips
+  // and so more CTAs); the strip of plane g sits at rows [g C, g C + C) of the buffers
+  constexpr int G = MODE == COL_MEAN_MAG ? kMeanPlanes : 1;
+  for (int pl = 0; pl < planes; pl += G) {
+    const int ng = min(G, planes - pl);
+    __syncthreads(); // the previous planes' reads of b0/b1 are done
+    constexpr int U = MODE == COL_MEAN_MAG ? 4 : 8; // independent loads in flight per thread
+    for (int t0 = threadIdx.x; t0 < ng * h * C; t0 += U * blockDim.x) {
+      float2 ld[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t >= ng * h * C)
+          break;
+        const int     g = G > 1 ? fdiv(t, a.by_hc) : 0, r = t - g * h * C, y = r >> lc, c = r & (C - 1);
+        const int64_t src = MODE == COL_MEAN_MAG ? (int64_t)(pl + g) * a.nwin + img : img;
+        ld[u] = c < cw ? a.in[(src * h + y) * (int64_t)a.w + x0 + c] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t >= ng * h * C)
+          break;
+        const int g = G > 1 ? fdiv(t, a.by_hc) : 0, r = t - g * h * C, y = r >> lc, c = r & (C - 1);
+        b0[(g * C + c) * P + y] = ld[u];
+      }
     }
     __syncthreads();
-    const float2 *res = fft_rows_smem(b0, b1, P, C, a.pl, tw, a.inv);
+    const float2 *res = fft_rows_smem(b0, b1, P, ng * C, spl, tw, a.inv);
     for (int t = threadIdx.x; t < h * C; t += blockDim.x) {
-      const int y = t / C, c = t - y * C;
+      const int y = t >> lc, c = t & (C - 1);
       if (c >= cw)
         continue;
       const float2  v = res[c * P + y];
@@ -316,16 +554,23 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads) shk_cols_kern
         a.outc[o] = a.post ? cmul(v, a.post[(int64_t)y * a.w + x0 + c]) : v;
       else if constexpr (MODE == COL_MAG)
         a.outf[o] = sqrtf(v.x * v.x + v.y * v.y);
-      else if constexpr (MODE == COL_MEAN_MAG)
-        acc[t] += sqrtf(v.x * v.x + v.y * v.y); // band order, float32
-      else
+      else if constexpr (MODE == COL_MEAN_MAG) {
+        float s = acc[t] + sqrtf(v.x * v.x + v.y * v.y); // band order, float32
+#pragma unroll
+        for (int g = 1; g < G; ++g)
+          if (g < ng) {
+            const float2 u = res[(g * C + c) * P + y];
+            s += sqrtf(u.x * u.x + u.y * u.y);
+          }
+        acc[t] = s;
+      } else
         a.outf[o] = v.x * a.scale;
     }
   }
   if constexpr (MODE == COL_MEAN_MAG) {
     const float nz = (float)a.planes;
     for (int t = threadIdx.x; t < h * C; t += blockDim.x) {
-      const int y = t / C, c = t - y * C;
+      const int y = t >> lc, c = t & (C - 1);
       if (c >= cw)
         continue;
       const int yy = a.shift ? (y + h / 2) % h : y;
@@ -336,19 +581,20 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads) shk_cols_kern
 }
 
 size_t rows_smem(int n, int R) { return (size_t)n * sizeof(float2) * (1 + 2 * (size_t)R); }
-int    rows_per_cta(int n) { return std::max(1, std::min(16, 4096 / n)); }
+int    rows_per_cta(int n) { return std::max(1, std::min(kShkMaxRows, 4096 / n)); }
 int    col_strip(int h, bool mean) {
   const int c = h <= 256 ? 16 : (h <= 512 ? 8 : 4);
-  return mean ? std::min(c, 8) : c;
+  return mean ? std::max(1, c / kMeanPlanes) : c; // the mean pass holds kMeanPlanes planes' strips
 }
 size_t cols_smem(int h, int C, bool mean) {
   const int P = h | 1; // odd pitch: the transposed loads spread over the banks
-  return (size_t)h * sizeof(float2) + 2 * (size_t)C * P * sizeof(float2) + (mean ? (size_t)h * C * sizeof(float) : 0);
+  const int G = mean ? kMeanPlanes : 1;
+  return (size_t)h * sizeof(float2) + 2 * (size_t)G * C * P * sizeof(float2) + (mean ? (size_t)h * C * sizeof(float) : 0);
 }
 
 template <int MODE> int launch_rows(RowArgs a, cudaStream_t s) {
-  a.R             = rows_per_cta(a.pl.n);
-  const size_t sm = rows_smem(a.pl.n, a.R);
+  a.R             = rows_per_cta(a.n);
+  const size_t sm = rows_smem(a.n, a.R);
   HF_CUDA(cudaFuncSetAttribute(shk_rows_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int64_t grid = (a.n_rows + a.R - 1) / a.R;
   if (grid > INT_MAX)
@@ -359,10 +605,11 @@ template <int MODE> int launch_rows(RowArgs a, cudaStream_t s) {
 }
 
 template <int MODE> int launch_cols(ColArgs a, int64_t images, cudaStream_t s) {
-  a.C             = col_strip(a.pl.n, MODE == COL_MEAN_MAG);
-  a.pitch         = a.pl.n | 1;
+  a.C             = col_strip(a.h, MODE == COL_MEAN_MAG);
+  a.pitch         = a.h | 1;
   a.nstrip        = (a.w + a.C - 1) / a.C;
-  const size_t sm = cols_smem(a.pl.n, a.C, MODE == COL_MEAN_MAG);
+  a.by_hc         = make_div((uint32_t)(a.h * a.C));
+  const size_t sm = cols_smem(a.h, a.C, MODE == COL_MEAN_MAG);
   HF_CUDA(cudaFuncSetAttribute(shk_cols_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int64_t grid = images * a.nstrip;
   if (grid > INT_MAX)
@@ -412,7 +659,7 @@ int grid_1d(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n +
 // ------------------------------------------------------------------------------------------------
 // compute_means_kernel (cross_correlation2.cu:352-402): mean of the pixels inside the ROI, 0 when
 // none is.
-__global__ void __launch_bounds__(kShkThreads) shk_roi_mean_kernel(const float *img, float *means, int h, int w, Roi roi) {
+__global__ void __launch_bounds__(kRedThreads) shk_roi_mean_kernel(const float *img, float *means, int h, int w, Roi roi) {
   const float *im = img + (int64_t)blockIdx.x * h * w;
   float        sum = 0.f;
   int          cnt = 0;
@@ -423,8 +670,8 @@ __global__ void __launch_bounds__(kShkThreads) shk_roi_mean_kernel(const float *
       ++cnt;
     }
   }
-  __shared__ float ss[kShkThreads];
-  __shared__ int   sc[kShkThreads];
+  __shared__ float ss[kRedThreads];
+  __shared__ int   sc[kRedThreads];
   ss[threadIdx.x] = sum, sc[threadIdx.x] = cnt;
   __syncthreads();
   for (int st = blockDim.x / 2; st > 0; st >>= 1) {
@@ -446,7 +693,7 @@ __device__ __forceinline__ float signed_coord(int p, int n) { return p < (n + 1)
 // recover_phase_correlation_peaks (shack_hartmann_slopes.cu:124-158): the first maximum in
 // row-major order (a strict > scan), found here by a block reduction that keeps the smaller
 // index among equal values; then the parabolic refinement on the circular neighbours.
-__global__ void __launch_bounds__(kShkThreads) shk_peak_kernel(const float *maps, float2 *shifts, int h, int w) {
+__global__ void __launch_bounds__(kRedThreads) shk_peak_kernel(const float *maps, float2 *shifts, int h, int w) {
   const float *m    = maps + (int64_t)blockIdx.x * h * w;
   float        best = -FLT_MAX;
   int          bi   = INT_MAX;
@@ -455,8 +702,8 @@ __global__ void __launch_bounds__(kShkThreads) shk_peak_kernel(const float *maps
     if (v > best)
       best = v, bi = i;
   }
-  __shared__ float sv[kShkThreads];
-  __shared__ int   si[kShkThreads];
+  __shared__ float sv[kRedThreads];
+  __shared__ int   si[kRedThreads];
   sv[threadIdx.x] = best, si[threadIdx.x] = bi;
   __syncthreads();
   for (int st = blockDim.x / 2; st > 0; st >>= 1) {
@@ -722,25 +969,19 @@ struct hf_stfd {
   int64_t planes;
   int     H, W, real_in, win_h, win_w, sy, sx, nwy, nwx, global, output, skip_phase_shift, shift;
   float   lambda, dx, dy, z;
-  GPlan   pw, ph;
-  float2 *tw_w = nullptr, *tw_h = nullptr, *lens = nullptr, *wlens = nullptr, *scratch = nullptr;
+  DevPlan pw, ph;
+  float2 *lens = nullptr, *wlens = nullptr, *scratch = nullptr;
 };
 
 namespace {
 void release(hf_stfd *f) {
   if (!f)
     return;
-  cudaFree(f->tw_w), cudaFree(f->tw_h), cudaFree(f->lens), cudaFree(f->wlens), cudaFree(f->scratch);
+  release(f->pw), release(f->ph);
+  cudaFree(f->lens), cudaFree(f->wlens), cudaFree(f->scratch);
   delete f;
 }
 
-int upload_twiddles(int n, float2 **dst, cudaStream_t s) {
-  const std::vector<float2> t = twiddle_table(n);
-  HF_TRY(cuda_status(cudaMalloc(dst, t.size() * sizeof(float2)), "autofocus: twiddles"));
-  HF_TRY(cuda_status(cudaMemcpyAsync(*dst, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice, s),
-                     "autofocus: twiddles"));
-  return cuda_status(cudaStreamSynchronize(s), "autofocus: twiddles"); // the host table goes out of scope
-}
 
 int stfd_lenses(hf_stfd *f, cudaStream_t s) {
   // input_lens_geometry (short_time_fresnel_diffraction.cu:342-369): the largest side of the frame
@@ -785,7 +1026,7 @@ int hf_stfd_create(int64_t planes, int height, int width, int real_input, int wi
   auto *f = new (std::nothrow) hf_stfd();
   if (!f)
     return fail(HF_ERR_NOMEM, "ShortTimeFresnelDiffraction: host allocation failed");
-  if (!make_plan(win_w, f->pw) || !make_plan(win_h, f->ph)) {
+  if (win_w > kShkMaxN || win_h > kShkMaxN) {
     delete f;
     return fail(HF_ERR_UNSUPPORTED, "ShortTimeFresnelDiffraction: window sides must be in 2..1024");
   }
@@ -797,9 +1038,9 @@ int hf_stfd_create(int64_t planes, int height, int width, int real_input, int wi
   f->lambda = lambda, f->dx = dx, f->dy = dy, f->z = z;
   const size_t lens_px = f->global ? (size_t)height * width : (size_t)win_h * win_w;
   const size_t out_px  = (size_t)planes * f->nwy * f->nwx * win_h * win_w;
-  int          rc      = upload_twiddles(win_w, &f->tw_w, s);
+  int          rc      = dev_plan_init(f->pw, win_w);
   if (rc == HF_OK)
-    rc = upload_twiddles(win_h, &f->tw_h, s);
+    rc = dev_plan_init(f->ph, win_h);
   if (rc == HF_OK)
     rc = cuda_status(cudaMalloc(&f->lens, lens_px * sizeof(float2)), "ShortTimeFresnelDiffraction: lens");
   if (rc == HF_OK && output == HF_STFD_COMPLEX && !f->skip_phase_shift)
@@ -837,12 +1078,12 @@ int hf_stfd_exec(hf_stfd *f, const void *in, void *out, hf_stream_t s) {
   const int64_t nwin = (int64_t)f->nwy * f->nwx;
   float2       *rows = f->output == HF_STFD_COMPLEX ? static_cast<float2 *>(out) : f->scratch;
   RowArgs       ra{};
-  ra.pl = f->pw, ra.tw = f->tw_w, ra.n_rows = f->planes * nwin * f->win_h, ra.inv = false, ra.out = rows;
+  ra.pl = f->pw.pl, ra.n = f->pw.n, ra.tw = f->pw.tw, ra.n_rows = f->planes * nwin * f->win_h, ra.inv = false, ra.out = rows;
   ra.field = in, ra.real_in = f->real_in, ra.H = f->H, ra.W = f->W, ra.win_h = f->win_h, ra.nwx = f->nwx;
   ra.nwy = f->nwy, ra.stride_y = f->sy, ra.stride_x = f->sx, ra.global_lens = f->global, ra.lens = f->lens;
   HF_TRY(launch_rows<ROW_STFD>(ra, s));
   ColArgs ca{};
-  ca.pl = f->ph, ca.tw = f->tw_h, ca.w = f->win_w, ca.inv = false, ca.in = rows;
+  ca.pl = f->ph.pl, ca.h = f->ph.n, ca.tw = f->ph.tw, ca.w = f->win_w, ca.inv = false, ca.in = rows;
   switch (f->output) {
   case HF_STFD_COMPLEX:
     ca.outc = static_cast<float2 *>(out), ca.post = f->wlens;
@@ -871,8 +1112,8 @@ struct hf_shslopes {
   int      sy, sx, h, w, center, count;
   float    sppx, sppy;
   Roi      roi;
-  GPlan    pw, ph;
-  float2  *tw_w = nullptr, *tw_h = nullptr, *spec = nullptr, *cross = nullptr, *shifts = nullptr;
+  DevPlan  pw, ph;
+  float2  *spec = nullptr, *cross = nullptr, *shifts = nullptr;
   float   *means = nullptr, *maps = nullptr;
   uint8_t *active = nullptr;
   std::vector<uint8_t> active_host;
@@ -882,7 +1123,8 @@ namespace {
 void release(hf_shslopes *p) {
   if (!p)
     return;
-  cudaFree(p->tw_w), cudaFree(p->tw_h), cudaFree(p->spec), cudaFree(p->cross), cudaFree(p->shifts);
+  release(p->pw), release(p->ph);
+  cudaFree(p->spec), cudaFree(p->cross), cudaFree(p->shifts);
   cudaFree(p->means), cudaFree(p->maps), cudaFree(p->active);
   delete p;
 }
@@ -917,7 +1159,7 @@ int hf_shslopes_create(int sy, int sx, int height, int width, int sub_h, int sub
   auto *p = new (std::nothrow) hf_shslopes();
   if (!p)
     return fail(HF_ERR_NOMEM, "ShackHartmannSlopes: host allocation failed");
-  if (!make_plan(width, p->pw) || !make_plan(height, p->ph)) {
+  if (width > kShkMaxN || height > kShkMaxN) {
     delete p;
     return fail(HF_ERR_UNSUPPORTED, "ShackHartmannSlopes: subaperture sides must be in 2..1024");
   }
@@ -930,9 +1172,9 @@ int hf_shslopes_create(int sy, int sx, int height, int width, int sub_h, int sub
   for (const Sample &g : geo)
     p->active_host.push_back(g.active ? 1 : 0);
   const size_t px = (size_t)p->count * height * width;
-  int          rc = upload_twiddles(width, &p->tw_w, s);
+  int          rc = dev_plan_init(p->pw, width);
   if (rc == HF_OK)
-    rc = upload_twiddles(height, &p->tw_h, s);
+    rc = dev_plan_init(p->ph, height);
   if (rc == HF_OK)
     rc = cuda_status(cudaMalloc(&p->spec, px * sizeof(float2)), "ShackHartmannSlopes: spectra");
   if (rc == HF_OK)
@@ -968,27 +1210,27 @@ int hf_shslopes_exec(hf_shslopes *p, const float *images, float *slopes, float *
   HF_CHECK_ARG(p != nullptr && images != nullptr && slopes != nullptr, "ShackHartmannSlopes: null argument");
   const int64_t rows = (int64_t)p->count * p->h;
   float        *mo   = maps ? maps : p->maps;
-  shk_roi_mean_kernel<<<p->count, kShkThreads, 0, s>>>(images, p->means, p->h, p->w, p->roi);
+  shk_roi_mean_kernel<<<p->count, kRedThreads, 0, s>>>(images, p->means, p->h, p->w, p->roi);
   note_launch();
   HF_TRY(launch_status("shk_roi_mean_kernel"));
   // forward transform of the prepared images: rows (mean removal + taper fused), then columns
   RowArgs ra{};
-  ra.pl = p->pw, ra.tw = p->tw_w, ra.n_rows = rows, ra.inv = false, ra.out = p->spec;
+  ra.pl = p->pw.pl, ra.n = p->pw.n, ra.tw = p->pw.tw, ra.n_rows = rows, ra.inv = false, ra.out = p->spec;
   ra.img = images, ra.means = p->means, ra.roi = p->roi, ra.h = p->h;
   HF_TRY(launch_rows<ROW_XPACK>(ra, s));
   ColArgs ca{};
-  ca.pl = p->ph, ca.tw = p->tw_h, ca.w = p->w, ca.inv = false, ca.in = p->spec, ca.outc = p->spec;
+  ca.pl = p->ph.pl, ca.h = p->ph.n, ca.tw = p->ph.tw, ca.w = p->w, ca.inv = false, ca.in = p->spec, ca.outc = p->spec;
   HF_TRY(launch_cols<COL_COMPLEX>(ca, p->count, s));
   // cross power against the centre spectrum (fused into the inverse row pass), inverse columns
   RowArgs rb{};
-  rb.pl = p->pw, rb.tw = p->tw_w, rb.n_rows = rows, rb.inv = true, rb.out = p->cross;
+  rb.pl = p->pw.pl, rb.n = p->pw.n, rb.tw = p->pw.tw, rb.n_rows = rows, rb.inv = true, rb.out = p->cross;
   rb.spec = p->spec, rb.ref_img = p->center, rb.h = p->h;
   HF_TRY(launch_rows<ROW_CROSS>(rb, s));
   ColArgs cb{};
-  cb.pl = p->ph, cb.tw = p->tw_h, cb.w = p->w, cb.inv = true, cb.in = p->cross, cb.outf = mo;
+  cb.pl = p->ph.pl, cb.h = p->ph.n, cb.tw = p->ph.tw, cb.w = p->w, cb.inv = true, cb.in = p->cross, cb.outf = mo;
   cb.scale = (float)(1.0 / ((double)p->h * p->w)); // backward norm (cross_correlation2.cu:119-125)
   HF_TRY(launch_cols<COL_REAL>(cb, p->count, s));
-  shk_peak_kernel<<<p->count, kShkThreads, 0, s>>>(mo, p->shifts, p->h, p->w);
+  shk_peak_kernel<<<p->count, kRedThreads, 0, s>>>(mo, p->shifts, p->h, p->w);
   note_launch();
   HF_TRY(launch_status("shk_peak_kernel"));
   shk_slopes_kernel<<<1, 32, 0, s>>>(p->shifts, p->active, slopes, p->count, p->center, p->sppx, p->sppy);
