@@ -474,11 +474,16 @@ def run_autofocus(args, local):
             pipe.run(ring, RING_FRAMES, (step[0] * B * HOP) % RING_FRAMES, B, out=res)
             step[0] += 1
         t = timed(run, max(4, args.steps // 2))
+        pipe.timing(True)
+        run()
+        torch.cuda.synchronize()
+        stages = {k: round(v[0], 3) for k, v in pipe.stage_times().items() if v[0] > 0}
+        pipe.timing(False)
         pipe.close()
-        return B / (t / 1000.0), t
+        return B / (t / 1000.0), t, stages
 
-    on, on_ms = pipeline_rate(AF_ORDERS) if not args.af_no_pipeline else (0.0, 0.0)
-    off, off_ms = pipeline_rate(()) if not args.af_no_pipeline else (0.0, 0.0)
+    on, on_ms, on_st = pipeline_rate(AF_ORDERS) if not args.af_no_pipeline else (0.0, 0.0, {})
+    off, off_ms, off_st = pipeline_rate(()) if not args.af_no_pipeline else (0.0, 0.0, {})
 
     cpu = None
     if not args.no_cpu:
@@ -504,7 +509,8 @@ def run_autofocus(args, local):
         "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
         "pipeline_config1_chosen": {"autofocus_on_windows_per_s": round(on, 1), "ms_per_8_windows_on": round(on_ms, 3),
                                     "autofocus_off_windows_per_s": round(off, 1),
-                                    "ms_per_8_windows_off": round(off_ms, 3)},
+                                    "ms_per_8_windows_off": round(off_ms, 3),
+                                    "stages_ms_per_8_windows_on": on_st, "stages_ms_per_8_windows_off": off_st},
         "clocks": clk.summary()}), flush=True)
 
 
