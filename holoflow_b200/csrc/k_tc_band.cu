@@ -10,7 +10,9 @@
 // 64j .. 64j+63, all 512 columns for W = 1024).
 // The epilogue moves 4 bins at a time from TMEM into shared memory (adding the DC correction and
 // multiplying by the Fresnel lens), runs each bin's length-W row FFT in place (four-step, padded
-// exchange) and stores the row of that band plane.
+// exchange) and stores the row of that band plane.  In raw mode (`raw`, lens null) it stores the
+// DC-corrected band rows themselves, for steps that act on the planes before the lens (Filter2D,
+// the autofocus).
 //
 // Warp roles (384 threads, one CTA per SM, persistent over rows):
 //   warps 0-3  : load + unpack the next row into the A operand, rebuild B per window, and (thread 0)
@@ -347,7 +349,13 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
           }
         named_bar(bar, 128);
         const int bin = 4 * g + q;
-        if (bin < a.nz) {
+        if (bin < a.nz && a.raw) { // the bin's row as it is, coalesced
+          const float2 *buf  = tbuf + q * RS;
+          float2       *orow = a.out + (int64_t)w * a.out_win + (int64_t)bin * a.out_plane + (int64_t)r * a.out_row;
+#pragma unroll 4
+          for (int n1 = 0; n1 < N1; ++n1)
+            orow[lane + 32 * n1] = buf[lane + 32 * n1];
+        } else if (bin < a.nz) {
           float2 *buf = tbuf + q * RS;
           float2  x[N1];
 #pragma unroll

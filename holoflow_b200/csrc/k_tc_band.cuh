@@ -22,6 +22,8 @@ struct BandRowsArgs {
   int          *status;      // device status word (bounded waits)
   int           max_ctas;    // persistent grid size cap (SMs left to concurrent work otherwise)
   int          *row_counter; // device int, zeroed by the launcher: CTAs take rows from it
+  int           raw = 0;     // 1: store the band planes as they are (no row FFT; lens normally
+                             // null), for steps that act on them before the lens
 };
 
 bool band_rows_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes);

@@ -99,6 +99,7 @@ struct hf_plan {
   void      *cov_ws = nullptr;
   bool       cov_tc = false;   // tensor-core Gram matrix (chosen form)
   bool       rows_tc = false;  // tensor-core band DFT fused with lens + row FFT (chosen form)
+  bool       raw_tc = false;   // tensor-core band DFT storing raw planes (chosen form, Filter2D or autofocus)
   bool       cols_tma = false; // TMA-fed column FFT + moments over `band` through band_tmap
   CUtensorMap band_tmap{};
   size_t     bytes = 0;
@@ -229,14 +230,26 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     return cols_moments(p, nwin, out, s);
   }
 
-  BandArgs ba{};
-  ba.ring = fr, ba.T = d.frames, ba.P = p->P, ba.H = d.height, ba.W = d.width, ba.nz = p->nz;
-  ba.wmat = wmat, ba.wmat_stride = wstride, ba.z0 = d.z_begin;
-  ba.lens = d.propagation == HF_PROP_FRESNEL && !p->filter2d && !p->af ? p->lens : nullptr;
-  ba.out = p->band, ba.OH = d.height, ba.OW = d.width, ba.oy = 0, ba.ox = 0;
-  ba.out_plane = p->P, ba.out_win = win_px, ba.scale = 1.0f;
   int rec = p->timer.begin(s, ST_BAND);
-  HF_TRY(launch_band_dft(ba, d.input_dtype, nwin, s));
+  if (p->raw_tc && (reinterpret_cast<uintptr_t>(fr.base) & 15) == 0) {
+    // chosen form with a step before the lens: the tensor-core band DFT stores the raw planes
+    BandRowsArgs br{};
+    br.ring = fr, br.T = d.frames, br.H = d.height, br.W = d.width, br.nz = p->nz;
+    br.wmat = wmat, br.wmat_stride = wstride, br.lens = nullptr, br.out = p->band, br.raw = 1;
+    br.lambda = d.lambda, br.z = d.z, br.dx = d.pitch;
+    br.out_win = win_px, br.out_plane = p->P, br.out_row = d.width, br.nwin = nwin, br.shift = 2048.f;
+    br.status = p->status, br.max_ctas = std::max(1, sm_count() - reserve_sms);
+    br.row_counter = p->row_counter;
+    HF_TRY(launch_band_rows_tc(br, d.input_dtype, s));
+  } else {
+    BandArgs ba{};
+    ba.ring = fr, ba.T = d.frames, ba.P = p->P, ba.H = d.height, ba.W = d.width, ba.nz = p->nz;
+    ba.wmat = wmat, ba.wmat_stride = wstride, ba.z0 = d.z_begin;
+    ba.lens = d.propagation == HF_PROP_FRESNEL && !p->filter2d && !p->af ? p->lens : nullptr;
+    ba.out = p->band, ba.OH = d.height, ba.OW = d.width, ba.oy = 0, ba.ox = 0;
+    ba.out_plane = p->P, ba.out_win = win_px, ba.scale = 1.0f;
+    HF_TRY(launch_band_dft(ba, d.input_dtype, nwin, s));
+  }
   if (p->filter2d) // band planes -> FFT2 x annulus -> IFFT2, in place, before the lens
     HF_TRY(launch_filter2d(p->f2d, (int64_t)nwin * p->nz, d.height, d.width, 0, p->band, p->band, p->band2, nullptr, s));
   p->timer.end(s, rec);
@@ -461,9 +474,11 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
     if ((rc = cuda_status(cudaMemsetAsync(p->status, 0, sizeof(int), stream), "status reset")))
       break;
     // the tensor-core band pass holds 2 (z1 - z0) real columns per pixel: the one-sided band only
-    p->rows_tc = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
-                 d.time_method == HF_TIME_RFFT && !p->filter2d && !p->af &&
-                 band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
+    const bool tc_band = d.form == HF_FORM_CHOSEN && d.propagation == HF_PROP_FRESNEL && p->fast &&
+                         d.time_method == HF_TIME_RFFT &&
+                         band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
+    p->rows_tc = tc_band && !p->filter2d && !p->af;
+    p->raw_tc  = tc_band && (p->filter2d || p->af);
     if (d.propagation == HF_PROP_FRESNEL && p->fast && col_moments_tma_supported(d.height, d.width)) {
       const uint64_t rows = (uint64_t)B * p->nz * d.height;
       if ((rc = make_tmap_2d_f32(&p->band_tmap, p->band, 2 * (uint64_t)d.width, rows, 8 * (uint64_t)d.width, 16,

@@ -342,3 +342,29 @@ def test_pipeline_with_autofocus(cuda, form, n_iter):
         v = np.sort(img.ravel())[::-1]
         return v[:64].sum() / v.sum()
     assert peak_share(got[0]) > 1.2 * peak_share(plain)
+
+
+def test_pipeline_with_autofocus_tensor_core_band(cuda):
+    """uint16 frames in the chosen form: the tensor-core band pass stores the raw band planes
+    for the autofocus (its lens and row FFT move to the per-window row pass)."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    T, side, k0, a4, nb = 64, 256, 9, 4.0, 5
+    fr = doppler_frames(T, side, k0, a4)
+    frames = np.clip(np.rint(2048.0 + fr * (1800.0 / np.abs(fr).max())), 0, 4095).astype(np.uint16)
+    ring = torch.from_numpy(frames.view(np.int16)).to(cuda)
+    cfg = pl.PipelineConfig(height=side, width=side, frames=T, hop=T, z_begin=6, z_end=13, input_dtype=hf.HF_U16,
+                            lam=LAM, pitch=DX, z=Z, form=1, max_batch=1, autofocus_nb_subaps=nb,
+                            autofocus_orders=(4, 5, 6))
+    p = pl.Pipeline(cfg)
+    got = p.run(ring, T, 0, 1).cpu().numpy()[0]
+    assert p.status() == 0
+    coeff = p.autofocus_coefficients(0).cpu().numpy()
+    ocfg = O.PathConfig(side, side, T, T, 6, 13, lam=LAM, pitch=DX, z=Z, autofocus=dict(nb=nb, orders=[4, 5, 6]))
+    exp = O.reconstruct_window(frames.astype(np.float64), ocfg)
+    _, ecoeff = O.autofocus_planes(O.band_planes(frames.astype(np.float64), ocfg), ocfg)
+    assert np.abs(coeff - ecoeff).max() < 1e-3 * max(1.0, np.abs(ecoeff).max())
+    for m in range(3):
+        assert O.rel_l2(got[m], exp[m]) < 1e-3, m
+    assert abs(coeff[0] - a4) < 0.35 * a4
