@@ -29,6 +29,27 @@ __device__ __forceinline__ void row_load(const RowPass &a, int w, int64_t row, i
   const int ir    = r - a.oy;
   const bool in_rows = ir >= 0 && ir < a.IH;
   const int64_t ibase = w * a.in_win + plane * a.in_plane + (int64_t)ir * a.in_row;
+  if (a.ox == 0 && a.oy == 0 && a.IW == N1 * 32 && a.IH == a.H) {
+    // no padding: every sample exists, so all loads (and then all lens loads) issue back to back
+    // instead of one bounds-checked load at a time
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int64_t off = ibase + (int64_t)(lane + 32 * n1) * a.in_col;
+      x[n1] = a.in_real ? make_float2(__ldg(reinterpret_cast<const float *>(a.in) + off), 0.f)
+                        : __ldg(reinterpret_cast<const float2 *>(a.in) + off);
+    }
+    if (a.pre != nullptr) {
+      const float2 *pr = a.pre + (int64_t)r * (N1 * 32) + lane;
+      float2        pv[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1)
+        pv[n1] = __ldg(pr + 32 * n1);
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1)
+        x[n1] = cmul(x[n1], pv[n1]);
+    }
+    return;
+  }
 #pragma unroll
   for (int n1 = 0; n1 < N1; ++n1) {
     const int col = lane + 32 * n1;
