@@ -92,12 +92,39 @@ bool make_plan(int n, GPlan &pl) {
     st.by_nb = make_div((uint32_t)st.nb), st.by_Ns = make_div((uint32_t)Ns), st.by_p = make_div((uint32_t)p);
     Ns *= p;
   };
+  // prime-power factors first (4 before 2), then pairs of the small ones merged into one
+  // register radix (6, 8, 9, 10, 12, 15, 16): one shared-memory pass and barrier fewer per pair
+  std::vector<int> f;
   for (int p : {4, 2, 3, 5, 7, 11, 13, 17})
     while (rem % p == 0)
-      push(p), rem /= p;
+      f.push_back(p), rem /= p;
   for (int p = 19; rem > 1; p += 2)
     while (rem % p == 0)
-      push(p), rem /= p;
+      f.push_back(p), rem /= p;
+  auto mergeable = [](int a, int b) {
+    const int c = a * b;
+    return (a <= 5 && b <= 5) && (c == 6 || c == 8 || c == 9 || c == 10 || c == 12 || c == 15 || c == 16);
+  };
+  std::vector<int> radices;
+  for (size_t i = 0; i < f.size(); ++i) {
+    size_t best = f.size();
+    if (f[i] <= 5)
+      for (size_t k = i + 1; k < f.size(); ++k)
+        if (f[k] > 0 && mergeable(f[i], f[k]) && (best == f.size() || f[i] * f[k] > f[i] * f[best]))
+          best = k;
+    if (f[i] == 0)
+      continue;
+    if (best < f.size()) {
+      radices.push_back(f[i] * f[best]);
+      f[best] = 0;
+    } else {
+      radices.push_back(f[i]);
+    }
+  }
+  if ((int)radices.size() > kShkStages)
+    return false;
+  for (int p : radices)
+    push(p);
   return true;
 }
 
@@ -149,8 +176,46 @@ __device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
 // Y[q] = v0 + sum_r (v_r + v_{P-r}) cos(2 pi q r / P) - i sum_r (v_r - v_{P-r}) sin(2 pi q r / P),
 // r = 1 .. (P-1)/2, with Y[P-q] the same with +i: ((P-1)/2)^2 complex-by-real products for both.
 // cos and sin of 2 pi m / P come from the length-n table at m n / P.
+template <int P> struct Split { // P = A B with A the radix taken first (0: P is 2, 4 or prime)
+  static constexpr int A = P % 4 == 0 && P > 4 ? 4 : (P % 2 == 0 && P > 4 ? 2 : (P % 3 == 0 && P > 3 ? 3 : 0));
+  static constexpr int B = A ? P / A : 0;
+};
+
+template <int P> __device__ __forceinline__ void dft_small(float2 (&v)[P], bool inv, const float2 *tw, int step);
+
+// Composite P = A B in registers (Cooley-Tukey): B DFTs of length A over v[i2 + B i1], the inner
+// twiddles w_P^(i2 k1) (table entries (i2 k1) n / P), A DFTs of length B; output k1 + A k2.
+template <int P> __device__ __forceinline__ void dft_composite(float2 (&v)[P], bool inv, const float2 *tw, int step) {
+  constexpr int A = Split<P>::A, B = Split<P>::B;
+  float2        u[P];
+#pragma unroll
+  for (int i2 = 0; i2 < B; ++i2) {
+    float2 t[A];
+#pragma unroll
+    for (int i1 = 0; i1 < A; ++i1)
+      t[i1] = v[i2 + B * i1];
+    dft_small<A>(t, inv, tw, step * B);
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1)
+      u[i2 * A + k1] = (i2 == 0 || k1 == 0) ? t[k1] : cmul(t[k1], twid(tw, ((i2 * k1) % P) * step, inv));
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < A; ++k1) {
+    float2 t[B];
+#pragma unroll
+    for (int i2 = 0; i2 < B; ++i2)
+      t[i2] = u[i2 * A + k1];
+    dft_small<B>(t, inv, tw, step * A);
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2)
+      v[k1 + A * k2] = t[k2];
+  }
+}
+
 template <int P> __device__ __forceinline__ void dft_small(float2 (&v)[P], bool inv, const float2 *tw, int step) {
-  if constexpr (P == 2) {
+  if constexpr (Split<P>::A != 0) {
+    dft_composite<P>(v, inv, tw, step);
+  } else if constexpr (P == 2) {
     const float2 a = v[0], b = v[1];
     v[0] = cadd(a, b), v[1] = csub(a, b);
   } else if constexpr (P == 4) {
@@ -272,7 +337,7 @@ __device__ void stage_bfly_odd(const float2 *x, float2 *y, int pitch, int rows, 
 template <int P>
 __device__ void stage_bfly(const float2 *x, float2 *y, int pitch, int rows, const Stage &st, const float2 *tw, int n,
                            bool inv) {
-  if constexpr (P % 2 == 1) {
+  if constexpr (P % 2 == 1 && Split<P>::A == 0) {
     stage_bfly_odd<P>(x, y, pitch, rows, st, tw, n, inv);
     return;
   }
@@ -342,6 +407,13 @@ __device__ float2 *fft_rows_smem(float2 *a, float2 *b, int pitch, int rows, cons
     case 11: stage_bfly<11>(a, b, pitch, rows, st, tw, pl.n, inv); break;
     case 13: stage_bfly<13>(a, b, pitch, rows, st, tw, pl.n, inv); break;
     case 17: stage_bfly<17>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 6: stage_bfly<6>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 8: stage_bfly<8>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 9: stage_bfly<9>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 10: stage_bfly<10>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 12: stage_bfly<12>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 15: stage_bfly<15>(a, b, pitch, rows, st, tw, pl.n, inv); break;
+    case 16: stage_bfly<16>(a, b, pitch, rows, st, tw, pl.n, inv); break;
     default: stage_generic(a, b, pitch, rows, st, pl.by_n, tw, pl.n, inv); break;
     }
     __syncthreads();
