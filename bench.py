@@ -64,9 +64,9 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_table():
-    """Per-window DRAM bytes of each stage from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "ncu_traffic_config1.txt"
+def traffic_table(name="ncu_traffic_config1.txt"):
+    """Per-window (per-launch) DRAM bytes of each stage from a committed ncu summary, if present."""
+    p = ROOT / "profiles" / name
     out = {}
     if p.exists():
         for line in p.read_text().splitlines():
@@ -451,8 +451,9 @@ def run_autofocus(args, local):
     dom = max(("short_time_fresnel_mean", "correct_phase"), key=lambda k: split[k])
     peak, peak_kind = peaks()
     achieved = algo[dom] / (split[dom] / 1000.0) / 1e9
+    tr = traffic_table("ncu_traffic_autofocus.txt").get(dom) if nz == Z1 - Z0 else None
     roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": tr,
             "algorithmic_bytes_per_launch": algo[dom], "ms_per_launch": round(split[dom], 4),
             "calls_ms": {k: round(v, 4) for k, v in split.items()}}
 
