@@ -142,6 +142,12 @@ void from_json(const nlohmann::json &j, DopplerMomentsSettings &s) {
     s.filter = j.at("filter").get<AngularSpectrumFilter>();
   if (j.contains("padding"))
     s.padding = j.at("padding").get<AngularSpectrumPadding>();
+  opt("autofocus_enabled", s.autofocus_enabled);
+  opt("autofocus_nb_subaps", s.autofocus_nb_subaps);
+  opt("autofocus_nb_iter", s.autofocus_nb_iter);
+  opt("autofocus_zernike_orders", s.autofocus_zernike_orders);
+  opt("autofocus_skip_subapertures_outside_pupil", s.autofocus_skip_subapertures_outside_pupil);
+  opt("pp_pctclip_radius", s.pp_pctclip_radius);
 }
 
 // ================================================================================================
@@ -810,6 +816,19 @@ DopplerPlan doppler_plan(const Check &check, const TDesc &idesc, const DopplerMo
     d.as_filter = 1;
     d.r_inner = s.filter->r_inner, d.r_outer = s.filter->r_outer;
     d.s_inner = s.filter->s_inner, d.s_outer = s.filter->s_outer;
+  }
+  if (s.autofocus_enabled) { // graph_builder.cc:139-147, 311-334
+    check(d.propagation == HF_PROP_FRESNEL, "Shack-Hartmann autofocus needs fresnel propagation");
+    check(s.autofocus_nb_iter > 0, "autofocus_nb_iter must be positive");
+    check(s.autofocus_nb_subaps > 0, "autofocus_nb_subaps must be positive");
+    check(s.autofocus_nb_subaps % 2 == 1, "autofocus_nb_subaps must be odd");
+    check(s.autofocus_zernike_orders.size() <= 9, "at most 9 autofocus_zernike_orders");
+    d.autofocus_nb_subaps = s.autofocus_nb_subaps, d.autofocus_n_iter = s.autofocus_nb_iter;
+    d.autofocus_n_orders  = (int)s.autofocus_zernike_orders.size();
+    for (size_t i = 0; i < s.autofocus_zernike_orders.size(); ++i)
+      d.autofocus_orders[i] = s.autofocus_zernike_orders[i];
+    d.autofocus_roi_radius   = s.pp_pctclip_radius;
+    d.autofocus_keep_outside = s.autofocus_skip_subapertures_outside_pupil ? 0 : 1;
   }
   dp.nmom = __builtin_popcount((unsigned)d.moment_mask);
   dp.OH   = d.pad_h ? d.pad_h : d.height;

@@ -1741,6 +1741,7 @@ int autofocus_fold_lens(hf_autofocus *a, const float2 *lens, float2 *out, cudaSt
   return launch_status("shk_fold_lens_kernel");
 }
 
+int autofocus_set_z(hf_autofocus *a, float z, cudaStream_t s) { return hf_stfd_set_z(a->stfd, z, s); }
 int autofocus_passes(const hf_autofocus *a) { return a->n_iter; }
 int autofocus_orders(const hf_autofocus *a) { return a->nidx; }
 const float *autofocus_cumulative_coeffs(const hf_autofocus *a) { return a->cum_coeffs; }

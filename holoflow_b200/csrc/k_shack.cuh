@@ -16,6 +16,8 @@ int autofocus_measure(hf_autofocus *a, const void *planes, cudaStream_t s);
 int autofocus_correct(hf_autofocus *a, const void *planes, void *out, cudaStream_t s);
 // out = lens exp(-i phase): the last measured correction folded into a [H][W] lens.
 int autofocus_fold_lens(hf_autofocus *a, const float2 *lens, float2 *out, cudaStream_t s);
+// A new propagation distance: rebuilds the short-time Fresnel input lens.
+int autofocus_set_z(hf_autofocus *a, float z, cudaStream_t s);
 int autofocus_passes(const hf_autofocus *a);
 int autofocus_orders(const hf_autofocus *a);
 const float *autofocus_cumulative_coeffs(const hf_autofocus *a);

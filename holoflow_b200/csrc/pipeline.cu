@@ -510,7 +510,10 @@ int hf_plan_set_z(hf_plan *p, float z, hf_stream_t s) {
   clear_error();
   HF_CHECK_ARG(p != nullptr, "hf_plan_set_z: null plan");
   p->d.z = z;
-  return plan_tables(p, s);
+  HF_TRY(plan_tables(p, s));
+  if (p->af) // the sub-aperture transform's input lens depends on z; the slopes and the fit do not
+    HF_TRY(autofocus_set_z(p->af, z, s));
+  return HF_OK;
 }
 
 int hf_plan_output_shape(const hf_plan *p, int32_t *oh, int32_t *ow, int32_t *nm) {

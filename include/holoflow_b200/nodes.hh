@@ -61,6 +61,13 @@ struct DopplerMomentsSettings {
   std::string                           time_method = "rfft";            // rfft | fft (settings.hh TimeMethod)
   std::optional<AngularSpectrumFilter>  filter;
   std::optional<AngularSpectrumPadding> padding;
+  // Shack-Hartmann autofocus before the Fresnel propagation, under the reference's Settings names
+  // (settings.hh autofocus_*, pp_pctclip_radius for the correlation ROI)
+  bool             autofocus_enabled = false;
+  int              autofocus_nb_subaps = 0, autofocus_nb_iter = 1;
+  std::vector<int> autofocus_zernike_orders;
+  bool             autofocus_skip_subapertures_outside_pupil = true;
+  float            pp_pctclip_radius = 0.5f;
 };
 
 // Source node reading a .holo file (holotask/include/holotask/sources/holofile.hh:30-50).

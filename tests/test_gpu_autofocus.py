@@ -368,3 +368,24 @@ def test_pipeline_with_autofocus_tensor_core_band(cuda):
     for m in range(3):
         assert O.rel_l2(got[m], exp[m]) < 1e-3, m
     assert abs(coeff[0] - a4) < 0.35 * a4
+
+
+def test_doppler_moments_node_with_autofocus(cuda):
+    """The DopplerMoments node with the reference's autofocus settings names runs the same plan as
+    PipelineConfig(autofocus_*): identical moments."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import nodes as N
+    from holoflow_b200 import pipeline as pl
+    T, side = 32, 256
+    frames = doppler_frames(T, side, 5, 4.0)
+    dev = torch.from_numpy(frames).to(cuda)
+    s = {"time_z_begin": 3, "time_z_end": 9, "propagation": "fresnel", "lambda": LAM, "dx": DX, "z": Z,
+         "input_format": "f32", "form": "chosen", "autofocus_enabled": True, "autofocus_nb_subaps": 5,
+         "autofocus_zernike_orders": [4, 5, 6]}
+    (got,) = N.run_sync_factory("DopplerMoments", s, [dev.reshape(1, T, side, side)])
+    cfg = pl.PipelineConfig(height=side, width=side, frames=T, hop=T, z_begin=3, z_end=9, input_dtype=hf.HF_F32,
+                            lam=LAM, pitch=DX, z=Z, form=1, max_batch=1, autofocus_nb_subaps=5,
+                            autofocus_orders=(4, 5, 6))
+    exp = pl.Pipeline(cfg).run(dev, T, 0, 1)
+    assert torch.equal(got, exp)

@@ -236,3 +236,14 @@ def test_autofocus_kinds_infer():
     assert N.infer("ZernikeDefocusZProp", zd, [desc([2])]) == []
     invalid("ZernikeDefocusZProp", dict(zd, indexes=[5, 6]), [desc([2])],
             "ZernikeDefocusZPropFactory inference error: indexes must contain Z4 defocus")
+
+
+def test_doppler_moments_autofocus_settings():
+    """DopplerMoments takes the reference's autofocus settings names (settings.hh autofocus_*)."""
+    s = {"time_z_begin": 3, "time_z_end": 9, "propagation": "fresnel", "lambda": 852e-9, "dx": 20e-6, "z": 0.25,
+         "input_format": "f32", "autofocus_enabled": True, "autofocus_nb_subaps": 5, "autofocus_zernike_orders": [4, 5]}
+    assert out_of("DopplerMoments", s, [desc([1, 32, 256, 256])]) == ((1, 3, 256, 256), F32)
+    p = "DopplerMomentsFactory inference error: "
+    invalid("DopplerMoments", {**s, "autofocus_nb_subaps": 4}, [desc([1, 32, 256, 256])], p + "autofocus_nb_subaps must be odd")
+    invalid("DopplerMoments", {**s, "propagation": "angular_spectrum"}, [desc([1, 32, 256, 256])],
+            p + "Shack-Hartmann autofocus needs fresnel propagation")
