@@ -46,7 +46,7 @@ class HfDesc(C.Structure):
         ("s_outer", C.c_uint32), ("time_method", C.c_int32),
         ("autofocus_nb_subaps", C.c_int32), ("autofocus_n_iter", C.c_int32), ("autofocus_n_orders", C.c_int32),
         ("autofocus_orders", C.c_int32 * 9), ("autofocus_roi_radius", C.c_float),
-        ("autofocus_keep_outside", C.c_int32),
+        ("autofocus_keep_outside", C.c_int32), ("autofocus_flatfield_period", C.c_float),
     ]
 
 
@@ -197,7 +197,8 @@ _PROTOS = {
     "hf_defocus_z": (C.c_int, [C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_double),
                                C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "hf_autofocus_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
-                                      C.c_float, C.c_int, C.POINTER(C.c_int), C.c_int, _vp, C.POINTER(_vp)]),
+                                      C.c_float, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_float, _vp,
+                                      C.POINTER(_vp)]),
     "hf_autofocus_pupil_radius": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "hf_autofocus_exec": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "hf_autofocus_outputs": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),

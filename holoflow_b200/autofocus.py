@@ -181,13 +181,14 @@ class Autofocus(_Handle):
 
     def __init__(self, nz: int, height: int, width: int, nb_subaps: int, lam: float, dx: float, z: float,
                  indexes: Sequence[int] = (), n_iter: int = 1, roi_radius: float = 0.5,
-                 skip_outside_pupil: bool = True, stream=None):
+                 skip_outside_pupil: bool = True, flatfield_period: float = 0.0, stream=None):
         super().__init__()
         self.shape, self.nb, self.indexes = (nz, height, width), nb_subaps, list(indexes)
         self.sub = (height // nb_subaps, width // nb_subaps)
         arr, n = _ints(self.indexes)
         check(lib().hf_autofocus_create(nz, height, width, nb_subaps, n_iter, lam, dx, z, roi_radius,
-                                        int(skip_outside_pupil), arr, n, _stream(stream), C.byref(self._h)))
+                                        int(skip_outside_pupil), arr, n, flatfield_period, _stream(stream),
+                                        C.byref(self._h)))
 
     @property
     def pupil_radius(self) -> float:

@@ -148,6 +148,8 @@ void from_json(const nlohmann::json &j, DopplerMomentsSettings &s) {
   opt("autofocus_zernike_orders", s.autofocus_zernike_orders);
   opt("autofocus_skip_subapertures_outside_pupil", s.autofocus_skip_subapertures_outside_pupil);
   opt("pp_pctclip_radius", s.pp_pctclip_radius);
+  opt("pp_flatfield", s.pp_flatfield);
+  opt("pp_flatfield_cutoff_period_m", s.pp_flatfield_cutoff_period_m);
 }
 
 // ================================================================================================
@@ -829,6 +831,10 @@ DopplerPlan doppler_plan(const Check &check, const TDesc &idesc, const DopplerMo
       d.autofocus_orders[i] = s.autofocus_zernike_orders[i];
     d.autofocus_roi_radius   = s.pp_pctclip_radius;
     d.autofocus_keep_outside = s.autofocus_skip_subapertures_outside_pupil ? 0 : 1;
+    if (s.pp_flatfield) {
+      check(s.pp_flatfield_cutoff_period_m > 0.f, "flatfield cutoff period and image pitches must be positive");
+      d.autofocus_flatfield_period = s.pp_flatfield_cutoff_period_m;
+    }
   }
   dp.nmom = __builtin_popcount((unsigned)d.moment_mask);
   dp.OH   = d.pad_h ? d.pad_h : d.height;

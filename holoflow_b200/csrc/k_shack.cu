@@ -1578,6 +1578,7 @@ struct hf_autofocus {
   hf_stfd        *stfd  = nullptr;
   hf_shslopes    *sl    = nullptr;
   hf_zernike_fit *fit   = nullptr;
+  hf_flatfield   *ff    = nullptr; // optional high-pass of the sub-aperture images
   float          *m0    = nullptr, *slopes = nullptr, *coeffs = nullptr, *cum_coeffs = nullptr;
   float          *phase = nullptr, *cum_phase = nullptr;
 };
@@ -1587,6 +1588,7 @@ void release(hf_autofocus *a) {
   if (!a)
     return;
   release(a->stfd), release(a->sl), release(a->fit);
+  hf_flatfield_destroy(a->ff);
   cudaFree(a->m0), cudaFree(a->slopes), cudaFree(a->coeffs), cudaFree(a->cum_coeffs);
   cudaFree(a->phase), cudaFree(a->cum_phase);
   delete a;
@@ -1596,8 +1598,8 @@ void release(hf_autofocus *a) {
 extern "C" {
 
 int hf_autofocus_create(int nz, int height, int width, int nb_subaps, int n_iter, float lambda, float dx, float z,
-                        float roi_radius, int skip_outside, const int *indexes, int n_indexes, hf_stream_t s,
-                        hf_autofocus **out) {
+                        float roi_radius, int skip_outside, const int *indexes, int n_indexes,
+                        float flatfield_period, hf_stream_t s, hf_autofocus **out) {
   clear_error();
   HF_CHECK_ARG(out != nullptr, "Autofocus: null argument");
   *out = nullptr;
@@ -1626,6 +1628,14 @@ int hf_autofocus_create(int nz, int height, int width, int nb_subaps, int n_iter
   if (rc == HF_OK && n_indexes > 0)
     rc = hf_zernike_fit_create(nb_subaps, nb_subaps, a->sh, a->sw, a->sh, a->sw, lambda, dx, dx, skip_outside, indexes,
                                n_indexes, &a->fit);
+  if (rc == HF_OK && flatfield_period > 0.f) {
+    // graph_builder.cc:348-352: sigma = 0.187 period / pitch, with the one-FFT Fresnel output
+    // pitch lambda |z| / (n d) of a sub-aperture (fresnel_1fft_output_pitch), in float32
+    const float dy_out = lambda * std::fabs(z) / ((float)a->sh * dx);
+    const float dx_out = lambda * std::fabs(z) / ((float)a->sw * dx);
+    rc = hf_flatfield_create((int64_t)nsub, a->sh, a->sw, 0.187f * flatfield_period / dy_out,
+                             0.187f * flatfield_period / dx_out, s, &a->ff);
+  }
   if (rc == HF_OK)
     rc = cuda_status(cudaMalloc(&a->m0, nsub * a->sh * a->sw * sizeof(float)), "Autofocus: M0");
   if (rc == HF_OK)
@@ -1722,6 +1732,8 @@ int autofocus_begin(hf_autofocus *a, cudaStream_t s) {
 
 int autofocus_measure(hf_autofocus *a, const void *planes, cudaStream_t s) {
   HF_TRY(hf_stfd_exec(a->stfd, planes, a->m0, s));
+  if (a->ff) // in place: each pass reads its input only where it writes, or before it writes
+    HF_TRY(hf_flatfield_exec(a->ff, a->m0, a->m0, s));
   HF_TRY(hf_shslopes_exec(a->sl, a->m0, a->slopes, nullptr, s));
   if (a->nidx > 0) {
     HF_TRY(hf_zernike_fit_exec(a->fit, a->slopes, a->coeffs, a->cum_coeffs, s));

@@ -427,8 +427,8 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       if ((rc = hf_autofocus_create(p->nz, d.height, d.width, d.autofocus_nb_subaps, std::max(1, d.autofocus_n_iter),
                                     d.lambda, d.pitch, d.z,
                                     d.autofocus_roi_radius > 0.f ? d.autofocus_roi_radius : 0.5f,
-                                    d.autofocus_keep_outside ? 0 : 1, d.autofocus_orders, d.autofocus_n_orders, stream,
-                                    &p->af)))
+                                    d.autofocus_keep_outside ? 0 : 1, d.autofocus_orders, d.autofocus_n_orders,
+                                    d.autofocus_flatfield_period, stream, &p->af)))
         break;
       if ((rc = dev_alloc(&p->lens_af, (size_t)(B * p->P), p->bytes)) ||
           (rc = dev_alloc(&p->af_coeff, (size_t)(9 * B), p->bytes)))

@@ -103,6 +103,7 @@ class PipelineConfig:
     autofocus_orders: Sequence[int] = ()  # Noll indexes 2..10 (empty = off)
     autofocus_roi_radius: float = 0.5
     autofocus_keep_outside: int = 0
+    autofocus_flatfield_period: float = 0.0  # pp_flatfield cutoff period [m] on the sub-aperture images
 
     def desc(self) -> HfDesc:
         orders = list(self.autofocus_orders)
@@ -112,7 +113,7 @@ class PipelineConfig:
                       self.pad_w, self.pad_h, self.as_filter, self.r_inner, self.r_outer,
                       self.s_inner, self.s_outer, self.time_method, self.autofocus_nb_subaps,
                       self.autofocus_n_iter, len(orders), (C.c_int32 * 9)(*orders), self.autofocus_roi_radius,
-                      self.autofocus_keep_outside)
+                      self.autofocus_keep_outside, self.autofocus_flatfield_period)
 
     @property
     def frame_bytes(self) -> int:

@@ -209,6 +209,7 @@ typedef struct hf_desc {
   int32_t autofocus_orders[9];   /* Noll indexes 2..10                                         */
   float   autofocus_roi_radius;  /* correlation ROI radius (pp_pctclip_radius; 0 reads as 0.5) */
   int32_t autofocus_keep_outside; /* 1: keep sub-apertures outside the pupil                   */
+  float   autofocus_flatfield_period; /* pp_flatfield cutoff period [m] on the sub-aperture images (0 = off) */
 } hf_desc;
 #define HF_TIME_RFFT 0
 #define HF_TIME_FFT 1
@@ -525,8 +526,10 @@ int hf_defocus_z(float a4, float lambda, float z_curr, float pupil_radius, doubl
                  double *delta_z_mm);
 
 /* One autofocus pass chain on one spectrum (build_shack_hartmann, graph_builder.cc:307-501, with
- * pp_accumulation 1 and no flatfield): sub-apertures of W / nb x H / nb (nb odd), short-time
- * Fresnel with the global phase, mean |.| over the nz planes, fftshift, single-reference slopes
+ * pp_accumulation 1): sub-apertures of W / nb x H / nb (nb odd), short-time Fresnel with the
+ * global phase, mean |.| over the nz planes, fftshift, optionally the flatfield of pp_flatfield
+ * (flatfield_period > 0: the cutoff period in metres, sigma = 0.187 period / (lambda |z| / (n dx));
+ * 0: off), single-reference slopes
  * in the ROI circle of radius roi_radius, device Zernike fit, phase map over H x W, and
  * corrected = delayed exp(-i phase) (delayed NULL: the planes themselves).  n_iter passes chain
  * as the reference's (each later pass measures and corrects the previous output);
@@ -535,8 +538,8 @@ int hf_defocus_z(float a4, float lambda, float z_curr, float pupil_radius, doubl
  * summed over the passes.  With n_indexes 0 the planes pass through. */
 typedef struct hf_autofocus hf_autofocus;
 int hf_autofocus_create(int nz, int height, int width, int nb_subaps, int n_iter, float lambda, float dx, float z,
-                        float roi_radius, int skip_outside_pupil, const int *indexes, int n_indexes, hf_stream_t s,
-                        hf_autofocus **a);
+                        float roi_radius, int skip_outside_pupil, const int *indexes, int n_indexes,
+                        float flatfield_period, hf_stream_t s, hf_autofocus **a);
 int hf_autofocus_pupil_radius(const hf_autofocus *a, float *radius);
 int hf_autofocus_exec(hf_autofocus *a, const void *planes, const void *delayed, void *corrected, hf_stream_t s);
 int hf_autofocus_outputs(const hf_autofocus *a, float *m0, float *slopes, float *coeffs, float *phase, hf_stream_t s);

@@ -68,6 +68,8 @@ struct DopplerMomentsSettings {
   std::vector<int> autofocus_zernike_orders;
   bool             autofocus_skip_subapertures_outside_pupil = true;
   float            pp_pctclip_radius = 0.5f;
+  bool             pp_flatfield = false;            // flatfield of the sub-aperture images
+  float            pp_flatfield_cutoff_period_m = 0.f;
 };
 
 // Source node reading a .holo file (holotask/include/holotask/sources/holofile.hh:30-50).

@@ -552,7 +552,7 @@ def autofocus_planes(planes: np.ndarray, cfg: PathConfig):
     from . import shack as SH
     a = cfg.autofocus
     acfg = SH.AutofocusConfig(a["nb"], cfg.lam, cfg.pitch, cfg.z, list(a["orders"]), a.get("roi_radius", 0.5),
-                              not a.get("keep_outside", False))
+                              not a.get("keep_outside", False), a.get("flatfield_period", 0.0))
     total = np.zeros(len(acfg.indexes))
     cur = np.asarray(planes, np.complex128)
     for _ in range(a.get("n_iter", 1)):

@@ -356,6 +356,23 @@ class AutofocusConfig:
     indexes: Sequence[int] = (4,)
     roi_radius: float = 0.5
     skip_outside: bool = True
+    flatfield_period: float = 0.0  # pp_flatfield cutoff period [m]; 0 = off
+
+
+def subaperture_flatfield(m0: np.ndarray, cfg: AutofocusConfig) -> np.ndarray:
+    """graph_builder.cc:348-352: the flatfield of every sub-aperture image with sigma =
+    0.187 period / pitch, the pitch being the one-FFT Fresnel output pitch lambda |z| / (n d)
+    of a sub-aperture (graph_builder.cc:32-66), all in float32."""
+    from . import oracle as O
+    nb, _, sh, sw = m0.shape
+    dy_out = F32(cfg.lam) * abs(F32(cfg.z)) / (F32(sh) * F32(cfg.dx))
+    dx_out = F32(cfg.lam) * abs(F32(cfg.z)) / (F32(sw) * F32(cfg.dx))
+    sy = float(F32(0.187) * F32(cfg.flatfield_period) / dy_out)
+    sx = float(F32(0.187) * F32(cfg.flatfield_period) / dx_out)
+    flat = m0.reshape(nb * nb, sh, sw)
+    out = O.flatfield_fourier(flat, sy, sx) if O.flatfield_uses_fourier(sh, sw, sy, sx) else \
+        O.flatfield_spatial(flat, sy, sx)
+    return np.asarray(out, np.float64).reshape(m0.shape)
 
 
 def autofocus(planes: np.ndarray, cfg: AutofocusConfig, delayed: Optional[np.ndarray] = None):
@@ -366,6 +383,8 @@ def autofocus(planes: np.ndarray, cfg: AutofocusConfig, delayed: Optional[np.nda
     nb = cfg.nb_subaps
     sh, sw = H // nb, W // nb
     m0 = subaperture_m0(planes, nb, cfg.lam, cfg.dx, cfg.z)
+    if cfg.flatfield_period > 0.0:
+        m0 = subaperture_flatfield(m0, cfg)
     roi = (0.5, 0.5, cfg.roi_radius, cfg.roi_radius, 0.0)
     slopes = shack_hartmann_slopes(m0, cfg.lam, cfg.dx, cfg.dx, cfg.z, roi, cfg.skip_outside)
     geo = geometry(nb, nb, sh, sw, sh, sw, cfg.dx, cfg.dx, cfg.skip_outside)

@@ -30,17 +30,17 @@ def ints(v):
 def test_autofocus_create_validation(nb, msg):
     h = C.c_void_p()
     arr, n = ints([4])
-    rc, text = err(lib().hf_autofocus_create(2, 64, 64, nb, 1, LAM, DX, Z, 0.5, 1, arr, n, None, C.byref(h)))
+    rc, text = err(lib().hf_autofocus_create(2, 64, 64, nb, 1, LAM, DX, Z, 0.5, 1, arr, n, 0.0, None, C.byref(h)))
     assert rc == hf.HF_ERR_INVALID and msg in text and not h
 
 
 def test_autofocus_iterations_and_orders_validation():
     h = C.c_void_p()
     arr, n = ints([4])
-    rc, text = err(lib().hf_autofocus_create(2, 64, 64, 5, 0, LAM, DX, Z, 0.5, 1, arr, n, None, C.byref(h)))
+    rc, text = err(lib().hf_autofocus_create(2, 64, 64, 5, 0, LAM, DX, Z, 0.5, 1, arr, n, 0.0, None, C.byref(h)))
     assert rc == hf.HF_ERR_INVALID and "autofocus_nb_iter must be positive" in text
     arr, n = ints([4, 11])
-    rc, text = err(lib().hf_autofocus_create(2, 64, 64, 5, 1, LAM, DX, Z, 0.5, 1, arr, n, None, C.byref(h)))
+    rc, text = err(lib().hf_autofocus_create(2, 64, 64, 5, 1, LAM, DX, Z, 0.5, 1, arr, n, 0.0, None, C.byref(h)))
     assert rc == hf.HF_ERR_INVALID and "only Noll indexes 2..10 are supported" in text
 
 

@@ -389,3 +389,36 @@ def test_doppler_moments_node_with_autofocus(cuda):
                             autofocus_orders=(4, 5, 6))
     exp = pl.Pipeline(cfg).run(dev, T, 0, 1)
     assert torch.equal(got, exp)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_pipeline_with_autofocus_flatfield(cuda, form):
+    """pp_flatfield on the sub-aperture images (graph_builder.cc:348-352), sigma from the cutoff
+    period and the one-FFT Fresnel output pitch, in the fused pipeline and the standalone pass."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import autofocus as af
+    from holoflow_b200 import pipeline as pl
+    T, side, per = 32, 256, 2e-3
+    frames = doppler_frames(T, side, 5, 4.0)
+    ring = torch.from_numpy(frames).to(cuda)
+    cfg = pl.PipelineConfig(height=side, width=side, frames=T, hop=T, z_begin=3, z_end=9, input_dtype=hf.HF_F32,
+                            lam=LAM, pitch=DX, z=Z, form=form, max_batch=1, autofocus_nb_subaps=5,
+                            autofocus_orders=(4, 5, 6), autofocus_flatfield_period=per)
+    p = pl.Pipeline(cfg)
+    got = p.run(ring, T, 0, 1).cpu().numpy()[0]
+    coeff = p.autofocus_coefficients(0).cpu().numpy()
+    ocfg = O.PathConfig(side, side, T, T, 3, 9, lam=LAM, pitch=DX, z=Z,
+                        autofocus=dict(nb=5, orders=[4, 5, 6], flatfield_period=per))
+    planes = O.band_planes(frames.astype(np.float64), ocfg)
+    _, ecoeff = O.autofocus_planes(planes, ocfg)
+    assert np.abs(coeff - ecoeff).max() < 1e-3 * max(1.0, np.abs(ecoeff).max())
+    exp = O.reconstruct_window(frames.astype(np.float64), ocfg)
+    for m in range(3):
+        assert O.rel_l2(got[m], exp[m]) < (1e-4 if form == 0 else 1e-3), m
+    # the standalone pass: the flattened sub-aperture images against the oracle
+    op = af.Autofocus(planes.shape[0], side, side, 5, LAM, DX, Z, indexes=[4, 5, 6], flatfield_period=per)
+    op(torch.from_numpy(planes.astype(np.complex64)).to(cuda))
+    acfg = SH.AutofocusConfig(5, LAM, DX, Z, [4, 5, 6], flatfield_period=per)
+    em0 = SH.subaperture_flatfield(SH.subaperture_m0(planes, 5, LAM, DX, Z), acfg)
+    assert O.rel_l2(op.m0().cpu().numpy(), em0) < 2e-5
