@@ -227,8 +227,8 @@ def clutter_basis(frames: np.ndarray, rank: int) -> np.ndarray:
 def svd_filter(frames: np.ndarray, rank: int) -> np.ndarray:
     """Remove the top-``rank`` eigenvectors along time: Y = X (I - V V^T) per pixel.
 
-    BASELINE config 1 asks for the removal of the top-4 eigenvectors of the 64x64 complex
-    covariance of the propagated frames.  Propagation A (unit-modulus lens + unnormalised DFT)
+    The full-size workload (1024^2 12-bit frames, T = 64) removes the top-4 eigenvectors of the
+    64x64 complex covariance of the propagated frames.  Propagation A (unit-modulus lens + unnormalised DFT)
     satisfies A^H A = N I, so (A X)^H (A X) = N X^T X for real frames: the eigenvectors are those
     of the real covariance and the filter commutes with propagation (tested in
     tests/test_oracle_model.py).
@@ -480,7 +480,7 @@ def moments_from_magnitude(mag: np.ndarray, weights: np.ndarray, fftshift: bool 
 
 # -------------------------------------------------------------------------------------------------
 # a14: the per-window path end to end (graph_builder.cc:245-305 TFA, 522-566 propagation,
-# 604-678 view), with the SVD clutter filter of BASELINE config 1 inserted before the band DFT
+# 604-678 view), with the SVD clutter filter of the full-size workload inserted before the band DFT
 # -------------------------------------------------------------------------------------------------
 
 @dataclass

@@ -127,7 +127,8 @@ class Interferograms:
         return out
 
 
-# The BASELINE workloads (sizes, rates and bands), restated.
+# The benchmark workloads (sizes, rates and bands): config0 the small host-path case, config1 the
+# full-size 1024^2 12-bit case, and the uneven and serving mixes.
 def config0(n_frames: int = 32, acquisition: int = 0) -> SynthConfig:
     return SynthConfig(512, 512, n_frames, 37e3, 400, 0.30, seed=config_seed(0, acquisition))
 
