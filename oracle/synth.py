@@ -128,7 +128,7 @@ class Interferograms:
 
 
 # The benchmark workloads (sizes, rates and bands): config0 the small host-path case, config1 the
-# full-size 1024^2 12-bit case, and the uneven and serving mixes.
+# full-size 1024^2 12-bit case, config2 the same with a set clutter-to-signal ratio.
 def config0(n_frames: int = 32, acquisition: int = 0) -> SynthConfig:
     return SynthConfig(512, 512, n_frames, 37e3, 400, 0.30, seed=config_seed(0, acquisition))
 
