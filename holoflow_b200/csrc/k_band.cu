@@ -90,11 +90,19 @@ __global__ void __launch_bounds__(256) band_dft_tiled_kernel(BandArgs a, int til
   const int64_t tile_byte0 = tile0 * num / den;
   const int64_t valid_px   = min((int64_t)tile_px, a.P - tile0);
   const int     valid_words = (int)(valid_px * num / den + 3) / 4;
+  // asynchronous 4-byte copies: every frame's words are in flight at once instead of one
+  // load-then-store at a time (the tail beyond the image is zero-filled, src-size 0)
   for (int t = 0; t < a.T; ++t) {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(a.ring.frame(w, t) + tile_byte0);
-    for (int i = tid; i < row_words; i += blockDim.x)
-      tile[t * row_words + i] = i < valid_words ? __ldg(src + i) : 0u;
+    for (int i = tid; i < row_words; i += blockDim.x) {
+      const bool     ok  = i < valid_words;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(tile + t * row_words + i);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(ok ? src + i : src),
+                   "r"(ok ? 4 : 0)
+                   : "memory");
+    }
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   for (int i = tid; i < a.T * nzpad; i += blockDim.x) {
     const int t = i / nzpad, k = i % nzpad;
     w_sh[i]     = k < a.nz ? wmat_entry(a, w, t, k) : make_float2(0.f, 0.f);
