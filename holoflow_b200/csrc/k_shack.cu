@@ -6,14 +6,19 @@
 //
 // Sub-aperture sides are W / nb with nb odd (102, 170, 204, 73, ...), which the four-step
 // power-of-two passes of the Fresnel path do not cover.  This file therefore carries its own
-// shared-memory FFT for any length 2 <= n <= 1024: a Stockham auto-sort sequence of stages, each
-// one radix p of the factorisation of n (4 and 2 first, then 3 and 5 as register butterflies;
-// any other prime p as p-term sums per output).  A stage of radix p over sub-transforms of span
-// Ns reads x[j + r n/p], twiddles input r by w_n^(r m (j mod Ns)) with m = n / (Ns p), takes the
-// p-point DFT and writes output q to ((j / Ns) Ns p + j mod Ns) + q Ns.  Twiddles come from a
-// per-length table w_n^e built in float64 on the host.
+// shared-memory FFT for any length 2 <= n <= 1024: a Stockham auto-sort sequence of stages, one
+// per radix p of a factorisation of n planned on the host.
+//  - Factors 4, 2, 3, 5 are merged pairwise into the composite radices 6, 8, 9, 10, 12, 15, 16
+//    (one shared-memory pass and barrier fewer per pair).
+//  - Primes 3..17 take register butterflies in the symmetric form; a composite radix takes a
+//    register Cooley-Tukey split; any larger prime takes p-term sums per output.
+// A stage of radix p over sub-transforms of span Ns reads x[j + r n/p], twiddles input r by
+// w_n^(r m (j mod Ns)) with m = n / (Ns p) (the powers by recurrence from one table load), takes
+// the p-point DFT and writes output q to ((j / Ns) Ns p + j mod Ns) + q Ns.  Twiddles come from
+// a per-length table w_n^e built in float64 on the host; index divisions are multiply-high
+// divisions by invariant integers.
 //
-// Kernels (all memory-bound except the tiny solves):
+// Kernels (the transforms are instruction- and barrier-bound, the rest memory-bound or tiny):
 //  - shk_rows_kernel<MODE>: R rows of length n per CTA, gathered with the pre-operation of MODE
 //    (window gather x input lens for the short-time Fresnel transform; mean removal and cosine
 //    taper inside the correlation ROI; normalised cross power against the reference spectrum),
