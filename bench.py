@@ -33,6 +33,10 @@ Z0, Z1 = 4, 32                  # 4-33 kHz at df = fs/T = 1046.875 Hz
 RANK_CLUTTER = 4
 RING_FRAMES = 256               # 403 MB of packed frames (> 126 MB L2)
 METRIC = "1024²×64 M0 images/s and p99 frame-to-image latency, chosen vs plain form"
+E2E_STEPS = 200                 # end-to-end steps timed (p99 over this many latency samples)
+DTYPE = {"chosen": "u12 frames; i8 Gram and f16 hi+lo band DFT on tcgen05 tensor cores (f32 accumulate); "
+                   "f32 FFTs and moments; f64 Jacobi",
+         "plain": "u12 frames; f32 Gram, band DFT, FFTs and moments; f64 Jacobi"}
 WORKLOAD = "config1: 1024x1024 12-bit packed, T=64 hop=16, fs=67kHz, top-4 SVD clutter filter, Fresnel z=0.25m, M0/M1/M2 4-33kHz"
 
 
@@ -42,8 +46,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="chosen", choices=["plain", "chosen"],
-                    help="chosen: tensor-core Gram and band DFT (the headline); plain: all-FP32 kernels")
+    ap.add_argument("--form", default="both", choices=["both", "plain", "chosen"],
+                    help="both: the chosen form (the headline) and the plain form on the same ring and steps; "
+                         "chosen: tensor-core Gram and band DFT only; plain: all-FP32 kernels only")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the config-2 error, config-3 and config-4 legs of the default run")
     ap.add_argument("--batch", type=int, default=8, help="windows per step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -136,21 +143,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_baseline(sample_windows=1):
-    """The CPU restatement of the path (oracle port, float64 NumPy/SciPy, all host threads) on one
-    config-1 window; returns (windows/s, seconds, threads)."""
-    from oracle import oracle as O
-    from oracle import synth as S
-    frames = S.Interferograms(S.config1(T)).frames(0, T)
-    cfg = O.PathConfig(H, W, T, HOP, Z0, Z1, fs=FS, z=0.25, clutter_rank=RANK_CLUTTER)
-    O.reconstruct_window(frames, cfg)  # warm caches / thread pools
-    t0 = time.perf_counter()
-    for _ in range(sample_windows):
-        O.reconstruct_window(frames, cfg)
-    dt = time.perf_counter() - t0
-    return sample_windows / dt, dt, os.cpu_count()
-
-
 def max_over_ranks(value: float, world: int, device=None) -> float:
     """The largest `value` over all ranks (device-timed milliseconds); identity on one rank."""
     if world <= 1:
@@ -194,7 +186,7 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
-def run_batched(args, local):
+def run_batched(args, local, steps=None):
     """Sixteen seeded acquisitions of uneven frame size (256^2 .. 1536 x 1024), window length
     (32/64/128), z and fs: every acquisition's windows in ONE graph launch (chosen form, schedule
     picked by the autotuner) against per-acquisition launches of the plain form."""
@@ -204,6 +196,7 @@ def run_batched(args, local):
     from holoflow_b200.multi import Multi
     dev = torch.device("cuda", local)
     torch.cuda.set_device(local)
+    steps = steps or args.steps
     acqs = sy.config3_acquisitions()
     WIN = 2  # windows per acquisition per step
     rings, nfr, outs = [], [], []
@@ -230,12 +223,12 @@ def run_batched(args, local):
             p.run(r, n, 0, WIN, out=o)
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         for p, r, n, o in zip(plans, rings, nfr, outs):
             p.run(r, n, 0, WIN, out=o)
     e1.record(stream)
     torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1) / args.steps
+    plain_ms = e0.elapsed_time(e1) / steps
     for p in plans:
         p.close()
     del plans
@@ -246,16 +239,16 @@ def run_batched(args, local):
         m.exec(rings, nfr, first, outs)
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         m.exec(rings, nfr, first, outs)
     e1.record(stream)
     torch.cuda.synchronize()
-    graph_ms = e0.elapsed_time(e1) / args.steps
+    graph_ms = e0.elapsed_time(e1) / steps
     m.close()
     nwin = WIN * len(acqs)
-    print(json.dumps({
+    return {
         "metric": "uneven acquisitions: windows/s, one graph launch (chosen) vs per-acquisition launches (plain)",
-        "value": round(nwin / (graph_ms / 1000.0), 2), "unit": "windows/s", "n_gpus": 1, "steps": args.steps,
+        "value": round(nwin / (graph_ms / 1000.0), 2), "unit": "windows/s", "n_gpus": 1, "steps": steps,
         "warmup": args.warmup, "ms_per_step": round(graph_ms, 4), "higher_is_better": True,
         "baseline_plain_per_acquisition": {"value": round(nwin / (plain_ms / 1000.0), 2), "ms_per_step":
                                            round(plain_ms, 4)},
@@ -266,8 +259,8 @@ def run_batched(args, local):
                                "z 0.15-0.40 m, fs 37/67 kHz, top-4 clutter filter, Fresnel, M0/M1/M2",
                    "windows_per_step": nwin,
                    "acquisitions": [[a.scene.height, a.scene.width, a.frames, a.z_end - a.z_begin] for a in acqs]},
-        "dtype": "f32", "data": "synthetic (device-generated interferograms, seeded)",
-    }), flush=True)
+        "dtype": DTYPE["chosen"], "data": "synthetic (device-generated interferograms, seeded)",
+    }
 
 
 def run_serve(args, local, form, seed=1004, life=120):
@@ -515,61 +508,43 @@ def run_autofocus(args, local):
         "clocks": clk.summary()}), flush=True)
 
 
-def main():
-    args = parse()
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    if args.impl == "reference":
-        return run_reference(args, rank, world)
-    if args.workload == "batched":
-        return run_batched(args, local) if rank == 0 else None
-    if args.workload == "autofocus":
-        return run_autofocus(args, local) if rank == 0 else None
-    if args.workload == "serve":
-        if rank != 0:
-            return None
-        # untimed warm-up of both forms on the same seeded streams: loads every kernel module and
-        # builds every table once, so neither timed run pays the process's first-use costs
-        for f in (1, 0):
-            run_serve(args, local, f, life=8)
-        res = {f: run_serve(args, local, 1 if f == "chosen" else 0) for f in ("chosen", "plain")}
-        print(json.dumps({
-            "metric": "streaming server: sustained frames/s and p50/p99 frame-to-image latency, chosen vs plain",
-            "value": res["chosen"]["frames_per_s"], "unit": "frames/s", "n_gpus": 1, "higher_is_better": True,
-            "chosen": res["chosen"], "plain": res["plain"],
-            "config": {"workload": "config4: 12 Poisson-arriving streams (4 at start, 1.5 per round), 512^2.."
-                                   "1536x1024 12-bit packed, (T, hop) (64,16)/(128,32), fs 10-67 kHz, z 0.15-0.40 m, "
-                                   "top-4 clutter filter, 120 windows per stream, 8 GiB free-HBM reserve"},
-            "dtype": "f32", "data": "synthetic (device-generated interferograms, seeded)"}), flush=True)
-        return None
+def serve_pair(args, local):
+    """Config 4 for both forms: an untimed warm-up of each (loads every kernel module and builds
+    every table once, so neither timed run pays the process's first-use costs), then the timed
+    runs on the same seeded streams."""
+    for f in (1, 0):
+        run_serve(args, local, f, life=8)
+    res = {f: run_serve(args, local, 1 if f == "chosen" else 0) for f in ("chosen", "plain")}
+    return {
+        "metric": "streaming server: sustained frames/s and p50/p99 frame-to-image latency, chosen vs plain",
+        "value": res["chosen"]["frames_per_s"], "unit": "frames/s", "n_gpus": 1, "higher_is_better": True,
+        "chosen": res["chosen"], "plain": res["plain"],
+        "chosen_over_plain_frames_per_s": round(res["chosen"]["frames_per_s"] / res["plain"]["frames_per_s"], 3),
+        "config": {"workload": "config4: 12 Poisson-arriving streams (4 at start, 1.5 per round), 512^2.."
+                               "1536x1024 12-bit packed, (T, hop) (64,16)/(128,32), fs 10-67 kHz, z 0.15-0.40 m, "
+                               "top-4 clutter filter, 120 windows per stream, 8 GiB free-HBM reserve"},
+        "dtype": DTYPE["chosen"], "data": "synthetic (device-generated interferograms, seeded)"}
 
+
+def config1_cfg(form, B):
+    from holoflow_b200 import pipeline as pl
+    return pl.PipelineConfig(height=H, width=W, frames=T, hop=HOP, z_begin=Z0, z_end=Z1, fs=FS, z=0.25,
+                             clutter_rank=RANK_CLUTTER, max_batch=B, form=form)
+
+
+def measure_form(args, world, dev, local, form, packed, e2e_on=True):
+    """One numeric form on the config-1 workload: device-resident windows/s over exactly K timed
+    steps (the camera stream's ring filled before timing), per-stage times, the dominant stage's
+    roofline, then the end-to-end leg through the camera-stream API.  Returns the numbers and the
+    images of the last timed step's first window (its frames are generated frames 0..63 in order)."""
     import torch
     import torch.distributed as dist
     import holoflow_b200 as hf
     from holoflow_b200 import pipeline as pl
-    from holoflow_b200 import synth as sy
-
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     B = args.batch
-    form = hf.HF_FORM_CHOSEN if args.form == "chosen" else hf.HF_FORM_PLAIN
-    cfg = pl.PipelineConfig(height=H, width=W, frames=T, hop=HOP, z_begin=Z0, z_end=Z1, fs=FS, z=0.25,
-                            clutter_rank=RANK_CLUTTER, max_batch=B, form=form)
-    # synthetic frames: 64 distinct frames generated on the device, tiled over the ring
-    gen = sy.DeviceInterferograms(sy.config1_scene(acquisition=rank), device=dev)
-    base = gen.frames(0, 64)
+    cfg = config1_cfg(form, B)
     fb = cfg.frame_bytes
-    ring = torch.empty(RING_FRAMES * fb, dtype=torch.uint8, device=dev)
-    packed = pl.pack12(base.reshape(-1)).view(64, fb)
-    for i in range(RING_FRAMES // 64):
-        ring.view(RING_FRAMES, fb)[i * 64:(i + 1) * 64] = packed
-    del base
     pipe = pl.Pipeline(cfg)
     nmom = pipe.out_shape[0]
     out = torch.empty((B, *pipe.out_shape), dtype=torch.float32, device=dev)
@@ -586,12 +561,12 @@ def main():
     del src
     torch.cuda.synchronize()
 
-    def step(s):
+    def step():
         n = cam_dev.process(B, out)
         assert n == B
 
-    for s in range(args.warmup):
-        step(s)
+    for _ in range(args.warmup):
+        step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -602,118 +577,267 @@ def main():
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         e0.record(stream)
-        for s in range(args.steps):
-            step(args.warmup + s)
+        for _ in range(args.steps):
+            step()
         e1.record(stream)
         torch.cuda.synchronize()
     launches = lib.hf_launch_count()
     ms = e0.elapsed_time(e1)
     stages = {k: v for k, v in pipe.stage_times().items() if v[0] > 0}
     pipe.timing(False)
+    window0 = out[0].cpu().numpy().copy()
     cam_dev.close()
     ms = max_over_ranks(ms, world, dev)
-    value = aggregate_rate(world, args.steps, B, ms)
+    res = {"value": round(aggregate_rate(world, args.steps, B, ms), 2), "ms_per_step": round(ms / args.steps, 4),
+           "gpu_launches": int(launches), "clocks": clk.summary(),
+           "stages_ms_per_step": {k: round(v[0] / max(args.steps, 1), 4) for k, v in stages.items()}}
 
-    # roofline of the dominant stage (algorithmic bytes / its CUDA-event time)
+    # roofline of the dominant stage on the critical path (the next batch's eigen phase runs on a
+    # side stream): algorithmic bytes of that stage for the step's windows / its CUDA-event time
     peak, peak_kind = peaks()
     algo = algorithmic_bytes_per_window(nmom)
-    # the dominant stage on the critical path (the next batch's eigen phase runs on a side stream)
     crit = {k: v for k, v in stages.items() if k != "eigen_filter"}
     dom = max(crit, key=lambda k: crit[k][0]) if crit else None
-    roof = None
     if dom:
         per_launch_ms = stages[dom][0] / max(args.steps, 1)
         bytes_launch = algo.get(dom, 0.0) * B
         achieved = bytes_launch / (per_launch_ms / 1000.0) / 1e9
-        tr = traffic_table().get(dom)
-        roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": (tr * B) if tr else None,
-                "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": round(per_launch_ms, 4),
-                "stages_ms_per_step": {k: round(v[0] / max(args.steps, 1), 4) for k, v in stages.items()},
-                "stage_note": "eigen_filter of the next batch runs on a side stream, overlapped"}
+        tr = traffic_table().get(dom) if form == 1 else None
+        res["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                           "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                           "traffic": (tr * B) if tr else None, "algorithmic_bytes_per_launch": bytes_launch,
+                           "ms_per_launch": round(per_launch_ms, 4),
+                           "stage_note": "eigen_filter of the next batch runs on a side stream, overlapped"}
 
-    # end to end through the camera-stream API: pinned host frames in, pinned host moments out.
-    # Each step pushes one step of new frames (B*hop) on a copy stream, reconstructs B windows on
-    # the compute stream and copies their images to the host on the camera stream's copy stream.
-    # Frames are pushed PUSH_AHEAD steps before they are reconstructed (the lookahead Gram pass of
-    # step s reads step s+1's frames), so step s's H2D, step s-2's compute and step s-3's D2H
-    # overlap.  The timed region holds exactly K pushes, K reconstructions and K output copies.
-    e2e = None
-    if not args.no_e2e:
-        PUSH_AHEAD = 2
-        nstep_frames = B * HOP
-        host_frames = torch.empty(nstep_frames * fb, dtype=torch.uint8, pin_memory=True)
-        reps = (nstep_frames + 63) // 64
-        host_frames.view(nstep_frames, fb).copy_(torch.cat([packed] * reps)[:nstep_frames].cpu())
-        host_out = [torch.empty((B, *pipe.out_shape), dtype=torch.float32, pin_memory=True) for _ in range(2)]
-        h2d = torch.cuda.Stream(device=dev)
-        tstream = torch.cuda.Stream(device=dev)
-        cam = pl.CameraStream(pipe, (T - HOP) + (PUSH_AHEAD + 2) * nstep_frames)
-        pushed_at = {}
+    if e2e_on:
+        res["e2e"] = measure_e2e(args, world, dev, pipe, packed, fb, nmom)
+    pipe.close()
+    return res, window0
 
-        def push_step(j):
-            ev = torch.cuda.Event(enable_timing=True)
-            ev.record(h2d)
-            pushed_at[j] = ev
-            cam.push(host_frames, nstep_frames, stream=h2d)
 
-        cam.push(host_frames, T - HOP, stream=h2d)  # prefill: the first window needs T - hop older frames
-        for j in range(PUSH_AHEAD):
-            push_step(j)
-        total = args.warmup + args.steps
-        lat = []
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for s in range(total):
-            if s == args.warmup:
-                torch.cuda.synchronize()
-                if world > 1:
-                    dist.barrier()
-                f0.record(stream)
-                h2d.wait_event(f0)
-            push_step(s + PUSH_AHEAD)
-            n = cam.process(B, host_out[s % 2], stream=stream, async_copy=True)
-            assert n == B
-            cam.output_wait(tstream)
-            b = torch.cuda.Event(enable_timing=True)
-            b.record(tstream)
-            if s >= args.warmup:
-                lat.append((pushed_at[s], b))
-        cam.output_wait(stream)
-        f1.record(stream)
+def measure_e2e(args, world, dev, pipe, packed, fb, nmom):
+    """End to end through the camera-stream API: pinned host frames in, pinned host moments out.
+
+    Throughput leg: each step pushes one step of new frames (B*hop) on a copy stream, reconstructs
+    B windows on the compute stream and copies their images to the host on the camera stream's copy
+    stream.  Frames are pushed PUSH_AHEAD steps before they are reconstructed (the lookahead Gram
+    pass of step s reads step s+1's frames), so step s's H2D, step s-2's compute and step s-3's D2H
+    overlap.  The timed region holds exactly K pushes, K reconstructions and K output copies, with
+    K = max(--steps, 200) so that the latency percentiles rest on enough samples.
+    Unloaded-latency leg: one step at a time (push, reconstruct, copy out, wait), 200 steps: the
+    frame-to-image latency of a step that meets an idle device."""
+    import torch
+    import torch.distributed as dist
+    from holoflow_b200 import pipeline as pl
+    B = args.batch
+    K = max(args.steps, E2E_STEPS)
+    stream = torch.cuda.current_stream()
+    PUSH_AHEAD = 2
+    nstep_frames = B * HOP
+    host_frames = torch.empty(nstep_frames * fb, dtype=torch.uint8, pin_memory=True)
+    reps = (nstep_frames + 63) // 64
+    host_frames.view(nstep_frames, fb).copy_(torch.cat([packed] * reps)[:nstep_frames].cpu())
+    host_out = [torch.empty((B, *pipe.out_shape), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    h2d = torch.cuda.Stream(device=dev)
+    tstream = torch.cuda.Stream(device=dev)
+    cam = pl.CameraStream(pipe, (T - HOP) + (PUSH_AHEAD + 2) * nstep_frames)
+    pushed_at = {}
+
+    def push_step(j):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(h2d)
+        pushed_at[j] = ev
+        cam.push(host_frames, nstep_frames, stream=h2d)
+
+    cam.push(host_frames, T - HOP, stream=h2d)  # prefill: the first window needs T - hop older frames
+    for j in range(PUSH_AHEAD):
+        push_step(j)
+    total = args.warmup + K
+    lat = []
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for s in range(total):
+        if s == args.warmup:
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            f0.record(stream)
+            h2d.wait_event(f0)
+        push_step(s + PUSH_AHEAD)
+        n = cam.process(B, host_out[s % 2], stream=stream, async_copy=True)
+        assert n == B
+        cam.output_wait(tstream)
+        b = torch.cuda.Event(enable_timing=True)
+        b.record(tstream)
+        if s >= args.warmup:
+            lat.append((pushed_at[s], b))
+    cam.output_wait(stream)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ems = max_over_ranks(f0.elapsed_time(f1), world, dev)
+    cam.close()
+
+    def pct(v, q):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(round(q * (len(v) - 1))))]
+
+    step_lat = [a.elapsed_time(b) for a, b in lat]
+    # unloaded latency: nothing queued ahead of a step
+    cam = pl.CameraStream(pipe, (T - HOP) + 2 * nstep_frames)
+    cam.push(host_frames, T - HOP, stream=h2d)
+    idle = []
+    for s in range(args.warmup + E2E_STEPS):
         torch.cuda.synchronize()
-        ems = max_over_ranks(f0.elapsed_time(f1), world, dev)
-        step_lat = sorted(a.elapsed_time(b) for a, b in lat)
-        p50 = step_lat[len(step_lat) // 2]
-        p99 = step_lat[min(len(step_lat) - 1, int(round(0.99 * (len(step_lat) - 1))))]
-        e2e = {"value": round(aggregate_rate(world, args.steps, B, ems), 2), "unit": "images/s",
-               "h2d_bytes_per_step": nstep_frames * fb, "d2h_bytes_per_step": B * nmom * H * W * 4,
-               "ms_per_step": round(ems / args.steps, 4),
-               "latency_ms_p50": round(p50, 3), "latency_ms_p99": round(p99, 3),
-               "latency_definition": "start of the H2D push of a step's new frames (pinned host) to its "
-                                     "moment images in pinned host memory; frames are pushed 2 steps ahead "
-                                     "(H2D, compute and D2H of different steps overlap)"}
-        cam.close()
+        a = torch.cuda.Event(enable_timing=True)
+        a.record(h2d)
+        cam.push(host_frames, nstep_frames, stream=h2d)
+        cam.process(B, host_out[0], stream=stream, async_copy=True)
+        cam.output_wait(tstream)
+        b = torch.cuda.Event(enable_timing=True)
+        b.record(tstream)
+        torch.cuda.synchronize()
+        if s >= args.warmup:
+            idle.append(a.elapsed_time(b))
+    cam.close()
+    return {"value": round(aggregate_rate(world, K, B, ems), 2), "unit": "images/s",
+            "h2d_bytes_per_step": nstep_frames * fb, "d2h_bytes_per_step": B * nmom * H * W * 4,
+            "steps": K, "ms_per_step": round(ems / K, 4),
+            "latency_ms_p50": round(pct(step_lat, 0.5), 3), "latency_ms_p99": round(pct(step_lat, 0.99), 3),
+            "latency_definition": "start of the H2D push of a step's new frames (pinned host) to its "
+                                  "moment images in pinned host memory; frames are pushed 2 steps ahead "
+                                  "(H2D, compute and D2H of different steps overlap)",
+            "unloaded_latency_ms_p50": round(pct(idle, 0.5), 3), "unloaded_latency_ms_p99": round(pct(idle, 0.99), 3),
+            "unloaded_latency_definition": f"{E2E_STEPS} steps one at a time on an idle device: push of B*hop "
+                                           "new frames, reconstruction of B windows, images in pinned host memory"}
 
-    cpu = None
+
+def config2_errors(dev, oracle_mod):
+    """Config 2 as stated: 1024^2 x 64 frames with a rank-2 global clutter at SCR 0, -20, -40 dB
+    (device-generated), top-4 clutter removal; each form's M0/M1/M2 relative L2 error against the
+    FP64 oracle, which is the checker here and runs outside any timed region."""
+    import numpy as np
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    from holoflow_b200 import synth as sy
+    O = oracle_mod
+    out = {}
+    ocfg = O.PathConfig(H, W, T, HOP, Z0, Z1, fs=FS, z=0.25, clutter_rank=RANK_CLUTTER)
+    for scr in (0.0, -20.0, -40.0):
+        fr = sy.DeviceInterferograms(sy.config2_scene(scr), device=dev).frames(0, T)
+        ring = pl.pack12(fr.reshape(-1))
+        host = fr.cpu().numpy().view(np.uint16)
+        exp = O.reconstruct_window(host, ocfg)
+        row = {}
+        for name, form in (("chosen", hf.HF_FORM_CHOSEN), ("plain", hf.HF_FORM_PLAIN)):
+            p = pl.Pipeline(config1_cfg(form, 1))
+            got = p.run(ring, T, 0, 1).cpu().numpy()[0]
+            p.close()
+            row[name] = [float("%.3e" % O.rel_l2(got[m], exp[m])) for m in range(3)]
+        out[f"{scr:+.0f}dB"] = row
+        del fr, ring
+    return out
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if args.workload == "batched":
+        if rank == 0:
+            print(json.dumps(run_batched(args, local)), flush=True)
+        return None
+    if args.workload == "autofocus":
+        return run_autofocus(args, local) if rank == 0 else None
+    if args.workload == "serve":
+        if rank == 0:
+            print(json.dumps(serve_pair(args, local)), flush=True)
+        return None
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    from holoflow_b200 import synth as sy
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    B = args.batch
+    # synthetic frames: 64 distinct frames generated on the device, tiled over the ring
+    gen = sy.DeviceInterferograms(sy.config1_scene(acquisition=rank), device=dev)
+    base = gen.frames(0, 64)
+    packed = pl.pack12(base.reshape(-1)).view(64, config1_cfg(1, B).frame_bytes)
+    base_host = base.cpu().numpy().view(np.uint16).copy()
+    del base, gen
+
+    forms = ["chosen", "plain"] if args.form == "both" else [args.form]
+    results, windows = {}, {}
+    for f in forms:
+        code = hf.HF_FORM_CHOSEN if f == "chosen" else hf.HF_FORM_PLAIN
+        results[f], windows[f] = measure_form(args, world, dev, local, code, packed, e2e_on=not args.no_e2e)
+    head = forms[0]
+    r = results[head]
+
+    # the FP64 oracle as the checker (outside every timed region, rank 0 at N = 1): moment errors
+    # of the last timed step's first window, and the CPU baseline timed on the same window
+    cpu, merr, cfg2 = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, dt, cores = cpu_baseline()
-        cpu = {"value": round(v, 4), "unit": "images/s", "cores": cores, "kind": "port",
-               "sample": "1 full config-1 window (64 x 1024^2), float64 NumPy/SciPy oracle port, %.2f s" % dt}
+        from oracle import oracle as O
+        ocfg = O.PathConfig(H, W, T, HOP, Z0, Z1, fs=FS, z=0.25, clutter_rank=RANK_CLUTTER)
+        exp = O.reconstruct_window(base_host, ocfg)  # also warms the FFT plans and thread pools
+        merr = {f: [float("%.3e" % O.rel_l2(windows[f][m], exp[m])) for m in range(3)] for f in forms}
+        t0 = time.perf_counter()
+        O.reconstruct_window(base_host, ocfg)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(1.0 / dt, 4), "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": "1 full config-1 window (64 x 1024^2, the bench's own frames), float64 NumPy/SciPy "
+                         "oracle port, %.2f s" % dt}
+        if not args.no_extra:
+            cfg2 = config2_errors(dev, O)
+
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_extra and args.form == "both":
+        torch.cuda.empty_cache()
+        extra["config3_batched"] = run_batched(args, local, steps=min(args.steps, 10))
+        torch.cuda.empty_cache()
+        extra["config4_serve"] = serve_pair(args, local)
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "images/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "metric": METRIC, "value": r["value"], "unit": "images/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[head],
             "data": "synthetic (device-generated interferograms, seeded)",
-            "config": {"workload": WORKLOAD, "form": "chosen" if form else "plain",
-                       "windows_per_step": B, "ring_frames": RING_FRAMES,
+            "config": {"workload": WORKLOAD, "form": head, "windows_per_step": B, "ring_frames": RING_FRAMES,
                        "l2": "inputs larger than L2 (403 MB frame ring + 235 MB band planes per window)",
                        "parallelism": f"replicas x{world}"},
-            "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clk.summary(),
+            "gpu_launches": r["gpu_launches"], "roofline": r.get("roofline"), "cpu_baseline": cpu,
+            "e2e": r.get("e2e"), "clocks": r["clocks"], "stages_ms_per_step": r["stages_ms_per_step"],
         }
+        if "plain" in results and head != "plain":
+            p = results["plain"]
+            line["plain"] = {"value": p["value"], "ms_per_step": p["ms_per_step"], "dtype": DTYPE["plain"],
+                             "stages_ms_per_step": p["stages_ms_per_step"], "roofline": p.get("roofline"),
+                             "e2e": p.get("e2e"), "clocks": p["clocks"], "gpu_launches": p["gpu_launches"]}
+            line["chosen_over_plain"] = round(r["value"] / p["value"], 3)
+            if r.get("e2e") and p.get("e2e"):
+                line["chosen_over_plain_e2e"] = round(r["e2e"]["value"] / p["e2e"]["value"], 3)
+        if merr:
+            line["moment_error"] = {"metric": "relative L2 of M0/M1/M2 vs the FP64 oracle, last timed step's "
+                                              "first window", **merr}
+        if cfg2:
+            line["config2_moment_error"] = {"workload": "config2: config 1 + rank-2 global clutter, 1024^2 x 64, "
+                                                        "top-4 removal; relative L2 of M0/M1/M2 vs FP64 oracle",
+                                            **cfg2}
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

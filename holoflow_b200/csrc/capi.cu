@@ -114,7 +114,8 @@ int hf_covariance(const void *in, int in_dtype, int64_t batch, int T, int64_t P,
   HF_CHECK_ARG(real_fmt(in_dtype), "hf_covariance: unsupported dtype");
   HF_CHECK_ARG(in_dtype != HF_MONO12P || P % 2 == 0, "hf_covariance: packed frames need even P");
   FrameRing fr{reinterpret_cast<const uint8_t *>(in), batch * T, 0, T, frame_bytes_of(in_dtype, P)};
-  const bool tiled = (T == 32 || T == 64 || T == 128) && P % 8 == 0 && fr.frame_bytes % 4 == 0;
+  const bool tiled = (T == 32 || T == 64 || T == 128) && P % 8 == 0 && fr.frame_bytes % 4 == 0 &&
+                     ((uintptr_t)in & 3) == 0;
   if (tiled)
     HF_CHECK_ARG(ws != nullptr, "hf_covariance: workspace required");
   return launch_covariance(fr, in_dtype, T, P, (int)batch, ws, gram, s);

@@ -48,17 +48,20 @@ void note_launch(int n = 1);
 
 constexpr int kNumSMs = 148; // B200: 2 dies x 74 SMs; grids are sized in multiples of this.
 
+// SM count of the current device, cached per device ordinal (grid splits depend on it, so a thread
+// that switches devices must see each device's own count).
 inline int sm_count() {
-  static thread_local int cached = 0;
-  if (cached == 0) {
-    int dev = 0, n = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0)
-      cached = n;
-    else
-      cached = kNumSMs;
+  constexpr int kMaxDev = 64;
+  static thread_local int cached[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev)
+    return kNumSMs;
+  if (cached[dev] == 0) {
+    int n = 0;
+    cached[dev] = (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0) ? n
+                                                                                                          : kNumSMs;
   }
-  return cached;
+  return cached[dev];
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -233,7 +233,8 @@ template <int FMT> int launch_simple(const BandArgs &a, int nwin, cudaStream_t s
 int launch_band_dft(const BandArgs &a, int fmt, int nwin, cudaStream_t s) {
   HF_CHECK_ARG(a.T > 0 && a.P > 0 && a.nz > 0 && nwin > 0, "band_dft: empty problem");
   const bool tiled_ok = (a.P % kBandPX == 0) && (a.W % kBandPX == 0) && ((a.OW * 8) % 16 == 0) &&
-                        (a.ox % 2 == 0) && (a.ring.frame_bytes % 4 == 0);
+                        (a.ox % 2 == 0) && (a.ring.frame_bytes % 4 == 0) &&
+                        (((uintptr_t)a.ring.base & 3) == 0); // 4-byte cp.async copies of frame words
   if (tiled_ok) {
     int rc = HF_ERR_UNSUPPORTED;
     switch (fmt) {

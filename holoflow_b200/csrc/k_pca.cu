@@ -231,7 +231,8 @@ template <int FMT>
 int launch_cov_fmt(const FrameRing &ring, int T, int64_t P, int nwin, void *ws, double *gram,
                    cudaStream_t s) {
   if constexpr (FMT != HF_CF32) {
-    const bool tiled = (P % 8 == 0) && (ring.frame_bytes % 4 == 0);
+    // the tiled kernel reads frames as 4-byte words: the base must be 4-byte aligned too
+    const bool tiled = (P % 8 == 0) && (ring.frame_bytes % 4 == 0) && (((uintptr_t)ring.base & 3) == 0);
     if (tiled && T == 32)
       return launch_cov_tiled<FMT, 32>(ring, P, nwin, ws, gram, s);
     if (tiled && T == 64)
@@ -630,8 +631,9 @@ int cov_fixed_tiled(const FrameRing &ring, int64_t P, int nwin, void *ws, double
 
 template <int FMT>
 int cov_fixed_fmt(const FrameRing &ring, int T, int64_t P, int nwin, double *gram, cudaStream_t s) {
-  const bool tiled = (P % 8 == 0) && (ring.frame_bytes % 4 == 0) && (T == 32 || T == 64 || T == 128);
-  if (!tiled) { // the direct kernel needs no workspace
+  const bool tiled = (P % 8 == 0) && (ring.frame_bytes % 4 == 0) && (((uintptr_t)ring.base & 3) == 0) &&
+                     (T == 32 || T == 64 || T == 128);
+  if (!tiled) { // the direct kernel needs no workspace (and takes any alignment)
     cov_generic_kernel<FMT><<<dim3((T * T + 127) / 128, nwin), 128, 0, s>>>(ring, T, P, gram);
     note_launch();
     return launch_status("cov_generic_kernel");

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass
+from typing import Optional
 
 import torch
 
@@ -27,6 +28,7 @@ class Scene:
     tilt_deg: float = 1.5
     f_max: float = 18e3
     seed: int = 1000
+    scr_db: Optional[float] = None  # rank-2 global clutter at this signal-to-clutter ratio (None = off)
 
 
 class DeviceInterferograms:
@@ -57,6 +59,27 @@ class DeviceInterferograms:
         fd = torch.fft.ifft2(torch.fft.fft2(noise) * gy[:, None] * gx[None, :]).real
         self.fd = (fd - fd.min()) / torch.clamp(fd.max() - fd.min(), min=1e-30) * scene.f_max
         self._g = torch.Generator(device=self.dev).manual_seed(scene.seed * 7919 + 13)
+        self.clutter = None
+        if scene.scr_db is not None:
+            # rank-2 clutter K_t = a(t) G1 + b(t) G2: smooth complex spatial patterns (sigma = side/8)
+            # of unit rms, and slow complex processes a, b made of four tones below 500 Hz
+            sc = max(H, W) / 8.0
+            cy = torch.exp(-0.5 * (torch.fft.fftfreq(H, device=self.dev, dtype=torch.float64) * 2 * math.pi * sc) ** 2)
+            cx = torch.exp(-0.5 * (torch.fft.fftfreq(W, device=self.dev, dtype=torch.float64) * 2 * math.pi * sc) ** 2)
+
+            def smooth_noise():
+                n = torch.randn((H, W), generator=g, device=self.dev, dtype=torch.float64)
+                return torch.fft.ifft2(torch.fft.fft2(n) * cy[:, None] * cx[None, :]).real
+
+            pats = []
+            for _ in range(2):
+                p = torch.complex(smooth_noise(), smooth_noise())
+                pats.append(p / torch.sqrt(torch.mean(torch.abs(p) ** 2)))
+            gt = torch.Generator(device="cpu").manual_seed(scene.seed * 31 + 7)
+            tones = [(torch.rand(4, generator=gt, dtype=torch.float64) * 500.0,
+                      torch.rand(4, generator=gt, dtype=torch.float64) * 2 * math.pi,
+                      0.5 + 0.5 * torch.rand(4, generator=gt, dtype=torch.float64)) for _ in range(2)]
+            self.clutter = (pats, tones, 10.0 ** (-scene.scr_db / 20.0))
 
     def frames(self, t0: int, n: int) -> torch.Tensor:
         """uint16 values in an int16 tensor [n, H, W] for absolute times t0 .. t0+n-1."""
@@ -64,6 +87,14 @@ class DeviceInterferograms:
         out = torch.empty((n, s.height, s.width), dtype=torch.int16, device=self.dev)
         for i in range(n):
             ot = self.o0 * torch.exp(1j * 2 * math.pi * self.fd * ((t0 + i) / s.fs))
+            if self.clutter is not None:
+                pats, tones, scale = self.clutter
+                t = (t0 + i) / s.fs
+                for p, (f, ph, a) in zip(pats, tones):
+                    tone = sum(float(ai) * complex(math.cos(2 * math.pi * float(fi) * t + float(pi)),
+                                                   math.sin(2 * math.pi * float(fi) * t + float(pi)))
+                               for fi, pi, ai in zip(f, ph, a))
+                    ot = ot + scale * (1.0 + 0.5 * tone / len(f)) * p
             inten = torch.abs(self.ref + ot) ** 2
             inten = (inten * (2048.0 / inten.mean())).to(torch.float32)
             noisy = torch.poisson(inten, generator=self._g)
@@ -73,6 +104,11 @@ class DeviceInterferograms:
 
 def config1_scene(height=1024, width=1024, acquisition=0) -> Scene:
     return Scene(height, width, 67e3, int(round(900 * width / 1024)), 0.25, seed=1000 + 1 + 17 * acquisition)
+
+
+def config2_scene(scr_db: float, height=1024, width=1024) -> Scene:
+    """Config 1's scene with a rank-2 global phase/amplitude clutter at `scr_db` dB."""
+    return Scene(height, width, 67e3, int(round(900 * width / 1024)), 0.25, seed=1000 + 2, scr_db=scr_db)
 
 
 def config0_scene(acquisition=0) -> Scene:

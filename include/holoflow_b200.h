@@ -91,7 +91,8 @@ int hf_temporal_dft(const void *in, int in_dtype, int64_t batch, int T, int64_t 
 /* ---- a8: PCA / SVD clutter filter (PcaTask, holotask/src/syncs/pca.cc:68-119) -------------
  * hf_covariance: gram[b] = X_b^T X_b (T x T, float64, row-major, symmetric), X_b = [T][P] frames
  * of in_dtype (HF_U8, HF_U16, HF_MONO12P, HF_F32).  No centring, no 1/N (pca.cc:92-98).
- * `ws` must hold hf_covariance_workspace_bytes(T, P) bytes per batch item. */
+ * `ws` must hold hf_covariance_workspace_bytes(T, P) bytes per batch item (it may be NULL when
+ * `in` is not 4-byte aligned: such input takes the direct kernel, which needs no workspace). */
 size_t hf_covariance_workspace_bytes(int T, int64_t P);
 int    hf_covariance(const void *in, int in_dtype, int64_t batch, int T, int64_t P, double *gram,
                      void *ws, hf_stream_t s);
@@ -105,7 +106,10 @@ int    hf_covariance(const void *in, int in_dtype, int64_t batch, int T, int64_t
  * The workspace is a fixed HF_COVARIANCE_NOALLOC_SCRATCH_BYTES array inside the library, one per
  * device, reserved when the library's device code is loaded.  Nothing in it has to start at zero.
  *  - The first call on a device (made with that device current) looks up the array's address
- *    and caches it; make that first call before any stream capture on that device.
+ *    and caches it; make that first call before any stream capture on that device.  The cached
+ *    address belongs to the device's primary context: after cudaDeviceReset on that device it is
+ *    stale, so a process that resets a device must not call this function on it again.
+ *  - `in` may have any alignment: a base that is not 4-byte aligned takes the direct kernel.
  *  - A batch whose partial sums cannot fit (batch x one CTA's partials, T*T*4*G + T*8 bytes with
  *    G = 4, 2, 1 for T = 32, 64, 128) is rejected with HF_ERR_INVALID; larger problems are split
  *    over fewer CTAs so that they fit, which can change the float32 rounding of the partials.

@@ -7,7 +7,7 @@ Doppler path's tensors (frames x pixels, band bins, moment weights), and stores 
 and outputs.  The tests then pin this repository's oracle and CUDA kernels to those outputs
 without needing the reference at run time.
 
-    python tests/golden/make_golden.py [path/to/reference]     # default: /root/reference
+    python tests/golden/make_golden.py path/to/reference
 """
 import importlib.util
 import json
@@ -64,7 +64,9 @@ def cases(rng):
 
 
 def main():
-    root = pathlib.Path(sys.argv[1]) if len(sys.argv) > 1 else pathlib.Path("/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py path/to/reference")
+    root = pathlib.Path(sys.argv[1])
     ref = load_reference_oracle(root)
     rng = np.random.default_rng(20260)
     store = {}

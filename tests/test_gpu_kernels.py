@@ -132,6 +132,35 @@ def test_covariance(cuda, rng, fmt, T, P):
         assert np.array_equal(g[b], g[b].T)
 
 
+@pytest.mark.parametrize("fmt", ["u16", "u8", "mono12p"])
+def test_misaligned_inputs_take_the_direct_kernels(cuda, rng, fmt):
+    """Frames whose base is only 2-byte (u16) or 1-byte aligned are valid input: the Gram and
+    temporal-DFT entry points route them to kernels without 4-byte word loads and still match."""
+    import torch
+    hf, pl = _hf()
+    B, T, P = 2, 64, 4096
+    top = 256 if fmt == "u8" else 4096
+    x = rng.integers(0, top, (B, T, P))
+    if fmt == "u16":
+        host = x.astype(np.uint16).view(np.int16).reshape(-1)
+        buf = torch.zeros(host.size + 1, dtype=torch.int16, device=cuda)
+        buf[1:] = torch.from_numpy(host).to(cuda)
+        dev, dt = buf[1:], hf.HF_U16              # base at a 2-byte offset
+    else:
+        host = O.pack12(x.astype(np.uint16).reshape(-1)) if fmt == "mono12p" else x.astype(np.uint8).reshape(-1)
+        buf = torch.zeros(host.size + 3, dtype=torch.uint8, device=cuda)
+        buf[3:] = torch.from_numpy(host).to(cuda)
+        dev, dt = buf[3:], (hf.HF_MONO12P if fmt == "mono12p" else hf.HF_U8)  # 1-byte aligned
+    assert dev.data_ptr() % 4 != 0
+    g = pl.covariance(dev, dt, B, T, P).cpu().numpy()
+    for b in range(B):
+        X = x[b].astype(np.float64)
+        exp = X @ X.T
+        assert np.abs(g[b] - exp).max() / np.abs(exp).max() < 2e-7
+    got = pl.temporal_dft(dev, dt, B, T, P, 4, 32).cpu().numpy()
+    assert rel(got, np.fft.fft(x.astype(np.float64), axis=1)[:, 4:32]) < 1e-5
+
+
 @pytest.mark.parametrize("n", [2, 3, 16, 63, 64, 128])
 def test_jacobi_matches_eigh(cuda, rng, n):
     import torch

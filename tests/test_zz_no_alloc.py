@@ -71,3 +71,26 @@ def test_noalloc_rejects_batches_beyond_the_workspace(cuda, rng):
     pl.covariance_noalloc(dev2, dt2, 1, 64, 8192, g2)
     X = x2[0].astype(np.float64)
     assert np.abs(g2.cpu().numpy()[0] - X @ X.T).max() / np.abs(X @ X.T).max() < 2e-7
+
+
+@pytest.mark.gpu
+def test_noalloc_accepts_a_two_byte_aligned_base(cuda, rng):
+    """A uint16 frame view at an odd element offset is valid input; it takes the direct kernel."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    B, T, P = 2, 64, 8192
+    x = rng.integers(0, 4096, (B, T, P))
+    host = torch.from_numpy(x.astype(np.uint16).view(np.int16).reshape(-1))
+    buf = torch.zeros(host.numel() + 1, dtype=torch.int16, device=cuda)
+    buf[1:] = host.to(cuda)
+    view = buf[1:]
+    assert view.data_ptr() % 4 == 2
+    gram = torch.empty((B, T, T), dtype=torch.float64, device=cuda)
+    for _ in range(2):
+        gram.fill_(-1.0)
+        pl.covariance_noalloc(view, hf.HF_U16, B, T, P, gram)
+        g = gram.cpu().numpy()
+        for b in range(B):
+            X = x[b].astype(np.float64)
+            assert np.abs(g[b] - X @ X.T).max() / np.abs(X @ X.T).max() < 2e-7
