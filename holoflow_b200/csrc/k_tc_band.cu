@@ -116,7 +116,9 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
   // TMEM is allocated in powers of two columns (>= 32): 6 tiles (W = 768) take 512
   constexpr int NCOL   = NTILE * 64 <= 32 ? 32 : (NTILE * 64 <= 128 ? 128 : (NTILE * 64 <= 256 ? 256 : 512));
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // aligned by pointer arithmetic on the shared array, so every derived pointer stays a shared-space
+  // pointer (an integer round trip would turn the accesses into generic ones)
+  uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t *sA   = smem;                                  // NTILE x 16 KB
   uint8_t *sB   = sA + NTILE * kTileBytes;               // W16 hi, then lo: 2 x 64 rows x 128 B
   constexpr int RS = XBuf<N1>::kSize > W ? XBuf<N1>::kSize : W; // gbuf row stride (room for the exchange)

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(128) cov_tc_kernel(CovArgs a, int *status) {
   constexpr int TPT   = T * 16 / 128;  // (frame, 8-pixel group) items per thread per stage
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment of the swizzle atoms
-  uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t  *smem  = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u); // stays a shared-space pointer
   uint64_t *mbar  = reinterpret_cast<uint64_t *>(smem + kTcStages * STAGE);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + kTcStages);
   unsigned long long *ssum = reinterpret_cast<unsigned long long *>(tslot + 2);
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(128) cov_tc_i8_kernel(FrameRing ring, int64_t 
   constexpr int NMB   = R / 128;         // 128-row M-blocks
   constexpr int NCOL  = NMB * R;         // TMEM columns (int32)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t  *smem  = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u); // stays a shared-space pointer
   uint64_t *mbar  = reinterpret_cast<uint64_t *>(smem + kTcStages * STAGE);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + kTcStages);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(GroupCov<FMT, HOP8>::NTHR, 1)
   constexpr int HOP      = 8 * HOP8;
   constexpr uint32_t kHS = FMT == HF_MONO12P ? 0x20202020u : 0x02020202u; // shift / 64 per byte
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t  *smem  = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t  *smem  = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u); // stays a shared-space pointer
   uint8_t  *raw   = smem + G::S * G::STG;
   uint64_t *mbar  = reinterpret_cast<uint64_t *>(raw + (size_t)G::D * G::NT * G::RB); // [S] free
   uint64_t *fullb = mbar + G::S;                                                        // [S] full
