@@ -26,6 +26,7 @@ HF_M0, HF_M1, HF_M2 = 1, 2, 4
 HF_FORM_PLAIN, HF_FORM_CHOSEN = 0, 1
 HF_STFD_LOCAL, HF_STFD_GLOBAL = 0, 1
 HF_STFD_COMPLEX, HF_STFD_MAGNITUDE, HF_STFD_MEAN_MAGNITUDE = 0, 1, 2
+HF_SHSLOPES_SINGLE_REFERENCE, HF_SHSLOPES_FULL_PAIRWISE = 0, 1
 
 
 class HfError(RuntimeError):
@@ -47,6 +48,7 @@ class HfDesc(C.Structure):
         ("autofocus_nb_subaps", C.c_int32), ("autofocus_n_iter", C.c_int32), ("autofocus_n_orders", C.c_int32),
         ("autofocus_orders", C.c_int32 * 9), ("autofocus_roi_radius", C.c_float),
         ("autofocus_keep_outside", C.c_int32), ("autofocus_flatfield_period", C.c_float),
+        ("autofocus_pp_accumulation", C.c_int32), ("autofocus_full_pairwise", C.c_int32),
     ]
 
 
@@ -123,6 +125,9 @@ _PROTOS = {
     "hf_server_ready": (_i64, [_vp, C.c_int]),
     "hf_server_step": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int)]),
     "hf_server_sync": (C.c_int, [_vp]),
+    "hf_server_poll": (C.c_int, [_vp, _vp]),
+    "hf_server_inflight": (C.c_int, [_vp, C.c_int]),
+    "hf_server_reserve": (C.c_int, [_vp, _sz]),
     "hf_server_latencies": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "hf_server_open_count": (C.c_int, [_vp]),
     "hf_multi_create": (C.c_int, [C.c_int, C.POINTER(HfDesc), C.POINTER(_vp)]),
@@ -140,6 +145,12 @@ _PROTOS = {
     "hf_node_execute": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_int)]),
     "hf_node_output_desc": (C.c_int, [_vp, C.c_int, C.POINTER(HfTDesc)]),
     "hf_node_destroy": (C.c_int, [_vp]),
+    "hf_node_output_alias": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
+    "hf_node_is_async": (C.c_int, [_vp]),
+    "hf_node_acquire_input": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "hf_node_try_push": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "hf_node_try_pop": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+    "hf_node_release_output": (C.c_int, [_vp, C.c_int]),
     "hf_fftshift": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.POINTER(_i64), C.c_uint32, _vp]),
     "hf_flatfield_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_float, C.c_float, _vp, C.POINTER(_vp)]),
     "hf_flatfield_is_fourier": (C.c_int, [_vp, C.POINTER(C.c_int)]),
@@ -170,6 +181,11 @@ _PROTOS = {
     "hf_holo_write": (C.c_int, [_vp, _vp, _i64]),
     "hf_holo_finish": (C.c_int, [_vp]),
     "hf_plan_autofocus_coefficients": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "hf_plan_autofocus_reset": (C.c_int, [_vp, _vp]),
+    "hf_autofocus_set_accumulation": (C.c_int, [_vp, C.c_int, _vp]),
+    "hf_autofocus_reset": (C.c_int, [_vp, _vp]),
+    "hf_autofocus_set_slope_mode": (C.c_int, [_vp, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float,
+                                              C.c_float, _vp]),
     "hf_plan_stage_times": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
     "hf_stfd_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
@@ -182,6 +198,9 @@ _PROTOS = {
     "hf_shslopes_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                      C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(HfEllipse), C.c_int, _vp,
                                      C.POINTER(_vp)]),
+    "hf_shslopes_create_mode": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(HfEllipse), C.c_int,
+                                          C.c_int, C.c_int, _vp, C.POINTER(_vp)]),
     "hf_shslopes_active": (C.c_int, [_vp, _vp]),
     "hf_shslopes_exec": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "hf_shslopes_destroy": (C.c_int, [_vp]),

@@ -82,17 +82,22 @@ class ShortTimeFresnel(_Handle):
 
 
 class ShackHartmannSlopes(_Handle):
-    """Single-reference slopes of sub-aperture images [sy, sx, h, w] float32 -> [sy, sx, 2]."""
+    """Slopes of sub-aperture images [sy, sx, h, w] float32 -> [sy, sx, 2]: against the centre
+    sample (mode "single_reference") or from every pair of active samples with the complete-graph
+    Laplacian solve (mode "full_pairwise", pair_batch_size maps at a time)."""
     _destroy = "hf_shslopes_destroy"
 
     def __init__(self, sy: int, sx: int, height: int, width: int, lam: float, dx: float, dy: float, z: float,
                  roi: Sequence[float] = (0.5, 0.5, 0.5, 0.5, 0.0), skip_outside_pupil: bool = True,
-                 sub: Tuple[int, int] = (0, 0), stride: Tuple[int, int] = (0, 0), stream=None):
+                 sub: Tuple[int, int] = (0, 0), stride: Tuple[int, int] = (0, 0), stream=None,
+                 mode: str = "single_reference", pair_batch_size: int = 256):
         super().__init__()
         self.shape = (sy, sx, height, width)
         e = HfEllipse(*[float(v) for v in roi])
-        check(lib().hf_shslopes_create(sy, sx, height, width, sub[0], sub[1], stride[0], stride[1], lam, dx, dy, z,
-                                       C.byref(e), int(skip_outside_pupil), _stream(stream), C.byref(self._h)))
+        m = {"single_reference": 0, "full_pairwise": 1}[mode]
+        check(lib().hf_shslopes_create_mode(sy, sx, height, width, sub[0], sub[1], stride[0], stride[1], lam, dx, dy,
+                                            z, C.byref(e), int(skip_outside_pupil), m, int(pair_batch_size),
+                                            _stream(stream), C.byref(self._h)))
 
     def active(self) -> list:
         buf = (C.c_uint8 * (self.shape[0] * self.shape[1]))()

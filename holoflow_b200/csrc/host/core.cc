@@ -2,6 +2,8 @@
 // holoflow::core surface; tensor.hh, tasks.cc, registry.hh:24-68).
 #include "holoflow_b200/core.hh"
 
+#include <algorithm>
+
 namespace hfb::core {
 
 size_t size_of(DType dtype) noexcept {
@@ -68,11 +70,49 @@ std::unique_ptr<ISyncTask> ISyncTaskFactory::update(std::unique_ptr<ISyncTask> o
   return create(input_descs, jsettings, ctx);
 }
 
+std::unique_ptr<IAsyncTask> IAsyncTaskFactory::update(std::unique_ptr<IAsyncTask> old_task,
+                                                      std::span<const TDesc> input_descs,
+                                                      const nlohmann::json &jsettings, const AsyncCreateCtx &ctx) const {
+  old_task.reset();
+  return create(input_descs, jsettings, ctx);
+}
+
+std::optional<TView> ITask::acquire_input(int) { throw std::out_of_range("Input index out of range"); }
+
+void ITask::release_output(int) { throw std::out_of_range("Output index out of range"); }
+
+void ITask::bind_storage_access(IOStorageAccess *storage_access) {
+  if (storage_access == nullptr)
+    throw std::logic_error("Cannot bind null storage access to task");
+  storage_access_ = storage_access;
+}
+
+IOStorageAccess &ITask::storage_access() {
+  if (storage_access_ == nullptr)
+    throw std::logic_error("Storage access not bound to task");
+  return *storage_access_;
+}
+
 void Registry::register_sync(const Key &kind, SyncPtr factory) {
-  if (sync_factories_.count(kind))
+  if (sync_factories_.count(kind) || async_factories_.count(kind))
     throw std::invalid_argument("Registry: kind '" + kind + "' is already registered");
   sync_factories_.emplace(kind, std::move(factory));
 }
+
+void Registry::register_async(const Key &kind, AsyncPtr factory) {
+  if (sync_factories_.count(kind) || async_factories_.count(kind))
+    throw std::invalid_argument("Registry: kind '" + kind + "' is already registered");
+  async_factories_.emplace(kind, std::move(factory));
+}
+
+const IAsyncTaskFactory &Registry::get_async(const Key &kind) const {
+  auto it = async_factories_.find(kind);
+  if (it == async_factories_.end())
+    throw std::out_of_range("Registry: no asynchronous task of kind '" + kind + "'");
+  return *it->second;
+}
+
+bool Registry::is_async_registered(const Key &kind) const noexcept { return async_factories_.count(kind) != 0; }
 
 const ISyncTaskFactory &Registry::get_sync(const Key &kind) const {
   auto it = sync_factories_.find(kind);
@@ -87,6 +127,9 @@ std::vector<Registry::Key> Registry::kinds() const {
   std::vector<Key> out;
   for (const auto &kv : sync_factories_)
     out.push_back(kv.first);
+  for (const auto &kv : async_factories_)
+    out.push_back(kv.first);
+  std::sort(out.begin(), out.end());
   return out;
 }
 

@@ -150,6 +150,8 @@ void from_json(const nlohmann::json &j, DopplerMomentsSettings &s) {
   opt("pp_pctclip_radius", s.pp_pctclip_radius);
   opt("pp_flatfield", s.pp_flatfield);
   opt("pp_flatfield_cutoff_period_m", s.pp_flatfield_cutoff_period_m);
+  opt("pp_accumulation", s.pp_accumulation);
+  opt("autofocus_use_graph_laplacian", s.autofocus_use_graph_laplacian);
 }
 
 // ================================================================================================
@@ -224,18 +226,6 @@ struct DevBuf {
   template <class T> T *as() const { return static_cast<T *>(p); }
 };
 
-// Batch stride (bytes) over the leading dims [0, last) when they collapse into one uniform
-// stride; `ok` is false otherwise.
-size_t collapse_outer(const TDesc &d, size_t last, bool &ok) {
-  ok = true;
-  if (last == 0)
-    return d.num_bytes();
-  for (size_t i = 0; i + 1 < last; ++i)
-    if (d.strides[i] != d.strides[i + 1] * d.shape[i + 1])
-      ok = false;
-  return d.strides[last - 1];
-}
-
 InferResult sync_result(const TDesc &in, const TDesc &out, std::vector<core::InPlace> in_place = {}) {
   InferResult r;
   r.input_descs   = {in};
@@ -253,12 +243,70 @@ InferResult sync_result(const TDesc &in, const TDesc &out, std::vector<core::InP
 // FresnelDiffraction (fresnel_diffraction.cu:466-668)
 // ================================================================================================
 namespace {
+// How the planes of a transform over axes (ax0, ax1) are launched: the dimensions other than the
+// two axes split into one batch group, a run of them that collapses into a single uniform stride in
+// both the input and the output (the largest such run), and the rest, whose index combinations
+// become one launch each at a byte offset (the batch-group selection of fresnel_diffraction.cu:
+// 130-200, 545-570).
+struct PlaneLaunches {
+  int                  ax0 = 0, ax1 = 0;
+  int64_t              batch = 1;                   // planes per launch
+  int64_t              in_bstride = 0, out_bstride = 0; // elements between planes of a launch
+  std::vector<int64_t> in_off, out_off;              // byte offset of each launch
+};
+
+PlaneLaunches plane_launches(const TDesc &in, const TDesc &out, int ax0, int ax1) {
+  PlaneLaunches pl;
+  pl.ax0 = ax0, pl.ax1 = ax1;
+  const int        rank = (int)in.rank();
+  std::vector<int> outer;
+  for (int d = 0; d < rank; ++d)
+    if (d != ax0 && d != ax1)
+      outer.push_back(d);
+  const auto collapses = [&](int a, int b) {
+    return in.strides[(size_t)a] == in.strides[(size_t)b] * in.shape[(size_t)b] &&
+           out.strides[(size_t)a] == out.strides[(size_t)b] * out.shape[(size_t)b];
+  };
+  size_t best_lo = 0, best_hi = 0; // run outer[best_lo, best_hi)
+  int64_t best = outer.empty() ? 1 : 0;
+  for (size_t lo = 0; lo < outer.size(); ++lo) {
+    int64_t n  = (int64_t)in.shape[(size_t)outer[lo]];
+    size_t  hi = lo + 1;
+    while (hi < outer.size() && collapses(outer[hi - 1], outer[hi]))
+      n *= (int64_t)in.shape[(size_t)outer[hi++]];
+    if (n >= best)
+      best = n, best_lo = lo, best_hi = hi;
+  }
+  const size_t ie = core::size_of(in.dtype), oe = core::size_of(out.dtype);
+  pl.batch        = best;
+  if (best_hi > best_lo) {
+    pl.in_bstride  = (int64_t)(in.strides[(size_t)outer[best_hi - 1]] / ie);
+    pl.out_bstride = (int64_t)(out.strides[(size_t)outer[best_hi - 1]] / oe);
+  }
+  std::vector<int> rest;
+  for (size_t i = 0; i < outer.size(); ++i)
+    if (i < best_lo || i >= best_hi)
+      rest.push_back(outer[i]);
+  pl.in_off.push_back(0), pl.out_off.push_back(0);
+  for (int d : rest) { // every index combination of the remaining dimensions
+    std::vector<int64_t> ni, no;
+    for (size_t k = 0; k < in.shape[(size_t)d]; ++k)
+      for (size_t j = 0; j < pl.in_off.size(); ++j) {
+        ni.push_back(pl.in_off[j] + (int64_t)(k * in.strides[(size_t)d]));
+        no.push_back(pl.out_off[j] + (int64_t)(k * out.strides[(size_t)d]));
+      }
+    pl.in_off.swap(ni), pl.out_off.swap(no);
+  }
+  return pl;
+}
+
 class FresnelTask final : public ISyncTask {
 public:
   hf_fresnel_plan           *plan = nullptr;
   cudaStream_t               stream{};
   FresnelDiffractionSettings s;
   TDesc                      idesc;
+  PlaneLaunches              pl;
   ~FresnelTask() override {
     if (plan)
       hf_fresnel_plan_destroy(plan);
@@ -266,14 +314,13 @@ public:
   OpResult execute(SyncCtx &ctx) override {
     auto      &in = ctx.inputs[0];
     auto      &out = ctx.outputs[0];
-    const auto r  = in.desc.rank();
     const auto ie = core::size_of(in.desc.dtype), oe = core::size_of(out.desc.dtype);
-    bool       ok_i, ok_o;
-    const auto ib = collapse_outer(in.desc, r - 2, ok_i), ob = collapse_outer(out.desc, r - 2, ok_o);
-    hf_ok(hf_fresnel_exec(plan, in.data(), (int64_t)(ib / ie), (int64_t)(in.desc.strides[r - 2] / ie),
-                          (int64_t)(in.desc.strides[r - 1] / ie), out.data(), (int64_t)(ob / oe),
-                          (int64_t)(out.desc.strides[r - 2] / oe), (int64_t)(out.desc.strides[r - 1] / oe), stream),
-          "FresnelDiffraction");
+    const auto a0 = (size_t)pl.ax0, a1 = (size_t)pl.ax1;
+    for (size_t k = 0; k < pl.in_off.size(); ++k)
+      hf_ok(hf_fresnel_exec(plan, in.data() + pl.in_off[k], pl.in_bstride, (int64_t)(in.desc.strides[a0] / ie),
+                            (int64_t)(in.desc.strides[a1] / ie), out.data() + pl.out_off[k], pl.out_bstride,
+                            (int64_t)(out.desc.strides[a0] / oe), (int64_t)(out.desc.strides[a1] / oe), stream),
+            "FresnelDiffraction");
     return OpResult::Ok;
   }
 };
@@ -297,10 +344,6 @@ InferResult FresnelDiffractionFactory::infer(std::span<const TDesc> input_descs,
   check(s.dx > 0.0f, "dx must be positive");
   check(s.dy > 0.0f, "dy must be positive");
   check(s.dx == s.dy, "dx must equal dy");
-  check(ax0 == rank - 2 && ax1 == rank - 1, "this implementation transforms the last two axes only");
-  bool ok;
-  collapse_outer(idesc, idesc.rank() - 2, ok);
-  check(ok, "leading dimensions must collapse into one uniformly strided batch");
   TDesc odesc;
   if (s.output_magnitude)
     odesc = TDesc(idesc.shape, DType::F32, idesc.mem_loc);
@@ -313,14 +356,15 @@ InferResult FresnelDiffractionFactory::infer(std::span<const TDesc> input_descs,
 
 std::unique_ptr<ISyncTask> FresnelDiffractionFactory::create(std::span<const TDesc> input_descs,
                                                              const nlohmann::json &j, const SyncCreateCtx &ctx) const {
-  (void)infer(input_descs, j);
-  auto        t = std::make_unique<FresnelTask>();
-  const auto &d = input_descs[0];
-  const auto  r = d.rank();
-  t->s          = j.get<FresnelDiffractionSettings>();
-  t->idesc      = d;
-  t->stream     = ctx.stream;
-  hf_ok(hf_fresnel_plan_create((int64_t)prod(d.shape, 0, r - 2), (int)d.shape[r - 2], (int)d.shape[r - 1],
+  const auto  inf = infer(input_descs, j);
+  auto        t   = std::make_unique<FresnelTask>();
+  const auto &d   = input_descs[0];
+  t->s            = j.get<FresnelDiffractionSettings>();
+  t->idesc        = d;
+  t->stream       = ctx.stream;
+  const int rank  = (int)d.rank();
+  t->pl = plane_launches(d, inf.output_descs[0], norm_axis(t->s.axes[0], rank), norm_axis(t->s.axes[1], rank));
+  hf_ok(hf_fresnel_plan_create(t->pl.batch, (int)d.shape[(size_t)t->pl.ax0], (int)d.shape[(size_t)t->pl.ax1],
                                hf_dtype(d.dtype), t->s.lambda, t->s.dx, t->s.z, t->s.output_magnitude ? 1 : 0,
                                t->s.skip_phase_shift ? 1 : 0, &t->plan, ctx.stream),
         "FresnelDiffraction");
@@ -835,6 +879,12 @@ DopplerPlan doppler_plan(const Check &check, const TDesc &idesc, const DopplerMo
       check(s.pp_flatfield_cutoff_period_m > 0.f, "flatfield cutoff period and image pitches must be positive");
       d.autofocus_flatfield_period = s.pp_flatfield_cutoff_period_m;
     }
+    // graph_builder.cc:128-146: the dual reader's delayed window with a sliding correction
+    check(s.pp_accumulation > 0, "pp_accumulation must be positive");
+    check(!(s.pp_accumulation > 1 && s.autofocus_nb_iter > 1),
+          "sliding Shack-Hartmann correction only supports one autofocus iteration");
+    d.autofocus_pp_accumulation = s.pp_accumulation;
+    d.autofocus_full_pairwise   = s.autofocus_use_graph_laplacian ? 1 : 0;
   }
   dp.nmom = __builtin_popcount((unsigned)d.moment_mask);
   dp.OH   = d.pad_h ? d.pad_h : d.height;
@@ -1561,7 +1611,7 @@ InferResult ShackHartmannSlopesFactory::infer(std::span<const TDesc> input_descs
   check(s.pair_batch_size > 0, "pair_batch_size must be positive");
   check(!(s.mode == "full_pairwise" && s.output_xcorr_maps), "FullPairwise correlation-map output is not supported");
   if (s.mode == "full_pairwise")
-    throw std::logic_error("ShackHartmannSlopes: FullPairwise mode is not built (single_reference only)");
+    check(in.shape[1] * in.shape[2] >= 2, "FullPairwise mode requires at least two active subapertures");
   std::vector<TDesc> outs{TDesc({1, in.shape[1], in.shape[2], 2}, DType::F32, MemLoc::Device)};
   if (s.output_xcorr_maps)
     outs.emplace_back(in.shape, DType::F32, MemLoc::Device);
@@ -1581,10 +1631,15 @@ std::unique_ptr<ISyncTask> ShackHartmannSlopesFactory::create(std::span<const TD
   const auto      &s = t->settings;
   const hf_ellipse roi{s.correlation_roi.cx, s.correlation_roi.cy, s.correlation_roi.rx, s.correlation_roi.ry,
                        s.correlation_roi.angle};
-  hf_ok(hf_shslopes_create((int)t->idesc.shape[1], (int)t->idesc.shape[2], (int)t->idesc.shape[3],
-                           (int)t->idesc.shape[4], (int)s.subaperture_height, (int)s.subaperture_width, (int)s.stride_y,
-                           (int)s.stride_x, s.lambda, s.dx, s.dy, s.z, &roi, s.skip_subapertures_outside_pupil ? 1 : 0,
-                           ctx.stream, &t->p),
+  // FullPairwise: the complete-graph recovery (shack_hartmann_slopes_full_pairwise.cuh); the
+  // active-count check ("requires at least two active subapertures") runs at create, where the
+  // pupil geometry is built
+  hf_ok(hf_shslopes_create_mode((int)t->idesc.shape[1], (int)t->idesc.shape[2], (int)t->idesc.shape[3],
+                                (int)t->idesc.shape[4], (int)s.subaperture_height, (int)s.subaperture_width,
+                                (int)s.stride_y, (int)s.stride_x, s.lambda, s.dx, s.dy, s.z, &roi,
+                                s.skip_subapertures_outside_pupil ? 1 : 0,
+                                s.mode == "full_pairwise" ? HF_SHSLOPES_FULL_PAIRWISE : HF_SHSLOPES_SINGLE_REFERENCE,
+                                (int)s.pair_batch_size, ctx.stream, &t->p),
         "ShackHartmannSlopes");
   return t;
 }
@@ -1846,6 +1901,7 @@ core::Registry &default_registry() {
   static core::Registry *reg = [] {
     auto *r = new core::Registry();
     register_path_kinds(*r);
+    register_np_kinds(*r);
     return r;
   }();
   return *reg;

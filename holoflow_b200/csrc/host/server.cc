@@ -10,6 +10,13 @@
 // closed between steps joins or leaves the next step.  Each push is timestamped by a CUDA event;
 // a window's frame-to-image latency runs from the push that brought its last frame to the end of
 // the D2H copy of its images.
+//
+// Nothing in the serving loop waits for the whole device.  Plans and rings of the streams come
+// from a server-owned stream-ordered memory pool (cudaMallocFromPoolAsync / cudaFreeAsync on the
+// slot's own stream, the pool keeping freed memory for the next stream), so opening or closing a
+// stream neither synchronises the device nor stalls the batches of the others; completions are
+// observed per batch by querying its event (hf_server_poll), so a step can be issued while earlier
+// batches are still on the device.
 #include <algorithm>
 #include <deque>
 #include <mutex>
@@ -18,6 +25,7 @@
 
 #include "hf_common.cuh"
 #include "holoflow_b200.h"
+#include "host_util.cuh"
 
 using namespace hf;
 
@@ -41,11 +49,13 @@ struct Slot {
   int64_t              pushed = 0, next_win = 0;
   std::deque<PushMark> pushes;
   std::deque<DoneMark> done;
+  int64_t              completed = 0; // windows whose images have reached the host
 };
 } // namespace
 
 struct hf_server {
   size_t              reserve = 0;
+  cudaMemPool_t       mem     = nullptr; // plans and rings of every stream
   std::vector<Slot>   slots;
   std::vector<float>  latencies; // completed windows, ms
   std::vector<cudaEvent_t> pool;  // recycled timing events
@@ -63,12 +73,11 @@ struct hf_server {
 };
 
 static void slot_release(hf_server *srv, Slot &s) {
-  if (s.comp)
-    cudaStreamSynchronize(s.comp);
-  if (s.h2d)
-    cudaStreamSynchronize(s.h2d);
+  for (cudaStream_t q : {s.comp, s.h2d, s.mark}) // this stream's work only, not the device's
+    if (q)
+      cudaStreamSynchronize(q);
   if (s.cam)
-    hf_stream_destroy(s.cam);
+    hf_stream_destroy(s.cam); // pooled: frees on s.comp, waits for its own streams
   if (s.plan)
     hf_plan_destroy(s.plan);
   for (cudaStream_t q : {s.comp, s.h2d, s.mark})
@@ -91,7 +100,56 @@ int hf_server_create(size_t hbm_reserve_bytes, int max_streams, hf_server **out)
     return fail(HF_ERR_NOMEM, "hf_server_create: host allocation failed");
   srv->reserve = hbm_reserve_bytes;
   srv->slots.resize((size_t)max_streams);
+  int dev = 0;
+  cudaMemPoolProps props{};
+  props.allocType     = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  cudaError_t e       = cudaGetDevice(&dev);
+  props.location.id   = dev;
+  if (e == cudaSuccess)
+    e = cudaMemPoolCreate(&srv->mem, &props);
+  uint64_t keep = UINT64_MAX; // freed memory stays in the pool for the next stream
+  if (e == cudaSuccess)
+    e = cudaMemPoolSetAttribute(srv->mem, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (e != cudaSuccess) {
+    if (srv->mem)
+      cudaMemPoolDestroy(srv->mem);
+    delete srv;
+    return cuda_status(e, "hf_server_create: memory pool");
+  }
   *out = srv;
+  return HF_OK;
+}
+
+// Device memory a new stream can use: free device memory plus what the pool holds unused.
+static int available_bytes(hf_server *srv, size_t *avail) {
+  size_t   free_b = 0, total_b = 0;
+  uint64_t reserved = 0, used = 0;
+  HF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  HF_CUDA(cudaMemPoolGetAttribute(srv->mem, cudaMemPoolAttrReservedMemCurrent, &reserved));
+  HF_CUDA(cudaMemPoolGetAttribute(srv->mem, cudaMemPoolAttrUsedMemCurrent, &used));
+  *avail = free_b + (size_t)(reserved > used ? reserved - used : 0);
+  return HF_OK;
+}
+
+int hf_server_reserve(hf_server *srv, size_t bytes) {
+  clear_error();
+  HF_CHECK_ARG(srv != nullptr, "hf_server_reserve: null server");
+  if (bytes == 0)
+    return HF_OK;
+  cudaStream_t q = nullptr;
+  HF_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+  void       *p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, srv->mem, q);
+  if (e == cudaSuccess)
+    e = cudaFreeAsync(p, q);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(q);
+  cudaStreamDestroy(q);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return fail(HF_ERR_NOMEM, "hf_server_reserve: the pool could not reserve " + std::to_string(bytes) + " bytes");
+  }
   return HF_OK;
 }
 
@@ -103,6 +161,10 @@ int hf_server_destroy(hf_server *srv) {
       slot_release(srv, s);
   for (cudaEvent_t e : srv->pool)
     cudaEventDestroy(e);
+  if (srv->mem) {
+    cudaDeviceSynchronize(); // pooled frees are stream-ordered: let them land before the pool goes
+    cudaMemPoolDestroy(srv->mem);
+  }
   delete srv;
   return HF_OK;
 }
@@ -119,24 +181,34 @@ int hf_server_open(hf_server *srv, const hf_desc *desc, int64_t ring_frames, int
     }
   if (k < 0)
     return fail(HF_ERR_NOMEM, "hf_server_open: every stream slot is in use");
-  size_t free_b = 0, total_b = 0;
-  HF_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  if (free_b < srv->reserve)
+  size_t avail = 0;
+  HF_TRY(available_bytes(srv, &avail));
+  if (avail < srv->reserve)
     return fail(HF_ERR_NOMEM, "hf_server_open: free device memory is below the reserve");
   Slot &s = srv->slots[(size_t)k];
   s.d     = *desc;
-  int rc  = hf_plan_create(desc, &s.plan, nullptr);
-  if (rc == HF_OK)
-    rc = hf_stream_create(s.plan, ring_frames, &s.cam);
-  if (rc == HF_OK)
-    rc = cuda_status(cudaStreamCreateWithFlags(&s.comp, cudaStreamNonBlocking), "server stream");
+  int rc  = cuda_status(cudaStreamCreateWithFlags(&s.comp, cudaStreamNonBlocking), "server stream");
   if (rc == HF_OK)
     rc = cuda_status(cudaStreamCreateWithFlags(&s.h2d, cudaStreamNonBlocking), "server stream");
   if (rc == HF_OK)
     rc = cuda_status(cudaStreamCreateWithFlags(&s.mark, cudaStreamNonBlocking), "server stream");
+  if (rc == HF_OK) { // plan and ring from the pool, in the order of this stream's compute stream
+    AllocScope scope(srv->mem, s.comp);
+    rc = hf_plan_create(desc, &s.plan, s.comp);
+    if (rc == HF_OK)
+      rc = hf_stream_create(s.plan, ring_frames, &s.cam);
+  }
+  if (rc == HF_OK) { // pushes on the H2D stream start after the ring exists in stream order
+    cudaEvent_t ev = srv->take_event();
+    rc = ev ? cuda_status(cudaEventRecord(ev, s.comp), "server event") : fail(HF_ERR_CUDA, "server event");
+    if (rc == HF_OK)
+      rc = cuda_status(cudaStreamWaitEvent(s.h2d, ev, 0), "server event");
+    if (ev)
+      srv->pool.push_back(ev);
+  }
   if (rc == HF_OK) {
-    rc = cuda_status(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-    if (rc == HF_OK && free_b < srv->reserve)
+    rc = available_bytes(srv, &avail);
+    if (rc == HF_OK && avail < srv->reserve)
       rc = fail(HF_ERR_NOMEM, "hf_server_open: admitting this stream would leave less free device memory "
                               "than the reserve");
   }
@@ -216,8 +288,68 @@ int hf_server_step(hf_server *srv, float *const *out, int *n_done) {
   return HF_OK;
 }
 
-// Waits for every stream, turns completed batches into per-window latencies and recycles the
-// push marks no pending window needs any more.
+// Turns the completed batches of slot `s` (their events have fired) into per-window latencies,
+// counts their windows and recycles the push marks no pending window needs any more.  Never
+// waits: a batch still on the device stays queued.
+static int collect(hf_server *srv, Slot &s) {
+  while (!s.done.empty()) {
+    DoneMark         &dm = s.done.front();
+    const cudaError_t q  = cudaEventQuery(dm.ev);
+    if (q == cudaErrorNotReady)
+      break;
+    if (q != cudaSuccess)
+      return cuda_status(q, "hf_server_poll: batch event");
+    for (int64_t last : dm.window_last) {
+      // the push that brought frame `last`
+      auto it = std::find_if(s.pushes.begin(), s.pushes.end(), [&](const PushMark &p) { return p.last_frame >= last; });
+      if (it == s.pushes.end())
+        continue;
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, it->ev, dm.ev) == cudaSuccess)
+        srv->latencies.push_back(ms);
+    }
+    s.completed += dm.nwin;
+    srv->pool.push_back(dm.ev);
+    s.done.pop_front();
+  }
+  // pushes whose frames all precede the oldest window still to be delivered are no longer needed
+  const int64_t oldest      = s.done.empty() ? s.next_win : s.next_win - [&] {
+    int64_t n = 0;
+    for (const auto &dm : s.done)
+      n += dm.nwin;
+    return n;
+  }();
+  const int64_t first_needed = oldest * s.d.hop + s.d.frames - 1;
+  while (s.pushes.size() > 1 && s.pushes.front().last_frame < first_needed) {
+    srv->pool.push_back(s.pushes.front().ev);
+    s.pushes.pop_front();
+  }
+  return HF_OK;
+}
+
+int hf_server_poll(hf_server *srv, int64_t *completed) {
+  clear_error();
+  HF_CHECK_ARG(srv != nullptr, "hf_server_poll: null server");
+  for (size_t i = 0; i < srv->slots.size(); ++i) {
+    Slot &s = srv->slots[i];
+    if (s.open)
+      HF_TRY(collect(srv, s));
+    if (completed)
+      completed[i] = s.open ? s.completed : 0;
+  }
+  return HF_OK;
+}
+
+int hf_server_inflight(const hf_server *srv, int id) {
+  if (!srv || id < 0 || id >= (int)srv->slots.size() || !srv->slots[(size_t)id].open)
+    return 0;
+  int n = 0;
+  for (const auto &dm : srv->slots[(size_t)id].done)
+    n += cudaEventQuery(dm.ev) == cudaErrorNotReady ? 1 : 0;
+  return n;
+}
+
+// Waits for every open stream's own CUDA streams (not the device), then collects as poll does.
 int hf_server_sync(hf_server *srv) {
   clear_error();
   HF_CHECK_ARG(srv != nullptr, "hf_server_sync: null server");
@@ -227,25 +359,7 @@ int hf_server_sync(hf_server *srv) {
     HF_CUDA(cudaStreamSynchronize(s.h2d));
     HF_CUDA(cudaStreamSynchronize(s.comp));
     HF_CUDA(cudaStreamSynchronize(s.mark));
-    for (auto &dm : s.done) {
-      for (int64_t last : dm.window_last) {
-        // the push that brought frame `last`
-        auto it = std::find_if(s.pushes.begin(), s.pushes.end(), [&](const PushMark &p) { return p.last_frame >= last; });
-        if (it == s.pushes.end())
-          continue;
-        float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, it->ev, dm.ev) == cudaSuccess)
-          srv->latencies.push_back(ms);
-      }
-      srv->pool.push_back(dm.ev);
-    }
-    s.done.clear();
-    // pushes whose frames all precede the next window to process are no longer needed
-    const int64_t first_needed = s.next_win * s.d.hop + s.d.frames - 1;
-    while (s.pushes.size() > 1 && s.pushes.front().last_frame < first_needed) {
-      srv->pool.push_back(s.pushes.front().ev);
-      s.pushes.pop_front();
-    }
+    HF_TRY(collect(srv, s));
   }
   return HF_OK;
 }

@@ -9,12 +9,37 @@
 
 namespace hf {
 
+// Where plan and camera-stream buffers come from.  By default cudaMalloc / cudaFree; inside an
+// AllocScope with a memory pool, stream-ordered cudaMallocFromPoolAsync / cudaFreeAsync on the
+// scope's stream, which neither synchronise the device nor wait for other streams -- the
+// streaming server opens and closes streams this way while other streams' work runs.
+struct AllocCtx {
+  cudaMemPool_t pool   = nullptr;
+  cudaStream_t  stream = nullptr;
+};
+inline AllocCtx &alloc_ctx() {
+  static thread_local AllocCtx c;
+  return c;
+}
+class AllocScope {
+public:
+  AllocScope(cudaMemPool_t pool, cudaStream_t stream) : saved_(alloc_ctx()) { alloc_ctx() = AllocCtx{pool, stream}; }
+  ~AllocScope() { alloc_ctx() = saved_; }
+  AllocScope(const AllocScope &)            = delete;
+  AllocScope &operator=(const AllocScope &) = delete;
+
+private:
+  AllocCtx saved_;
+};
+
 template <typename T> inline int dev_alloc(T **p, size_t count, size_t &total) {
   *p = nullptr;
   if (count == 0)
     return HF_OK;
-  const size_t bytes = count * sizeof(T);
-  cudaError_t  e     = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+  const size_t    bytes = count * sizeof(T);
+  const AllocCtx &ctx   = alloc_ctx();
+  cudaError_t     e     = ctx.pool ? cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, ctx.pool, ctx.stream)
+                                   : cudaMalloc(reinterpret_cast<void **>(p), bytes);
   if (e != cudaSuccess) {
     *p = nullptr;
     (void)cudaGetLastError();
@@ -25,8 +50,13 @@ template <typename T> inline int dev_alloc(T **p, size_t count, size_t &total) {
 }
 
 template <typename T> inline void dev_free(T *&p) {
-  if (p)
-    cudaFree(p);
+  if (p) {
+    const AllocCtx &ctx = alloc_ctx();
+    if (ctx.pool)
+      cudaFreeAsync(p, ctx.stream);
+    else
+      cudaFree(p);
+  }
   p = nullptr;
 }
 

@@ -431,7 +431,7 @@ __device__ float2 *fft_rows_smem(float2 *a, float2 *b, int pitch, int rows, cons
 // ------------------------------------------------------------------------------------------------
 // Row pass
 // ------------------------------------------------------------------------------------------------
-enum RowMode { ROW_STFD = 0, ROW_XPACK = 1, ROW_CROSS = 2 };
+enum RowMode { ROW_STFD = 0, ROW_XPACK = 1, ROW_CROSS = 2, ROW_PAIR = 3 };
 
 struct Roi {
   float cx, cy, rx, ry, c, s; // c, s: cos and sin of the angle
@@ -463,6 +463,9 @@ struct RowArgs {
   int           h;
   const float2 *spec;
   int           ref_img;
+  // ROW_PAIR: map m of the batch is pair pair0 + m, moving image pair_src, reference pair_dst
+  const int    *pair_src, *pair_dst;
+  int64_t       pair0;
 };
 
 template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_rows_kernel(RowArgs a) {
@@ -492,6 +495,11 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_rows_k
       const int     fy = gy * a.stride_y + j, fx = gx * a.stride_x;
       s_off[r] = (pl * a.H + fy) * (int64_t)a.W + fx;                                  // field row start
       s_aux[r] = a.global_lens ? (int64_t)fy * a.W + fx : (int64_t)j * n;              // lens row start
+    } else if constexpr (MODE == ROW_PAIR) {
+      const int64_t m = row / a.h, pr = a.pair0 + m;
+      s_y[r]   = (int)(row - m * a.h);
+      s_off[r] = ((int64_t)a.pair_src[pr] * a.h + s_y[r]) * n; // the moving image's row
+      s_aux[r] = ((int64_t)a.pair_dst[pr] * a.h + s_y[r]) * n; // the reference's row
     } else {
       const int64_t im = row / a.h;
       s_y[r]   = (int)(row - im * a.h);
@@ -518,6 +526,9 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_rows_k
         aux[u] = a.lens[s_aux[r] + i];
       } else if constexpr (MODE == ROW_XPACK) {
         ld[u] = make_float2(a.img[row * n + i], 0.f);
+      } else if constexpr (MODE == ROW_PAIR) {
+        ld[u]  = a.spec[s_off[r] + i];
+        aux[u] = a.spec[s_aux[r] + i];
       } else {
         ld[u]  = a.spec[row * n + i];
         aux[u] = a.spec[s_aux[r] + i];
@@ -536,7 +547,7 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_rows_k
         const float d = roi_sq_distance(i, s_y[r], n, a.h, a.roi);
         // (v - mean) * 0.5 (1 + cos(pi sqrt(d))) inside the ellipse, 0 outside
         v = make_float2(d <= 1.0f ? (ld[u].x - a.means[s_off[r]]) * (0.5f * (1.0f + cospif(sqrtf(d)))) : 0.f, 0.f);
-      } else { // ROW_CROSS: unit-magnitude cross power against the reference image's spectrum
+      } else { // ROW_CROSS / ROW_PAIR: unit-magnitude cross power moving x conj(reference)
         const float2 mv = ld[u], rf = aux[u];
         const float2 p   = make_float2(mv.x * rf.x + mv.y * rf.y, mv.y * rf.x - mv.x * rf.y);
         const float  mag = sqrtf(p.x * p.x + p.y * p.y);
@@ -799,6 +810,43 @@ __global__ void __launch_bounds__(kRedThreads) shk_peak_kernel(const float *maps
     const float dxs = parabolic(m[py * w + xm], m[py * w + px], m[py * w + xp]);
     const float dys = parabolic(m[ym * w + px], m[py * w + px], m[yp * w + px]);
     shifts[blockIdx.x] = make_float2(signed_coord(px, w) + dxs, signed_coord(py, h) + dys);
+  }
+}
+
+// FullPairwise: the shifts of a batch of pairs, scaled to slopes, added to rhs[src] and
+// subtracted from rhs[dst] (accumulate_complete_graph_rhs, shack_hartmann_slopes_full_pairwise.cuh:
+// 223-239).  One thread in pair order, so the float32 sums do not depend on scheduling.
+__global__ void shk_pair_rhs_kernel(const float2 *shifts, const int *src, const int *dst, int64_t pair0, int npairs,
+                                    float2 *rhs, float sppx, float sppy) {
+  if (blockIdx.x != 0 || threadIdx.x != 0)
+    return;
+  for (int m = 0; m < npairs; ++m) {
+    const float sx = shifts[m].x * sppx, sy = shifts[m].y * sppy;
+    float2     &a = rhs[src[pair0 + m]], &b = rhs[dst[pair0 + m]];
+    a.x += sx, a.y += sy;
+    b.x -= sx, b.y -= sy;
+  }
+}
+
+// The complete-graph Laplacian solve in the zero-mean gauge (solve_complete_graph_and_scatter,
+// shack_hartmann_slopes_full_pairwise.cuh:241-262): slope_i = rhs_i / N - mean_k (rhs_k / N) over
+// the N active samples, in the reference's float32 order; inactive samples are 0.
+__global__ void shk_pair_solve_kernel(const float2 *rhs, const int *active_dense, int nact, int count, float *slopes) {
+  if (blockIdx.x != 0 || threadIdx.x != 0)
+    return;
+  const float fn = (float)nact;
+  float       mx = 0.f, my = 0.f;
+  for (int i = 0; i < nact; ++i) {
+    mx += rhs[i].x / fn;
+    my += rhs[i].y / fn;
+  }
+  mx /= fn, my /= fn;
+  for (int i = 0; i < 2 * count; ++i)
+    slopes[i] = 0.f;
+  for (int i = 0; i < nact; ++i) {
+    const int d       = active_dense[i];
+    slopes[2 * d]     = rhs[i].x / fn - mx;
+    slopes[2 * d + 1] = rhs[i].y / fn - my;
   }
 }
 
@@ -1194,6 +1242,15 @@ struct hf_shslopes {
   float   *means = nullptr, *maps = nullptr;
   uint8_t *active = nullptr;
   std::vector<uint8_t> active_host;
+  // FullPairwise mode: pairs (i < j) of active samples in the reference's edge order, processed
+  // pair_batch at a time; rhs indexed by active rank, pair_src / pair_dst by dense index into the
+  // spectra and rank into rhs (src_rank / dst_rank)
+  int      mode = 0, nact = 0, pair_batch = 0;
+  int64_t  npairs = 0;
+  int     *pair_src = nullptr, *pair_dst = nullptr, *pair_srank = nullptr, *pair_drank = nullptr;
+  int     *active_dense = nullptr;
+  float2  *pcross = nullptr, *pshift = nullptr, *rhs = nullptr;
+  float   *pmaps = nullptr;
 };
 
 namespace {
@@ -1203,8 +1260,11 @@ void release(hf_shslopes *p) {
   release(p->pw), release(p->ph);
   cudaFree(p->spec), cudaFree(p->cross), cudaFree(p->shifts);
   cudaFree(p->means), cudaFree(p->maps), cudaFree(p->active);
+  cudaFree(p->pair_src), cudaFree(p->pair_dst), cudaFree(p->pair_srank), cudaFree(p->pair_drank);
+  cudaFree(p->active_dense), cudaFree(p->pcross), cudaFree(p->pshift), cudaFree(p->rhs), cudaFree(p->pmaps);
   delete p;
 }
+int shslopes_set_mode(hf_shslopes *p, int mode, int pair_batch_size);
 } // namespace
 
 extern "C" {
@@ -1212,12 +1272,22 @@ extern "C" {
 int hf_shslopes_create(int sy, int sx, int height, int width, int sub_h, int sub_w, int stride_y, int stride_x,
                        float lambda, float dx, float dy, float z, const hf_ellipse *roi, int skip_outside, hf_stream_t s,
                        hf_shslopes **out) {
+  return hf_shslopes_create_mode(sy, sx, height, width, sub_h, sub_w, stride_y, stride_x, lambda, dx, dy, z, roi,
+                                 skip_outside, HF_SHSLOPES_SINGLE_REFERENCE, 256, s, out);
+}
+
+int hf_shslopes_create_mode(int sy, int sx, int height, int width, int sub_h, int sub_w, int stride_y, int stride_x,
+                            float lambda, float dx, float dy, float z, const hf_ellipse *roi, int skip_outside, int mode,
+                            int pair_batch_size, hf_stream_t s, hf_shslopes **out) {
   clear_error();
   HF_CHECK_ARG(out != nullptr, "ShackHartmannSlopesFactory inference error: null argument");
   *out = nullptr;
+  HF_CHECK_ARG(mode == HF_SHSLOPES_SINGLE_REFERENCE || mode == HF_SHSLOPES_FULL_PAIRWISE,
+               "Unknown Shack-Hartmann slope mode");
   HF_CHECK_ARG(sy > 0 && sx > 0, "ShackHartmannSlopesFactory inference error: subaperture grid dimensions must be positive");
-  HF_CHECK_ARG(sy % 2 == 1 && sx % 2 == 1, "ShackHartmannSlopesFactory inference error: subaperture grid dimensions must be "
-                                           "odd for an unambiguous center reference");
+  if (mode == HF_SHSLOPES_SINGLE_REFERENCE)
+    HF_CHECK_ARG(sy % 2 == 1 && sx % 2 == 1, "ShackHartmannSlopesFactory inference error: subaperture grid dimensions "
+                                             "must be odd for an unambiguous center reference");
   HF_CHECK_ARG(height >= 2 && width >= 2, "ShackHartmannSlopesFactory inference error: reconstruction dimensions must be at least 2");
   HF_CHECK_ARG(lambda > 0.f, "ShackHartmannSlopesFactory inference error: wavelength must be > 0");
   HF_CHECK_ARG(dx > 0.f && dy > 0.f, "ShackHartmannSlopesFactory inference error: pixel pitches must be > 0");
@@ -1267,6 +1337,8 @@ int hf_shslopes_create(int sy, int sx, int height, int width, int sub_h, int sub
   if (rc == HF_OK)
     rc = cuda_status(cudaMemcpy(p->active, p->active_host.data(), (size_t)p->count, cudaMemcpyHostToDevice),
                      "ShackHartmannSlopes: active");
+  if (rc == HF_OK && mode == HF_SHSLOPES_FULL_PAIRWISE)
+    rc = shslopes_set_mode(p, mode, pair_batch_size);
   if (rc != HF_OK) {
     release(p);
     return rc;
@@ -1281,6 +1353,59 @@ int hf_shslopes_active(const hf_shslopes *p, uint8_t *active) {
   std::memcpy(active, p->active_host.data(), p->active_host.size());
   return HF_OK;
 }
+
+} // extern "C"
+
+namespace {
+// Switches a created slopes object to `mode`, allocating the pair lists and batch buffers.
+int shslopes_set_mode(hf_shslopes *p, int mode, int pair_batch_size) {
+  HF_CHECK_ARG(mode == HF_SHSLOPES_SINGLE_REFERENCE || mode == HF_SHSLOPES_FULL_PAIRWISE,
+               "Unknown Shack-Hartmann slope mode");
+  HF_CHECK_ARG(pair_batch_size > 0, "ShackHartmannSlopesFactory inference error: pair_batch_size must be positive");
+  if (mode == HF_SHSLOPES_SINGLE_REFERENCE) {
+    p->mode = 0;
+    return HF_OK;
+  }
+  std::vector<int> dense;
+  for (int i = 0; i < p->count; ++i)
+    if (p->active_host[i])
+      dense.push_back(i);
+  const int nact = (int)dense.size();
+  HF_CHECK_ARG(nact >= 2, "ShackHartmannSlopesFactory inference error: FullPairwise mode requires at least two "
+                          "active subapertures");
+  // edges (i, j), i < j over the active ranks, source-major (generate_complete_graph_pairs)
+  const int64_t    npairs = (int64_t)nact * (nact - 1) / 2;
+  std::vector<int> src, dst, srank, drank;
+  for (int i = 0; i < nact; ++i)
+    for (int j = i + 1; j < nact; ++j)
+      src.push_back(dense[i]), dst.push_back(dense[j]), srank.push_back(i), drank.push_back(j);
+  const int    batch = (int)std::min<int64_t>(pair_batch_size, npairs);
+  const size_t px    = (size_t)batch * p->h * p->w;
+  cudaFree(p->pair_src), cudaFree(p->pair_dst), cudaFree(p->pair_srank), cudaFree(p->pair_drank);
+  cudaFree(p->active_dense), cudaFree(p->pcross), cudaFree(p->pshift), cudaFree(p->rhs), cudaFree(p->pmaps);
+  p->pair_src = p->pair_dst = p->pair_srank = p->pair_drank = p->active_dense = nullptr;
+  p->pcross = p->pshift = p->rhs = nullptr;
+  p->pmaps  = nullptr;
+  p->mode   = 0;
+  const struct {
+    int                  **dst;
+    const std::vector<int> *src;
+  } arrays[5] = {{&p->pair_src, &src}, {&p->pair_dst, &dst}, {&p->pair_srank, &srank}, {&p->pair_drank, &drank},
+                 {&p->active_dense, &dense}};
+  for (const auto &a : arrays) {
+    HF_CUDA(cudaMalloc(a.dst, a.src->size() * sizeof(int)));
+    HF_CUDA(cudaMemcpy(*a.dst, a.src->data(), a.src->size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  HF_CUDA(cudaMalloc(&p->pcross, px * sizeof(float2)));
+  HF_CUDA(cudaMalloc(&p->pmaps, px * sizeof(float)));
+  HF_CUDA(cudaMalloc(&p->pshift, (size_t)batch * sizeof(float2)));
+  HF_CUDA(cudaMalloc(&p->rhs, (size_t)nact * sizeof(float2)));
+  p->mode = 1, p->nact = nact, p->npairs = npairs, p->pair_batch = batch;
+  return HF_OK;
+}
+} // namespace
+
+extern "C" {
 
 int hf_shslopes_exec(hf_shslopes *p, const float *images, float *slopes, float *maps, hf_stream_t s) {
   clear_error();
@@ -1298,6 +1423,31 @@ int hf_shslopes_exec(hf_shslopes *p, const float *images, float *slopes, float *
   ColArgs ca{};
   ca.pl = p->ph.pl, ca.h = p->ph.n, ca.tw = p->ph.tw, ca.w = p->w, ca.inv = false, ca.in = p->spec, ca.outc = p->spec;
   HF_TRY(launch_cols<COL_COMPLEX>(ca, p->count, s));
+  if (p->mode == 1) { // FullPairwise: every pair of active samples, pair_batch maps at a time
+    HF_CHECK_ARG(maps == nullptr, "ShackHartmannSlopes: FullPairwise correlation-map output is not supported");
+    HF_CUDA(cudaMemsetAsync(p->rhs, 0, (size_t)p->nact * sizeof(float2), s));
+    for (int64_t e0 = 0; e0 < p->npairs; e0 += p->pair_batch) {
+      const int nb = (int)std::min<int64_t>(p->pair_batch, p->npairs - e0);
+      RowArgs   rp{};
+      rp.pl = p->pw.pl, rp.n = p->pw.n, rp.tw = p->pw.tw, rp.n_rows = (int64_t)nb * p->h, rp.inv = true;
+      rp.out = p->pcross, rp.spec = p->spec, rp.h = p->h, rp.pair_src = p->pair_src, rp.pair_dst = p->pair_dst;
+      rp.pair0 = e0;
+      HF_TRY(launch_rows<ROW_PAIR>(rp, s));
+      ColArgs cp{};
+      cp.pl = p->ph.pl, cp.h = p->ph.n, cp.tw = p->ph.tw, cp.w = p->w, cp.inv = true, cp.in = p->pcross, cp.outf = p->pmaps;
+      cp.scale = (float)(1.0 / ((double)p->h * p->w)); // inverse_fft_scale
+      HF_TRY(launch_cols<COL_REAL>(cp, nb, s));
+      shk_peak_kernel<<<nb, kRedThreads, 0, s>>>(p->pmaps, p->pshift, p->h, p->w);
+      note_launch();
+      HF_TRY(launch_status("shk_peak_kernel"));
+      shk_pair_rhs_kernel<<<1, 32, 0, s>>>(p->pshift, p->pair_srank, p->pair_drank, e0, nb, p->rhs, p->sppx, p->sppy);
+      note_launch();
+      HF_TRY(launch_status("shk_pair_rhs_kernel"));
+    }
+    shk_pair_solve_kernel<<<1, 32, 0, s>>>(p->rhs, p->active_dense, p->nact, p->count, slopes);
+    note_launch();
+    return launch_status("shk_pair_solve_kernel");
+  }
   // cross power against the centre spectrum (fused into the inverse row pass), inverse columns
   RowArgs rb{};
   rb.pl = p->pw.pl, rb.n = p->pw.n, rb.tw = p->pw.tw, rb.n_rows = rows, rb.inv = true, rb.out = p->cross;
@@ -1586,6 +1736,11 @@ struct hf_autofocus {
   hf_flatfield   *ff    = nullptr; // optional high-pass of the sub-aperture images
   float          *m0    = nullptr, *slopes = nullptr, *coeffs = nullptr, *cum_coeffs = nullptr;
   float          *phase = nullptr, *cum_phase = nullptr;
+  // causal sliding average of the sub-aperture images over the last acc_n spectra
+  // (pp_accumulation, graph_builder.cc:348): float32 history [acc_n][m0] and running sum
+  int             acc_n = 1, pass = 0;
+  int64_t         acc_count = 0;
+  float          *acc_hist = nullptr, *acc_sum = nullptr;
 };
 
 namespace {
@@ -1596,6 +1751,7 @@ void release(hf_autofocus *a) {
   hf_flatfield_destroy(a->ff);
   cudaFree(a->m0), cudaFree(a->slopes), cudaFree(a->coeffs), cudaFree(a->cum_coeffs);
   cudaFree(a->phase), cudaFree(a->cum_phase);
+  cudaFree(a->acc_hist), cudaFree(a->acc_sum);
   delete a;
 }
 } // namespace
@@ -1661,6 +1817,51 @@ int hf_autofocus_create(int nz, int height, int width, int nb_subaps, int n_iter
   return HF_OK;
 }
 
+int hf_autofocus_set_accumulation(hf_autofocus *a, int pp_accumulation, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(a != nullptr, "Autofocus: null argument");
+  HF_CHECK_ARG(pp_accumulation > 0, "pp_accumulation must be positive");
+  HF_CHECK_ARG(pp_accumulation == 1 || a->n_iter == 1, "sliding Shack-Hartmann correction only supports one autofocus "
+                                                       "iteration");
+  cudaFree(a->acc_hist), cudaFree(a->acc_sum);
+  a->acc_hist = a->acc_sum = nullptr;
+  a->acc_n = 1, a->acc_count = 0;
+  if (pp_accumulation > 1) {
+    const size_t n = (size_t)a->nb * a->nb * a->sh * a->sw;
+    HF_CUDA(cudaMalloc(&a->acc_hist, (size_t)pp_accumulation * n * sizeof(float)));
+    HF_CUDA(cudaMalloc(&a->acc_sum, n * sizeof(float)));
+    HF_CUDA(cudaMemsetAsync(a->acc_hist, 0, (size_t)pp_accumulation * n * sizeof(float), s));
+    HF_CUDA(cudaMemsetAsync(a->acc_sum, 0, n * sizeof(float), s));
+    a->acc_n = pp_accumulation;
+  }
+  return HF_OK;
+}
+
+int hf_autofocus_reset(hf_autofocus *a, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(a != nullptr, "Autofocus: null argument");
+  a->acc_count = 0;
+  if (a->acc_n > 1) {
+    const size_t n = (size_t)a->nb * a->nb * a->sh * a->sw;
+    HF_CUDA(cudaMemsetAsync(a->acc_hist, 0, (size_t)a->acc_n * n * sizeof(float), s));
+    HF_CUDA(cudaMemsetAsync(a->acc_sum, 0, n * sizeof(float), s));
+  }
+  return HF_OK;
+}
+
+int hf_autofocus_set_slope_mode(hf_autofocus *a, int mode, int pair_batch_size, float roi_radius, int skip_outside,
+                                float lambda, float dx, float z, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(a != nullptr, "Autofocus: null argument");
+  const hf_ellipse roi{0.5f, 0.5f, roi_radius > 0.f ? roi_radius : 0.5f, roi_radius > 0.f ? roi_radius : 0.5f, 0.0f};
+  hf_shslopes     *sl = nullptr;
+  HF_TRY(hf_shslopes_create_mode(a->nb, a->nb, a->sh, a->sw, a->sh, a->sw, a->sh, a->sw, lambda, dx, dx, z, &roi,
+                                 skip_outside, mode, pair_batch_size, s, &sl));
+  release(a->sl);
+  a->sl = sl;
+  return HF_OK;
+}
+
 int hf_autofocus_pupil_radius(const hf_autofocus *a, float *r) {
   clear_error();
   HF_CHECK_ARG(a != nullptr && r != nullptr, "Autofocus: null argument");
@@ -1718,6 +1919,18 @@ int hf_autofocus_destroy(hf_autofocus *a) {
 // ------------------------------------------------------------------------------------------------
 namespace hf {
 namespace {
+// causal_sliding_average_kernel (causal_sliding_average.cu:35-50): in place on the sub-aperture
+// images, sum += x - history[slot], history[slot] = x, x = sum / divisor, in float32.
+__global__ void shk_causal_avg_kernel(float *x, float *hist, float *sum, int64_t n, float divisor) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float v = x[i], old = hist[i];
+    const float s = sum[i] + v - old;
+    hist[i] = v;
+    sum[i]  = s;
+    x[i]    = s / divisor;
+  }
+}
+
 // lens exp(-i phase): the correction folded into the Fresnel lens that the row pass multiplies by
 __global__ void shk_fold_lens_kernel(const float2 *lens, const float *phase, float2 *out, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -1730,6 +1943,7 @@ __global__ void shk_fold_lens_kernel(const float2 *lens, const float *phase, flo
 } // namespace
 
 int autofocus_begin(hf_autofocus *a, cudaStream_t s) {
+  a->pass = 0;
   HF_CUDA(cudaMemsetAsync(a->cum_coeffs, 0, kShkMaxModes * sizeof(float), s));
   HF_CUDA(cudaMemsetAsync(a->cum_phase, 0, (size_t)a->H * a->W * sizeof(float), s));
   return HF_OK;
@@ -1737,6 +1951,16 @@ int autofocus_begin(hf_autofocus *a, cudaStream_t s) {
 
 int autofocus_measure(hf_autofocus *a, const void *planes, cudaStream_t s) {
   HF_TRY(hf_stfd_exec(a->stfd, planes, a->m0, s));
+  if (a->acc_n > 1 && a->pass == 0) { // the first pass of a spectrum enters the sliding average
+    const int64_t n    = (int64_t)a->nb * a->nb * a->sh * a->sw;
+    const int64_t slot = a->acc_count % a->acc_n;
+    const float   div  = (float)std::min<int64_t>(a->acc_count + 1, a->acc_n);
+    shk_causal_avg_kernel<<<grid_1d(n), 256, 0, s>>>(a->m0, a->acc_hist + slot * n, a->acc_sum, n, div);
+    note_launch();
+    HF_TRY(launch_status("shk_causal_avg_kernel"));
+    ++a->acc_count;
+  }
+  ++a->pass;
   if (a->ff) // in place: each pass reads its input only where it writes, or before it writes
     HF_TRY(hf_flatfield_exec(a->ff, a->m0, a->m0, s));
   HF_TRY(hf_shslopes_exec(a->sl, a->m0, a->slopes, nullptr, s));

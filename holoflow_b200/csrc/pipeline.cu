@@ -111,13 +111,23 @@ struct hf_plan {
   hf_autofocus *af       = nullptr;
   float2       *lens_af  = nullptr; // [H][W] lens with the window's correction folded in
   float        *af_coeff = nullptr; // [max_batch][9] coefficients of the last exec
+  // pp_accumulation > 1: the raw band planes of the last af_delay windows of the sequence (the
+  // dual reader's delayed windows), double-buffered so a call can read the old set while it
+  // writes the new one, and the sequence position
+  int           af_delay = 0;
+  float2       *af_hist[2] = {nullptr, nullptr};
+  int64_t       af_seq     = 0;
+  AllocCtx      alloc{}; // where the buffers came from (a pool + stream, or cudaMalloc)
 };
 
 static void plan_free(hf_plan *p) {
+  AllocScope scope(p->alloc.pool, p->alloc.stream); // free the way the buffers were allocated
   hf_autofocus_destroy(p->af);
   p->af = nullptr;
   dev_free(p->lens_af);
   dev_free(p->af_coeff);
+  dev_free(p->af_hist[0]);
+  dev_free(p->af_hist[1]);
   dev_free(p->f2d);
   dev_free(p->lens);
   dev_free(p->tf);
@@ -133,9 +143,7 @@ static void plan_free(hf_plan *p) {
   }
   dev_free(p->status);
   dev_free(p->row_counter);
-  if (p->cov_ws)
-    cudaFree(p->cov_ws);
-  p->cov_ws = nullptr;
+  dev_free(p->cov_ws);
   p->timer.destroy();
 }
 
@@ -271,6 +279,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     rp.IH = d.height, rp.IW = d.width, rp.H = d.height, rp.N = d.width, rp.nplanes = p->nz, rp.inverse = 0;
     rp.out = p->fast ? p->band : p->band2, rp.out_win = win_px, rp.out_plane = p->P, rp.out_row = d.width;
     rp.pre = p->filter2d ? p->lens : nullptr; // the lens, when the band pass could not fuse it
+    int64_t zero_first = 0;                   // leading windows without a delayed window
     if (p->af) {
       // per window: passes 1..n-1 correct the planes in place, the last pass's correction is
       // folded into the lens of the window's row pass (no extra read and write of the planes)
@@ -288,22 +297,51 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
                                 cudaMemcpyDeviceToDevice, s));
       }
       p->timer.end(s, rec);
+      // Window w's correction applies to window w - dl (dl = 0 without pp_accumulation).  The
+      // delayed planes are this batch's raw planes or the kept ones of the previous calls; the
+      // kept set for the next call (the sequence's last dl raw windows) is copied first, since
+      // the row passes below overwrite the raw planes in place.
+      const int  dl   = p->af_delay;
+      const auto seqw = [&](int w) { return p->af_seq + w - dl; }; // sequence index of w's delayed window
+      if (dl > 0)
+        for (int i = 0; i < dl; ++i) { // concatenation (old kept ++ batch), last dl entries
+          const int     idx = nwin + i;
+          const float2 *src = idx < dl ? p->af_hist[0] + (int64_t)idx * win_px : p->band + (int64_t)(idx - dl) * win_px;
+          HF_CUDA(cudaMemcpyAsync(p->af_hist[1] + (int64_t)i * win_px, src, (size_t)win_px * sizeof(float2),
+                                  cudaMemcpyDeviceToDevice, s));
+        }
       rec = p->timer.begin(s, ST_ROWS);
-      for (int w = 0; w < nwin; ++w) { // one row pass per window, each with its own lens
+      // one row pass per window, each with its own lens; in decreasing order, so that the raw
+      // planes a later pass reads as its delayed window (w - dl < w) are not yet overwritten
+      for (int w = nwin - 1; w >= 0; --w) {
+        if (seqw(w) < 0)
+          continue; // no delayed window yet: the images of w are zero (set below)
         RowPass rw = rp;
-        rw.in      = p->band + w * win_px;
+        rw.in      = w >= dl ? p->band + (int64_t)(w - dl) * win_px : p->af_hist[0] + (int64_t)w * win_px;
         rw.out     = rp.out + w * win_px;
         rw.pre     = p->lens_af + (int64_t)w * p->P;
         HF_TRY(launch_row_pass(rw, 1, s));
       }
       p->timer.end(s, rec);
+      std::swap(p->af_hist[0], p->af_hist[1]);
+      zero_first = std::max<int64_t>(0, std::min<int64_t>(nwin, dl - p->af_seq));
+      p->af_seq += nwin;
     } else {
       rec = p->timer.begin(s, ST_ROWS);
       HF_TRY(launch_row_pass(rp, nwin, s));
       p->timer.end(s, rec);
     }
-    if (p->fast)
-      return cols_moments(p, nwin, out, s);
+    // windows whose delayed window precedes the sequence give zero images (after the moments,
+    // which compute every window of the batch)
+    const auto zero_leading = [&]() -> int {
+      if (zero_first > 0)
+        HF_CUDA(cudaMemsetAsync(out, 0, (size_t)zero_first * owin * sizeof(float), s));
+      return HF_OK;
+    };
+    if (p->fast) {
+      HF_TRY(cols_moments(p, nwin, out, s));
+      return zero_leading();
+    }
     ColPass cp{};
     cp.in = rp.out, cp.in_win = win_px, cp.in_plane = p->P, cp.in_row = d.width;
     cp.H = d.height, cp.W = d.width, cp.nplanes = p->nz, cp.inverse = 0;
@@ -319,7 +357,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
         HF_TRY(launch_band_moments(p->band + w * win_px, HF_CF32, p->nz, p->P, mw, d.moment_mask, out + w * owin, s));
     }
     p->timer.end(s, rec);
-    return HF_OK;
+    return zero_leading();
   }
 
   // angular spectrum: rows forward (with placement) -> columns fwd x TF inv -> rows inverse + moments
@@ -353,6 +391,8 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
   clear_error();
   HF_CHECK_ARG(desc != nullptr && out != nullptr, "hf_plan_create: null argument");
   *out = nullptr;
+  HF_CHECK_ARG(alloc_ctx().pool == nullptr || alloc_ctx().stream == stream,
+               "hf_plan_create: a pooled plan must be created on its allocation stream");
   const hf_desc &d = *desc;
   HF_CHECK_ARG(d.height > 0 && d.width > 0, "plan: frame size must be positive");
   HF_CHECK_ARG(d.frames >= 2 && d.frames <= 128, "plan: frames per window must be in [2, 128]");
@@ -387,6 +427,7 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
   hf_plan *p = new (std::nothrow) hf_plan();
   if (!p)
     return fail(HF_ERR_NOMEM, "plan: host allocation failed");
+  p->alloc       = alloc_ctx();
   p->d           = d;
   p->P           = d.height * d.width;
   p->nz          = (d.z_end - d.z_begin) * (d.time_method == HF_TIME_FFT ? 2 : 1);
@@ -424,6 +465,14 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
         rc = fail(HF_ERR_INVALID, "plan: at most 9 autofocus orders");
         break;
       }
+      if (d.autofocus_pp_accumulation < 0) {
+        rc = fail(HF_ERR_INVALID, "pp_accumulation must be positive");
+        break;
+      }
+      if (d.autofocus_pp_accumulation > 1 && std::max(1, d.autofocus_n_iter) > 1) { // graph_builder.cc:143-146
+        rc = fail(HF_ERR_INVALID, "sliding Shack-Hartmann correction only supports one autofocus iteration");
+        break;
+      }
       if ((rc = hf_autofocus_create(p->nz, d.height, d.width, d.autofocus_nb_subaps, std::max(1, d.autofocus_n_iter),
                                     d.lambda, d.pitch, d.z,
                                     d.autofocus_roi_radius > 0.f ? d.autofocus_roi_radius : 0.5f,
@@ -433,6 +482,19 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
       if ((rc = dev_alloc(&p->lens_af, (size_t)(B * p->P), p->bytes)) ||
           (rc = dev_alloc(&p->af_coeff, (size_t)(9 * B), p->bytes)))
         break;
+      if (d.autofocus_full_pairwise &&
+          (rc = hf_autofocus_set_slope_mode(p->af, HF_SHSLOPES_FULL_PAIRWISE, 256,
+                                            d.autofocus_roi_radius > 0.f ? d.autofocus_roi_radius : 0.5f,
+                                            d.autofocus_keep_outside ? 0 : 1, d.lambda, d.pitch, d.z, stream)))
+        break;
+      if (d.autofocus_pp_accumulation > 1) {
+        if ((rc = hf_autofocus_set_accumulation(p->af, d.autofocus_pp_accumulation, stream)))
+          break;
+        p->af_delay = (d.autofocus_pp_accumulation - 1) / 2;
+        const size_t hist = (size_t)p->af_delay * p->nz * p->P;
+        if (hist && ((rc = dev_alloc(&p->af_hist[0], hist, p->bytes)) || (rc = dev_alloc(&p->af_hist[1], hist, p->bytes))))
+          break;
+      }
     }
     const int64_t plane = (int64_t)p->P, oplane = (int64_t)OH * OW;
     if ((rc = dev_alloc(&p->band, (size_t)(B * p->nz * plane), p->bytes)))
@@ -489,8 +551,10 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
     rc = plan_tables(p, stream);
   } while (0);
   if (rc != HF_OK) {
+    const std::string msg = hf_last_error(); // releasing the parts built so far must not erase it
     plan_free(p);
     delete p;
+    set_error(msg);
     return rc;
   }
   *out = p;
@@ -500,7 +564,12 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
 int hf_plan_destroy(hf_plan *p) {
   if (!p)
     return HF_OK;
-  cudaDeviceSynchronize();
+  // a pooled plan waits for its own stream only (its buffers are freed in that stream's order);
+  // otherwise for the device, as cudaFree would
+  if (p->alloc.pool)
+    cudaStreamSynchronize(p->alloc.stream);
+  else
+    cudaDeviceSynchronize();
   plan_free(p);
   delete p;
   return HF_OK;
@@ -565,6 +634,15 @@ int hf_plan_timing(hf_plan *p, int enable) {
   p->timer.on    = enable != 0;
   p->timer.n     = 0;
   p->timer.nexec = 0;
+  return HF_OK;
+}
+
+int hf_plan_autofocus_reset(hf_plan *p, hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(p != nullptr, "hf_plan_autofocus_reset: null argument");
+  p->af_seq = 0;
+  if (p->af)
+    HF_TRY(hf_autofocus_reset(p->af, s));
   return HF_OK;
 }
 
@@ -665,6 +743,7 @@ struct hf_stream {
   bool         d2h_pending[2] = {};
   int          stage_k        = 0;
   int          last_k         = -1;
+  AllocCtx     alloc{}; // where ring and staging came from (a pool + stream, or cudaMalloc)
 };
 
 namespace {
@@ -712,6 +791,7 @@ int hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **out) {
     return fail(HF_ERR_NOMEM, "hf_stream_create: host allocation failed");
   st->plan        = plan;
   st->ring_frames = ring_frames;
+  st->alloc       = alloc_ctx();
   const size_t out_elems = (size_t)plan->d.max_batch * plan->nmom * plan->OH * plan->OW;
   int rc = dev_alloc(&st->ring, (size_t)(ring_frames * plan->frame_bytes), st->bytes);
   for (int k = 0; k < 2 && rc == HF_OK; ++k)
@@ -729,6 +809,8 @@ int hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **out) {
     if (rc == HF_OK)
       rc = cuda_status(cudaEventCreateWithFlags(&st->proc_rec[i].ev, cudaEventDisableTiming), "stream event");
   }
+  if (rc == HF_OK && plan->af) // a camera stream is a new window sequence
+    rc = hf_plan_autofocus_reset(plan, plan->alloc.pool ? plan->alloc.stream : nullptr);
   if (rc != HF_OK) {
     hf_stream_destroy(st);
     return rc;
@@ -740,7 +822,16 @@ int hf_stream_create(hf_plan *plan, int64_t ring_frames, hf_stream **out) {
 int hf_stream_destroy(hf_stream *st) {
   if (!st)
     return HF_OK;
-  cudaDeviceSynchronize();
+  // pooled: wait for this camera stream's own CUDA streams (the caller has synchronised the
+  // streams it pushed and processed on) and free in the allocation stream's order
+  if (st->alloc.pool) {
+    for (cudaStream_t q : {st->side, st->d2h, st->alloc.stream})
+      if (q)
+        cudaStreamSynchronize(q);
+  } else {
+    cudaDeviceSynchronize();
+  }
+  AllocScope scope(st->alloc.pool, st->alloc.stream);
   dev_free(st->ring);
   for (float *&b : st->stage)
     dev_free(b);

@@ -84,8 +84,8 @@ class Node:
 
     def execute(self, inputs: Sequence[Any], outputs: Sequence[Optional[torch.Tensor]]) -> int:
         """Inputs are tensors or raw origin pointers (ints, e.g. another node's output_ptr()).
-        An output the node owns (a cached "Holofile" source) is given as None; its pointer is then
-        available from output_ptr()."""
+        An output the node owns (a cached "Holofile" source) or that views an input (a "Slice") is
+        given as None; its pointer is then available from output_ptr() (see views())."""
         def addr(t):
             return int(t) if isinstance(t, int) else _ptr(t).value
         ins = (C.c_void_p * max(1, len(inputs)))(*[addr(t) for t in inputs])
@@ -93,6 +93,23 @@ class Node:
         r = C.c_int()
         check(lib().hf_node_execute(self._n, ins, outs, C.byref(r)))
         return r.value
+
+    def alias(self, i: int) -> int:
+        """The input that output i views (InferResult::in_place), or -1."""
+        a = C.c_int()
+        check(lib().hf_node_output_alias(self._n, i, C.byref(a)))
+        return a.value
+
+    def view(self, i: int, inputs: Sequence[torch.Tensor]) -> torch.Tensor:
+        """Output i, an in-place view of one of `inputs`, as a torch view of that tensor."""
+        a = self.alias(i)
+        src = inputs[a]
+        d = self.output_desc(i)
+        es = _SIZE[d.dtype]
+        p, _ = self.output_ptr(i)
+        base = src.data_ptr() - src.storage_offset() * src.element_size()
+        return torch.as_strided(src, shape_of(d), tuple(d.strides[k] // es for k in range(d.rank)),
+                                (p - base) // es)
 
     def output_ptr(self, i: int = 0) -> tuple[int, bool]:
         """(origin pointer of output i as of the last execute, whether the node owns it)."""
@@ -112,6 +129,65 @@ class Node:
             pass
 
 
+class _DevPtr:
+    """A raw device pointer with a shape, exposed to torch through __cuda_array_interface__."""
+    _TYPESTR = {0: "|u1", 1: "<i2", 2: "<f4", 3: "<c8"}
+
+    def __init__(self, ptr: int, d: HfTDesc):
+        es = _SIZE[d.dtype]
+        self.__cuda_array_interface__ = {
+            "shape": shape_of(d), "typestr": self._TYPESTR[d.dtype], "data": (ptr, False), "version": 3,
+            "strides": tuple(d.strides[k] for k in range(d.rank)) if any(d.strides[k] for k in range(d.rank)) else None}
+        self.es = es
+
+
+def _wrap(ptr: int, d: HfTDesc) -> torch.Tensor:
+    if d.mem_loc == 1:
+        return torch.as_tensor(_DevPtr(ptr, d), device="cuda")
+    n = 1
+    for k in range(d.rank):
+        n *= d.shape[k]
+    buf = (C.c_char * (n * _SIZE[d.dtype])).from_address(ptr)
+    return torch.frombuffer(buf, dtype=_TORCH[d.dtype]).reshape(shape_of(d))
+
+
+class AsyncNode(Node):
+    """An asynchronous kind (a queue): the producer writes the view acquire_input() returns and
+    calls try_push(); the consumer's try_pop() makes the owned outputs readable (output()) until
+    release_output()."""
+
+    def acquire_input(self, i: int = 0, desc: Optional[HfTDesc] = None) -> Optional[torch.Tensor]:
+        p = C.c_void_p()
+        check(lib().hf_node_acquire_input(self._n, i, C.byref(p)))
+        if not p.value:
+            return None
+        return _wrap(p.value, desc if desc is not None else self.input_descs[i])
+
+    def try_push(self) -> int:
+        r = C.c_int()
+        check(lib().hf_node_try_push(self._n, C.byref(r)))
+        return r.value
+
+    def try_pop(self, outputs: Sequence[Optional[torch.Tensor]] = ()) -> int:
+        outs = (C.c_void_p * 8)(*[None if t is None else _ptr(t).value for t in outputs])
+        r = C.c_int()
+        check(lib().hf_node_try_pop(self._n, outs, C.byref(r)))
+        return r.value
+
+    def output(self, i: int = 0) -> torch.Tensor:
+        p, _ = self.output_ptr(i)
+        return _wrap(p, self.output_desc(i))
+
+    def release_output(self, i: int = 0) -> None:
+        check(lib().hf_node_release_output(self._n, i))
+
+
+def async_node(kind: str, settings: dict[str, Any], descs: Sequence[HfTDesc], stream=None) -> AsyncNode:
+    n = AsyncNode(kind, settings, descs, stream)
+    n.input_descs = list(descs)
+    return n
+
+
 def empty_like_desc(d: HfTDesc, device) -> torch.Tensor:
     return torch.empty(shape_of(d), dtype=_TORCH[d.dtype], device=device)
 
@@ -126,11 +202,12 @@ def run_sync_factory(kind: str, settings: dict[str, Any], inputs: Sequence[torch
         outs = []
         for i in range(n_out):
             d = node.output_desc(i)
-            outs.append(empty_like_desc(d, inputs[0].device if d.mem_loc == 1 else "cpu"))
+            dev = (inputs[0].device if inputs else "cuda") if d.mem_loc == 1 else "cpu"
+            outs.append(None if node.alias(i) >= 0 else empty_like_desc(d, dev))
         r = node.execute(inputs, outs)
         if r != 0:
             raise HfError(r, f"{kind}: execute returned OpResult {r}")
         torch.cuda.synchronize()
-        return outs
+        return [node.view(i, inputs) if o is None else o for i, o in enumerate(outs)]
     finally:
         node.close()

@@ -104,6 +104,8 @@ class PipelineConfig:
     autofocus_roi_radius: float = 0.5
     autofocus_keep_outside: int = 0
     autofocus_flatfield_period: float = 0.0  # pp_flatfield cutoff period [m] on the sub-aperture images
+    autofocus_pp_accumulation: int = 1  # sliding correction over n windows, applied to window w - (n - 1) / 2
+    autofocus_full_pairwise: int = 0    # graph-Laplacian (full pairwise) slopes
 
     def desc(self) -> HfDesc:
         orders = list(self.autofocus_orders)
@@ -113,7 +115,8 @@ class PipelineConfig:
                       self.pad_w, self.pad_h, self.as_filter, self.r_inner, self.r_outer,
                       self.s_inner, self.s_outer, self.time_method, self.autofocus_nb_subaps,
                       self.autofocus_n_iter, len(orders), (C.c_int32 * 9)(*orders), self.autofocus_roi_radius,
-                      self.autofocus_keep_outside, self.autofocus_flatfield_period)
+                      self.autofocus_keep_outside, self.autofocus_flatfield_period,
+                      self.autofocus_pp_accumulation, self.autofocus_full_pairwise)
 
     @property
     def frame_bytes(self) -> int:
@@ -171,6 +174,11 @@ class Pipeline:
         ns, ne = C.c_int(), C.c_int()
         check(lib().hf_plan_stage_times(self._plan, ms, names, C.byref(ns), C.byref(ne)))
         return {names[k].decode(): (ms[k], ne.value) for k in range(ns.value)}
+
+    def autofocus_reset(self, stream=None) -> None:
+        """Starts a new window sequence (pp_accumulation): clears the sliding average and the kept
+        delayed windows."""
+        check(lib().hf_plan_autofocus_reset(self._plan, _stream(stream)))
 
     def autofocus_coefficients(self, w: int = 0) -> torch.Tensor:
         """Window w's Zernike coefficients (radians, autofocus_orders order) of the last run."""

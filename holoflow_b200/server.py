@@ -49,7 +49,23 @@ class Server:
         return {i: done[i] for i in range(self.max_streams) if done[i] > 0}
 
     def sync(self) -> None:
+        """Waits for the server's own streams, then collects (latencies, delivered windows)."""
         check(lib().hf_server_sync(self._s))
+
+    def poll(self) -> dict[int, int]:
+        """Collects the batches whose images have reached the host, without waiting for the others;
+        returns {stream: cumulative windows delivered} for the open streams."""
+        done = (C.c_int64 * self.max_streams)()
+        check(lib().hf_server_poll(self._s, done))
+        return {sid: done[sid] for sid in self.cfgs}
+
+    def inflight(self, sid: int) -> int:
+        """Batches of stream `sid` still on the device."""
+        return lib().hf_server_inflight(self._s, sid)
+
+    def reserve(self, nbytes: int) -> None:
+        """Grows the server's memory pool once, so later streams open without device allocations."""
+        check(lib().hf_server_reserve(self._s, nbytes))
 
     def latencies(self) -> list[float]:
         buf = (C.c_float * 65536)()

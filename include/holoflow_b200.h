@@ -214,6 +214,13 @@ typedef struct hf_desc {
   float   autofocus_roi_radius;  /* correlation ROI radius (pp_pctclip_radius; 0 reads as 0.5) */
   int32_t autofocus_keep_outside; /* 1: keep sub-apertures outside the pupil                   */
   float   autofocus_flatfield_period; /* pp_flatfield cutoff period [m] on the sub-aperture images (0 = off) */
+  /* pp_accumulation (0 or 1: off): the sub-aperture images are averaged causally over the last n
+   * windows and the fit corrects the window d = (n - 1) / 2 earlier, which the plan keeps
+   * (the dual-reader queue's delayed window, dual_reader_batch_queue.cc:214-227; graph_builder.cc:
+   * 128-153).  Output window w is then the corrected window w - d, and the first d windows of a
+   * sequence are zero images.  One pass only.  hf_plan_autofocus_reset starts a new sequence.   */
+  int32_t autofocus_pp_accumulation;
+  int32_t autofocus_full_pairwise; /* 1: graph-Laplacian slopes (autofocus_use_graph_laplacian)   */
 } hf_desc;
 #define HF_TIME_RFFT 0
 #define HF_TIME_FFT 1
@@ -251,6 +258,9 @@ int hf_plan_status(hf_plan *plan, int *status, int reset);
  * autofocus_orders order) of the last hf_pipeline_exec, copied into the device buffer `coeffs`
  * (autofocus_n_orders floats) on stream s. */
 int hf_plan_autofocus_coefficients(hf_plan *plan, int w, float *coeffs, hf_stream_t s);
+/* Starts a new window sequence for autofocus_pp_accumulation: clears the sliding average and the
+ * kept delayed windows (a camera stream does this when it is created). */
+int hf_plan_autofocus_reset(hf_plan *plan, hf_stream_t s);
 
 /* Debug/inspection: after hf_pipeline_exec, copy window `w`'s T x T Gram matrix (float64) and
  * its filter+DFT matrix W (complex64 [T][Nz]) to device buffers (either may be NULL). */
@@ -287,15 +297,18 @@ int     hf_stream_process(hf_stream *stream, int max_windows, float *out, int ou
 int     hf_stream_output_wait(hf_stream *stream, hf_stream_t s, int host_block);
 
 /* ---- streaming server: many camera streams on one GPU, continuous batching -------------------
- * Each open stream owns a plan, a device frame ring and its own CUDA streams.  hf_server_open
- * admits a stream only while the device keeps `hbm_reserve_bytes` free after the stream's buffers
- * are created (else HF_ERR_NOMEM: retry after other streams close).  hf_server_step gives every
+ * Each open stream owns a plan, a device frame ring and its own CUDA streams; plans and rings come
+ * from a server-owned stream-ordered memory pool, so opening and closing never synchronise the
+ * device or stall other streams' batches.  hf_server_open admits a stream only while the device
+ * keeps `hbm_reserve_bytes` available (free, or held unused by the pool) after the stream's
+ * buffers are created (else HF_ERR_NOMEM: retry after other streams close).  hf_server_step gives every
  * open stream with ready windows one batch on its own CUDA stream, so batches of different streams
  * run concurrently; images of stream i go to out[i] (pinned host, [max_batch][n_moments][OH][OW],
  * NULL to skip the stream) and n_done[i] receives the windows done.  out[i] may be read, and a
- * later step may reuse it, once hf_server_sync has returned.  A window's frame-to-image latency
- * (from the push that brought its last frame to its images reaching the host) is collected at
- * hf_server_sync and read by hf_server_latencies. */
+ * later step may reuse it, once hf_server_poll counts the step's windows (or hf_server_sync, which
+ * waits for the server's own streams, has returned).  A window's frame-to-image latency (from the
+ * push that brought its last frame to its images reaching the host) is collected by poll / sync
+ * and read by hf_server_latencies. */
 typedef struct hf_server hf_server;
 int     hf_server_create(size_t hbm_reserve_bytes, int max_streams, hf_server **server);
 int     hf_server_destroy(hf_server *server);
@@ -305,6 +318,15 @@ int     hf_server_push(hf_server *server, int stream_id, const void *frames, int
 int64_t hf_server_ready(const hf_server *server, int stream_id);
 int     hf_server_step(hf_server *server, float *const *out, int *n_done);
 int     hf_server_sync(hf_server *server);
+/* Non-blocking completion: collects every batch whose images have reached the host (latencies
+ * included) without waiting for the others, and writes each slot's cumulative count of delivered
+ * windows into completed[max_streams] (NULL: skip).  A stream's out[i] buffer of a step may be
+ * reused once the windows of that step are counted.  hf_server_inflight: batches of stream `id`
+ * still on the device.  hf_server_reserve: grows the server's memory pool by `bytes` once (plans
+ * and rings of later streams then come from it without new device allocations; synchronous). */
+int     hf_server_poll(hf_server *server, int64_t *completed);
+int     hf_server_inflight(const hf_server *server, int stream_id);
+int     hf_server_reserve(hf_server *server, size_t bytes);
 int     hf_server_latencies(hf_server *server, float *ms, int cap, int *n);
 int     hf_server_open_count(const hf_server *server);
 
@@ -331,8 +353,10 @@ int hf_multi_plan(hf_multi *multi, int i, hf_plan **plan);
 /* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
  * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------
  * Kinds: "FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
- * "Conversion", "FFTShiftNp", "Flatfield", "Filter2D", "PctClip", "Holofile" (the reference's, with its JSON
- * settings keys) and "DopplerMoments" (the fused per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
+ * "Conversion", "FFTShiftNp", "Flatfield", "Filter2D", "PctClip", "Holofile", the autofocus kinds,
+ * the thin holonp kinds "Slice", "Reshape", "Copy", "Concatenate", "Arange", "Multiply", "Abs",
+ * "CausalSlidingAverage", the asynchronous "BatchQueue", "DualReaderBatchQueue", "SlidingAverage"
+ * (the reference's, with its JSON settings keys) and "DopplerMoments" (the fused per-window path).  A descriptor mirrors holoflow::core::TDesc: dtype in DType order (HF_U8,
  * HF_U16, HF_F32, HF_CF32), strides in BYTES (all zero = C-contiguous), mem_loc 1 = device.
  * infer() failures return HF_ERR_INVALID with "<Factory> inference error: ..." in hf_last_error();
  * work is enqueued on the stream given at create/update. */
@@ -364,6 +388,21 @@ int hf_node_output_desc(const hf_node *node, int index, hf_tdesc *out);
  * caller-provided output, the node's own for an owned one); *owned = 1 if the node owns it. */
 int hf_node_output_ptr(const hf_node *node, int index, void **ptr, int *owned);
 int hf_node_destroy(hf_node *node);
+/* In-place outputs (InferResult::in_place, e.g. "Slice" and a viewing "Reshape"): output `index`
+ * is a view of input *input_index (-1: not a view); hf_node_execute takes NULL for it and
+ * hf_node_output_ptr returns the view's origin inside the input. */
+int hf_node_output_alias(const hf_node *node, int index, int *input_index);
+/* Asynchronous kinds (IAsyncTask, tasks.hh:208-250: "BatchQueue", "DualReaderBatchQueue",
+ * "SlidingAverage"), created by hf_node_create with AsyncCreateCtx{s, s}.  The producer takes the
+ * view of owned input `index` to write (*ptr NULL: no room now), then hf_node_try_push publishes it;
+ * the consumer's hf_node_try_pop (op_result 1 = NotReady) hands out owned outputs, read through
+ * hf_node_output_ptr, and takes caller buffers for the outputs the node does not own (NULL entries
+ * for owned ones); hf_node_release_output retires an owned output of the last pop. */
+int hf_node_is_async(const hf_node *node);
+int hf_node_acquire_input(hf_node *node, int index, void **ptr);
+int hf_node_try_push(hf_node *node, int *op_result);
+int hf_node_try_pop(hf_node *node, void *const *outputs, int *op_result);
+int hf_node_release_output(hf_node *node, int index);
 
 /* ---- post-moment display chain (graph_builder.cc:633-676) -------------------------------------
  * The steps between a moment image and the display: fftshift, flatfield, sliding average,
@@ -501,6 +540,17 @@ int hf_shslopes_create(int sy, int sx, int height, int width, int sub_h, int sub
                        hf_stream_t s, hf_shslopes **p);
 int hf_shslopes_active(const hf_shslopes *p, uint8_t *active);
 int hf_shslopes_exec(hf_shslopes *p, const float *images, float *slopes, float *maps, hf_stream_t s);
+/* hf_shslopes_create with a slope recovery mode (ShackHartmannSlopeMode, shack_hartmann_slopes.hh:
+ * 27-31; the graph-Laplacian `autofocus_use_graph_laplacian` switch of graph_builder.cc:359-361).
+ * FULL_PAIRWISE phase-correlates every pair (i < j) of active samples, pair_batch_size maps at a time
+ * (its memory bound), and solves the complete-graph Laplacian in the zero-mean gauge
+ * (shack_hartmann_slopes_full_pairwise.cuh:69-262): it takes any grid with at least two active
+ * samples and gives no correlation maps.  Synchronous (uploads the pair lists). */
+#define HF_SHSLOPES_SINGLE_REFERENCE 0
+#define HF_SHSLOPES_FULL_PAIRWISE 1
+int hf_shslopes_create_mode(int sy, int sx, int height, int width, int sub_h, int sub_w, int stride_y, int stride_x,
+                            float lambda, float dx, float dy, float z, const hf_ellipse *roi, int skip_outside, int mode,
+                            int pair_batch_size, hf_stream_t s, hf_shslopes **p);
 int hf_shslopes_destroy(hf_shslopes *p);
 
 /* ZernikeFromSlopes (holotask/include/holotask/syncs/zernike_from_slopes.hh:27-45): Noll indexes
@@ -544,6 +594,18 @@ typedef struct hf_autofocus hf_autofocus;
 int hf_autofocus_create(int nz, int height, int width, int nb_subaps, int n_iter, float lambda, float dx, float z,
                         float roi_radius, int skip_outside_pupil, const int *indexes, int n_indexes,
                         float flatfield_period, hf_stream_t s, hf_autofocus **a);
+/* pp_accumulation > 1 (graph_builder.cc:128-153, 348): the sub-aperture images of each exec's
+ * first pass enter a causal sliding average over the last pp_accumulation execs (divisor
+ * min(k + 1, n), float32 running sum, causal_sliding_average.cu:35-90) before the slopes; one pass
+ * only.  The caller supplies the delayed spectrum to correct (hf_autofocus_exec's `delayed`).
+ * hf_autofocus_reset clears the average (a new stream).  Both enqueue on s. */
+int hf_autofocus_set_accumulation(hf_autofocus *a, int pp_accumulation, hf_stream_t s);
+int hf_autofocus_reset(hf_autofocus *a, hf_stream_t s);
+/* Slope recovery of the pass: HF_SHSLOPES_SINGLE_REFERENCE or HF_SHSLOPES_FULL_PAIRWISE (the
+ * `autofocus_use_graph_laplacian` switch, graph_builder.cc:359-361) with the same ROI radius,
+ * pupil rule and optics as at create. */
+int hf_autofocus_set_slope_mode(hf_autofocus *a, int mode, int pair_batch_size, float roi_radius,
+                                int skip_outside_pupil, float lambda, float dx, float z, hf_stream_t s);
 int hf_autofocus_pupil_radius(const hf_autofocus *a, float *radius);
 int hf_autofocus_exec(hf_autofocus *a, const void *planes, const void *delayed, void *corrected, hf_stream_t s);
 int hf_autofocus_outputs(const hf_autofocus *a, float *m0, float *slopes, float *coeffs, float *phase, hf_stream_t s);

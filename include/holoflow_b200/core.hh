@@ -3,8 +3,10 @@
 // Holoflow's compiler and tests drive theirs.
 //
 // The types mirror holoflow::core (tensor.hh: DType, MemLoc, Storage, TDesc, TView;
-// tasks.hh:81-304: SyncCtx, OpResult, InPlace, TaskKind, InferResult, SyncCreateCtx, ISyncTask,
-// ITaskFactory, ISyncTaskFactory; registry.hh:24-68: Registry) with the same member names and
+// tasks.hh:81-332: SyncCtx, AsyncPushCtx, AsyncPopCtx, OpResult, IOStorageAccess, ITask (with
+// acquire_input / release_output for owned tensors), ISyncTask, IAsyncTask, InPlace, TaskKind,
+// InferResult, SyncCreateCtx, AsyncCreateCtx, ITaskFactory, ISyncTaskFactory, IAsyncTaskFactory;
+// registry.hh:24-68: Registry) with the same member names and
 // meanings: TDesc strides are in BYTES, infer() throws std::invalid_argument prefixed
 // "<Factory> inference error: ", execute() returns OpResult for control flow only and reports
 // failures by exception.  They live in namespace hfb::core so that a program can link this library
@@ -19,6 +21,7 @@
 #include <map>
 #include <memory>
 #include <nlohmann/json.hpp>
+#include <optional>
 #include <span>
 #include <stdexcept>
 #include <string>
@@ -65,13 +68,39 @@ struct TView {
   bool       is_nullptr() { return storage == nullptr || storage->ptr == nullptr; }
 };
 
+// The reference's event channel types (holoflow_event/router.hh); opaque here: the path's tasks
+// neither emit nor read events, but the context carries them for tasks that do.
+struct EventWriter;
+struct EventReader;
+
 struct SyncCtx {
   std::span<TView>   inputs;
+  std::span<TView>   outputs;
+  std::atomic<bool> *cancelled    = nullptr;
+  EventWriter       *event_writer = nullptr;
+  EventReader       *event_reader = nullptr;
+};
+
+struct AsyncPushCtx {
+  std::span<TView>   inputs;
+  std::atomic<bool> *cancelled = nullptr;
+};
+
+struct AsyncPopCtx {
   std::span<TView>   outputs;
   std::atomic<bool> *cancelled = nullptr;
 };
 
 enum class OpResult : uint8_t { Ok, NotReady, Cancelled, Eof };
+
+// Storage of the tensors a task owns (InferResult::owned_inputs / owned_outputs): the scheduler
+// keeps one Storage per owned tensor and the task points it at its own memory.
+class IOStorageAccess {
+public:
+  virtual ~IOStorageAccess()                                      = default;
+  [[nodiscard]] virtual Storage &owned_input_storage(size_t index)  = 0;
+  [[nodiscard]] virtual Storage &owned_output_storage(size_t index) = 0;
+};
 
 struct InPlace {
   int in_idx;
@@ -93,14 +122,40 @@ struct SyncCreateCtx {
   cudaStream_t stream = static_cast<cudaStream_t>(0);
 };
 
+struct AsyncCreateCtx {
+  cudaStream_t producer_stream = static_cast<cudaStream_t>(0);
+  cudaStream_t consumer_stream = static_cast<cudaStream_t>(0);
+};
+
 class ITask {
 public:
   virtual ~ITask() = default;
+  // An owned input's view to write into before the push (nullopt: no room now).  The defaults
+  // throw std::out_of_range: a task without owned tensors has no such index (tasks.cc).
+  [[nodiscard]] virtual std::optional<TView> acquire_input(int index);
+  // The consumer has finished with owned output `index` of the last pop.
+  virtual void release_output(int index);
+  void         bind_storage_access(IOStorageAccess *storage_access);
+
+protected:
+  // @throw std::logic_error when no storage access is bound
+  [[nodiscard]] IOStorageAccess &storage_access();
+
+private:
+  IOStorageAccess *storage_access_ = nullptr;
 };
 
 class ISyncTask : public ITask {
 public:
   [[nodiscard]] virtual OpResult execute(SyncCtx &ctx) = 0;
+};
+
+// A queue-like task: the producer pushes (after writing its owned inputs), the consumer pops
+// (and later releases the owned outputs); both return NotReady when they cannot proceed now.
+class IAsyncTask : public ITask {
+public:
+  [[nodiscard]] virtual OpResult try_push(AsyncPushCtx &ctx) = 0;
+  [[nodiscard]] virtual OpResult try_pop(AsyncPopCtx &ctx)   = 0;
 };
 
 class ITaskFactory {
@@ -118,19 +173,33 @@ public:
                                             const nlohmann::json &jsettings, const SyncCreateCtx &ctx) const;
 };
 
+class IAsyncTaskFactory : public ITaskFactory {
+public:
+  virtual std::unique_ptr<IAsyncTask> create(std::span<const TDesc> input_descs, const nlohmann::json &jsettings,
+                                             const AsyncCreateCtx &ctx) const = 0;
+  // Default: re-create (tasks.cc).
+  virtual std::unique_ptr<IAsyncTask> update(std::unique_ptr<IAsyncTask> old_task, std::span<const TDesc> input_descs,
+                                             const nlohmann::json &jsettings, const AsyncCreateCtx &ctx) const;
+};
+
 class Registry {
 public:
-  using Key     = std::string;
-  using SyncPtr = std::unique_ptr<ISyncTaskFactory>;
-  // @throw std::invalid_argument if `kind` is already registered
+  using Key      = std::string;
+  using SyncPtr  = std::unique_ptr<ISyncTaskFactory>;
+  using AsyncPtr = std::unique_ptr<IAsyncTaskFactory>;
+  // @throw std::invalid_argument if `kind` is already registered (as either kind of task)
   void register_sync(const Key &kind, SyncPtr factory);
+  void register_async(const Key &kind, AsyncPtr factory);
   // @throw std::out_of_range if `kind` is not registered
-  const ISyncTaskFactory &get_sync(const Key &kind) const;
-  bool                    is_sync_registered(const Key &kind) const noexcept;
-  std::vector<Key>        kinds() const;
+  const ISyncTaskFactory  &get_sync(const Key &kind) const;
+  const IAsyncTaskFactory &get_async(const Key &kind) const;
+  bool                     is_sync_registered(const Key &kind) const noexcept;
+  bool                     is_async_registered(const Key &kind) const noexcept;
+  std::vector<Key>         kinds() const; // both kinds, sorted
 
 private:
-  std::map<Key, SyncPtr> sync_factories_;
+  std::map<Key, SyncPtr>  sync_factories_;
+  std::map<Key, AsyncPtr> async_factories_;
 };
 
 // A CUDA runtime failure inside a task (the reference's curaii::CudaError role).

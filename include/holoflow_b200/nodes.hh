@@ -70,6 +70,8 @@ struct DopplerMomentsSettings {
   float            pp_pctclip_radius = 0.5f;
   bool             pp_flatfield = false;            // flatfield of the sub-aperture images
   float            pp_flatfield_cutoff_period_m = 0.f;
+  int              pp_accumulation = 1;                    // sliding correction over n windows
+  bool             autofocus_use_graph_laplacian = false;  // FullPairwise slopes
 };
 
 // Source node reading a .holo file (holotask/include/holotask/sources/holofile.hh:30-50).
@@ -202,7 +204,39 @@ HFB_SYNC_FACTORY(CorrectPhaseFactory);
 HFB_SYNC_FACTORY(Wrap2PiFactory);
 HFB_SYNC_FACTORY(ZernikeDefocusZPropFactory); // sink: no outputs; the task keeps the last estimate
 HFB_SYNC_FACTORY(HolofileFactory); // frames [batch, H, W] (12-bit: packed rows [batch, H, 3W/2] U8)
+// the thin holonp kinds GraphBuilder wires between the path's stages (nodes_np.cc)
+HFB_SYNC_FACTORY(SliceFactory);   // a strided view of the input (in place)
+HFB_SYNC_FACTORY(ReshapeFactory); // a view when the layout allows, else a contiguous copy
+HFB_SYNC_FACTORY(CopyFactory);
+HFB_SYNC_FACTORY(ConcatenateFactory);
+HFB_SYNC_FACTORY(ArangeFactory);
+HFB_SYNC_FACTORY(MultiplyFactory);
+HFB_SYNC_FACTORY(AbsFactory);
+HFB_SYNC_FACTORY(CausalSlidingAverageFactory);
 #undef HFB_SYNC_FACTORY
+
+using core::AsyncCreateCtx;
+using core::IAsyncTask;
+using core::IAsyncTaskFactory;
+
+#define HFB_ASYNC_FACTORY(Name)                                                                           \
+  class Name final : public IAsyncTaskFactory {                                                           \
+  public:                                                                                                 \
+    InferResult infer(std::span<const TDesc> input_descs, const nlohmann::json &jsettings) const override; \
+    std::unique_ptr<IAsyncTask> create(std::span<const TDesc> input_descs, const nlohmann::json &jsettings, \
+                                       const AsyncCreateCtx &ctx) const override;                         \
+  }
+
+// the queues (holotask/src/asyncs): owned inputs written through acquire_input, zero-copy views out
+HFB_ASYNC_FACTORY(BatchQueueFactory);
+HFB_ASYNC_FACTORY(DualReaderBatchQueueFactory);
+HFB_ASYNC_FACTORY(SlidingAverageFactory);
+#undef HFB_ASYNC_FACTORY
+
+// Registers the kinds of nodes_np.cc: "Slice", "Reshape", "Copy", "Concatenate", "Arange",
+// "Multiply", "Abs", "CausalSlidingAverage" and the asynchronous "BatchQueue",
+// "DualReaderBatchQueue" and "SlidingAverage".
+void register_np_kinds(core::Registry &registry);
 
 // Registers every node above under its kind string: "FresnelDiffraction", "AngularSpectrum",
 // "Pca", "FFT", "RFFT", "Mean", "MeanAbs", "Conversion", "FFTShiftNp", "Flatfield", "Filter2D",

@@ -552,13 +552,42 @@ def autofocus_planes(planes: np.ndarray, cfg: PathConfig):
     from . import shack as SH
     a = cfg.autofocus
     acfg = SH.AutofocusConfig(a["nb"], cfg.lam, cfg.pitch, cfg.z, list(a["orders"]), a.get("roi_radius", 0.5),
-                              not a.get("keep_outside", False), a.get("flatfield_period", 0.0))
+                              not a.get("keep_outside", False), a.get("flatfield_period", 0.0),
+                              bool(a.get("full_pairwise", False)))
     total = np.zeros(len(acfg.indexes))
     cur = np.asarray(planes, np.complex128)
     for _ in range(a.get("n_iter", 1)):
         r = SH.autofocus(cur, acfg)
         cur, total = r[4], total + r[2]
     return cur, total
+
+
+def reconstruct_sequence(windows: Sequence[np.ndarray], cfg: PathConfig) -> list:
+    """Consecutive windows of one stream with the autofocus over pp_accumulation = n > 1 spectra
+    (graph_builder.cc:128-153, 348): window w's sub-aperture M0 images enter a causal sliding
+    average over the last n windows; the fit of that average corrects the DELAYED window w - d,
+    d = (n - 1) // 2, which the dual-reader queue supplies (dual_reader_batch_queue.cc:214-227;
+    zero planes while the stream is younger than d windows).  Output w is the moments of the
+    corrected delayed window (zeros for w < d).  One autofocus pass (graph_builder.cc:143-146)."""
+    from . import shack as SH
+    a = cfg.autofocus
+    n = int(a.get("pp_accumulation", 1))
+    if a.get("n_iter", 1) != 1 and n > 1:
+        raise ValueError("sliding Shack-Hartmann correction only supports one autofocus iteration")
+    d = (n - 1) // 2
+    acfg = SH.AutofocusConfig(a["nb"], cfg.lam, cfg.pitch, cfg.z, list(a["orders"]), a.get("roi_radius", 0.5),
+                              not a.get("keep_outside", False), a.get("flatfield_period", 0.0),
+                              bool(a.get("full_pairwise", False)))
+    avg = SH.CausalSlidingAverage(n) if n > 1 else None
+    weights = freq_weights(cfg.frames, cfg.z0, cfg.z1, cfg.fs, cfg.time_method)
+    hist, outs = [], []
+    for w, win in enumerate(windows):
+        planes = band_planes(win, cfg)
+        hist.append(planes)
+        delayed = hist[w - d] if w >= d else np.zeros_like(planes)
+        corrected = SH.autofocus(planes, acfg, delayed=delayed, average=avg)[4]
+        outs.append(moments_from_magnitude(propagate(corrected, cfg), weights, cfg.fftshift))
+    return outs
 
 
 def band_bins(f_lo: float, f_hi: float, fs: float, T: int) -> tuple[int, int]:

@@ -237,6 +237,40 @@ def shack_hartmann_slopes(images: np.ndarray, lam: float, dx: float, dy: float, 
     return (slopes, maps.reshape(sy, sx, h, w)) if return_maps else slopes
 
 
+def full_pairwise_slopes(images: np.ndarray, lam: float, dx: float, dy: float, z: float,
+                         roi=(0.5, 0.5, 0.5, 0.5, 0.0), skip_outside: bool = True) -> np.ndarray:
+    """ShackHartmannSlopes, FullPairwise mode (the graph-Laplacian recovery,
+    shack_hartmann_slopes_full_pairwise.cuh:69-241).  Every pair (i, j), i < j, of ACTIVE
+    sub-apertures is phase-correlated (moving i against reference j: normalised i conj(j),
+    phase_correlation.cuh:54-62); the peak shift of the pair, scaled to slopes, is added to rhs[i]
+    and subtracted from rhs[j] (accumulate_complete_graph_rhs); the complete-graph Laplacian solve
+    in the zero-mean gauge is slope_i = rhs_i / N - mean_k(rhs_k / N) (solve_complete_graph_and_
+    scatter); inactive samples are 0.  images [sy, sx, h, w] -> slopes [sy, sx, 2]."""
+    sy, sx, h, w = images.shape
+    flat = images.reshape(sy * sx, h, w).astype(np.float64)
+    geo = geometry(sy, sx, h, w, h, w, dy, dx, skip_outside)
+    act = np.flatnonzero(geo.active)
+    n = len(act)
+    spec = np.fft.fft2(phase_correlation_prep(flat[act], roi), axes=(-2, -1))
+    spp_x = (lam * z / (w * dx)) / z
+    spp_y = (lam * z / (h * dy)) / z
+    rhs = np.zeros((n, 2))
+    for i in range(n):
+        for j in range(i + 1, n):
+            p = spec[i] * np.conj(spec[j])
+            mag = np.abs(p)
+            p = np.where(mag <= 1e-12, 0.0, p / np.where(mag <= 1e-12, 1.0, mag))
+            # the unnormalised inverse times 1 / (h w): numpy's normalised inverse
+            ddx, ddy = peak_shift(np.real(np.fft.ifft2(p)))
+            rhs[i] += (ddx * spp_x, ddy * spp_y)
+            rhs[j] -= (ddx * spp_x, ddy * spp_y)
+    out = np.zeros((sy * sx, 2))
+    if n:
+        mean = (rhs / n).sum(axis=0) / n
+        out[act] = rhs / n - mean
+    return out.reshape(sy, sx, 2)
+
+
 # ------------------------------------------------------------------------------------------------
 # Zernike modes
 # ------------------------------------------------------------------------------------------------
@@ -357,6 +391,7 @@ class AutofocusConfig:
     roi_radius: float = 0.5
     skip_outside: bool = True
     flatfield_period: float = 0.0  # pp_flatfield cutoff period [m]; 0 = off
+    full_pairwise: bool = False    # autofocus_use_graph_laplacian (graph_builder.cc:359-361)
 
 
 def subaperture_flatfield(m0: np.ndarray, cfg: AutofocusConfig) -> np.ndarray:
@@ -375,18 +410,48 @@ def subaperture_flatfield(m0: np.ndarray, cfg: AutofocusConfig) -> np.ndarray:
     return np.asarray(out, np.float64).reshape(m0.shape)
 
 
-def autofocus(planes: np.ndarray, cfg: AutofocusConfig, delayed: Optional[np.ndarray] = None):
-    """build_shack_hartmann (graph_builder.cc:307-501) for one spectrum, pp_accumulation = 1, no
-    flatfield: sub-aperture M0, slopes, Zernike fit, phase over the full field, corrected planes.
-    Returns (m0, slopes, coefficients, phase, corrected)."""
+class CausalSlidingAverage:
+    """CausalSlidingAverage (causal_sliding_average.cu:35-90): a float32 history of the last n
+    inputs (starting at zero) and a float32 running sum, sum += x - x_(k-n); the output is the sum
+    divided by min(k + 1, n), so the first outputs average the inputs seen so far."""
+
+    def __init__(self, n: int):
+        self.n, self.count, self.hist, self.sum = n, 0, None, None
+
+    def __call__(self, x: np.ndarray) -> np.ndarray:
+        x = np.asarray(x, np.float32)
+        if self.hist is None:
+            self.hist = np.zeros((self.n,) + x.shape, np.float32)
+            self.sum = np.zeros(x.shape, np.float32)
+        slot = self.count % self.n
+        self.sum = ((self.sum + x).astype(np.float32) - self.hist[slot]).astype(np.float32)
+        self.hist[slot] = x
+        out = self.sum / np.float32(min(self.count + 1, self.n))
+        self.count += 1
+        return out.astype(np.float64)
+
+
+def autofocus(planes: np.ndarray, cfg: AutofocusConfig, delayed: Optional[np.ndarray] = None,
+              average: Optional[CausalSlidingAverage] = None):
+    """build_shack_hartmann (graph_builder.cc:307-501) for one spectrum: sub-aperture M0 (causally
+    averaged over the last pp_accumulation spectra when `average` is given, graph_builder.cc:348),
+    optional flatfield, slopes (single-reference, or full-pairwise when cfg.full_pairwise), Zernike
+    fit, phase over the full field, and the corrected planes -- `delayed` when given (the dual
+    reader's delayed window, graph_builder.cc:128-143).  Returns (m0, slopes, coefficients, phase,
+    corrected)."""
     Nz, H, W = planes.shape
     nb = cfg.nb_subaps
     sh, sw = H // nb, W // nb
     m0 = subaperture_m0(planes, nb, cfg.lam, cfg.dx, cfg.z)
+    if average is not None:
+        m0 = average(m0)
     if cfg.flatfield_period > 0.0:
         m0 = subaperture_flatfield(m0, cfg)
     roi = (0.5, 0.5, cfg.roi_radius, cfg.roi_radius, 0.0)
-    slopes = shack_hartmann_slopes(m0, cfg.lam, cfg.dx, cfg.dx, cfg.z, roi, cfg.skip_outside)
+    if cfg.full_pairwise:
+        slopes = full_pairwise_slopes(m0, cfg.lam, cfg.dx, cfg.dx, cfg.z, roi, cfg.skip_outside)
+    else:
+        slopes = shack_hartmann_slopes(m0, cfg.lam, cfg.dx, cfg.dx, cfg.z, roi, cfg.skip_outside)
     geo = geometry(nb, nb, sh, sw, sh, sw, cfg.dx, cfg.dx, cfg.skip_outside)
     coeffs = zernike_from_slopes(slopes, cfg.indexes, cfg.lam, geo)
     phase = zernike_phase(coeffs, cfg.indexes, H, W)

@@ -253,6 +253,87 @@ def test_validation_messages(cuda):
         af.ShortTimeFresnel((1, 2048, 2048), (2048, 2048), (2048, 2048), LAM, DX, DX, Z)
 
 
+def test_full_pairwise_known_answers(cuda):
+    """FullPairwise slope recovery (shack_hartmann_slopes_full_pairwise.cuh) on the device: the
+    reference's star-graph / batch-size and periodic-peak tests (shack_hartmann_test.cu:656-739),
+    and the oracle's restatement."""
+    import torch
+    shifts = [(-2, 1), (-1, 0), (0, -1), (-1, 1), (0, 0), (1, -1), (0, 1), (1, 0), (2, -1)]
+    img = translated(3, 3, 40, 40, shifts)
+    kw = dict(lam=40.0, dx=1.0, dy=1.0, z=2.0)
+    roi = (0.5, 0.5, 10.0, 10.0, 0.0)
+    dev = torch.from_numpy(img).to(cuda)
+    single = _af().ShackHartmannSlopes(3, 3, 40, 40, roi=roi, skip_outside_pupil=False, **kw)(dev).cpu().numpy()
+    single = single.reshape(-1, 2)
+    exp = SH.full_pairwise_slopes(img, roi=roi, skip_outside=False, **kw).reshape(-1, 2)
+    edges = 9 * 8 // 2
+    base = None
+    for batch in (1, 5, 32, edges + 11):
+        op = _af().ShackHartmannSlopes(3, 3, 40, 40, roi=roi, skip_outside_pupil=False, mode="full_pairwise",
+                                       pair_batch_size=batch, **kw)
+        got = op(dev).cpu().numpy().reshape(-1, 2)
+        if base is None:
+            base = got
+        assert np.abs(got - base).max() < 2e-6, batch          # batch-invariant
+        assert np.abs(got - np.array(shifts, float)).max() < 0.035
+        assert np.abs(got - single).max() < 0.025              # star vs complete graph
+        assert abs(got[:, 0].sum()) < 4e-6 and abs(got[:, 1].sum()) < 4e-6
+        assert np.abs(got - exp).max() < 1e-2                  # against the oracle
+    # periodic-peak and sub-pixel conventions on a 1 x 3 grid (an even-sized grid is allowed too)
+    sh = [(-9.0, 7.0), (-0.40, 0.35), (9.0, -7.0)]
+    img = translated(1, 3, 48, 48, sh)
+    op = _af().ShackHartmannSlopes(1, 3, 48, 48, roi=roi, skip_outside_pupil=False, mode="full_pairwise",
+                                   pair_batch_size=2, lam=48.0, dx=1.0, dy=1.0, z=2.0)
+    s = op(torch.from_numpy(img).to(cuda)).cpu().numpy().reshape(-1)
+    mx, my = sum(v[0] for v in sh) / 3.0, sum(v[1] for v in sh) / 3.0
+    for i, (dx, dy) in enumerate(sh):
+        assert abs(s[2 * i] - (dx - mx)) < 0.08 and abs(s[2 * i + 1] - (dy - my)) < 0.08
+    assert abs((s[0] - s[4]) + 18.0) < 0.2 and abs((s[1] - s[5]) - 14.0) < 0.2
+    op2 = _af().ShackHartmannSlopes(2, 2, 32, 32, roi=roi, skip_outside_pupil=False, mode="full_pairwise", **kw)
+    assert op2(torch.zeros((2, 2, 32, 32), device=cuda)).shape == (2, 2, 2)
+    with pytest.raises(Exception, match="at least two active subapertures"):
+        _af().ShackHartmannSlopes(1, 1, 32, 32, roi=roi, skip_outside_pupil=False, mode="full_pairwise", **kw)
+
+
+@pytest.mark.parametrize("sy,h,w,skip", [(5, 34, 51, True), (3, 64, 64, False)])
+def test_full_pairwise_textured_vs_oracle(cuda, sy, h, w, skip):
+    """FullPairwise slopes on textured sub-aperture images (sharp peaks) against the oracle."""
+    import torch
+    rng = np.random.default_rng(7 + sy)
+    base = rng.standard_normal((h, w)).astype(np.float32)
+    offs = [(int(rng.integers(-3, 4)), int(rng.integers(-3, 4))) for _ in range(sy * sy)]
+    img = np.stack([np.roll(base, (dy, dx), axis=(0, 1)) for dx, dy in offs]).reshape(sy, sy, h, w)
+    kw = dict(lam=float(w), dx=1.0, dy=w / h, z=2.0)
+    roi = (0.5, 0.5, 10.0, 10.0, 0.0)
+    op = _af().ShackHartmannSlopes(sy, sy, h, w, roi=roi, skip_outside_pupil=skip, mode="full_pairwise",
+                                   pair_batch_size=7, **kw)
+    got = op(torch.from_numpy(img).to(cuda)).cpu().numpy().reshape(-1, 2)
+    exp = SH.full_pairwise_slopes(img, roi=roi, skip_outside=skip, **kw).reshape(-1, 2)
+    assert np.abs(got - exp).max() < 2e-3
+
+
+def test_full_pairwise_slopes_node(cuda):
+    """The ShackHartmannSlopes node in "full_pairwise" mode gives the binding's slopes; map output
+    is refused as in the reference (shack_hartmann_slopes.cu:343-345)."""
+    import torch
+    from holoflow_b200 import nodes as N
+    rng = np.random.default_rng(3)
+    base = rng.standard_normal((40, 40)).astype(np.float32)
+    img = np.stack([np.roll(base, (int(rng.integers(-2, 3)), int(rng.integers(-2, 3))), axis=(0, 1))
+                    for _ in range(9)]).reshape(1, 3, 3, 40, 40)
+    dev = torch.from_numpy(img).to(cuda)
+    sl = {"lambda": 40.0, "dx": 1.0, "dy": 1.0, "z": 2.0, "subaperture_height": 40, "subaperture_width": 40,
+          "stride_y": 40, "stride_x": 40, "mode": "full_pairwise", "pair_batch_size": 4,
+          "skip_subapertures_outside_pupil": False,
+          "correlation_roi": {"cx": 0.5, "cy": 0.5, "rx": 10.0, "ry": 10.0, "angle": 0.0}}
+    (slopes,) = N.run_sync_factory("ShackHartmannSlopes", sl, [dev])
+    op = _af().ShackHartmannSlopes(3, 3, 40, 40, roi=(0.5, 0.5, 10.0, 10.0, 0.0), skip_outside_pupil=False,
+                                   mode="full_pairwise", pair_batch_size=4, lam=40.0, dx=1.0, dy=1.0, z=2.0)
+    assert torch.equal(slopes.reshape(3, 3, 2), op(dev[0]))
+    with pytest.raises(Exception, match="FullPairwise correlation-map output is not supported"):
+        N.run_sync_factory("ShackHartmannSlopes", {**sl, "output_xcorr_maps": True}, [dev])
+
+
 def test_autofocus_as_nodes(cuda):
     """ShortTimeFresnelDiffraction -> Mean -> FFTShiftNp -> ShackHartmannSlopes -> (host)
     ZernikeFromSlopes -> ZernikePhase -> CorrectPhase, driven as the reference's graph wires them
@@ -422,3 +503,69 @@ def test_pipeline_with_autofocus_flatfield(cuda, form):
     acfg = SH.AutofocusConfig(5, LAM, DX, Z, [4, 5, 6], flatfield_period=per)
     em0 = SH.subaperture_flatfield(SH.subaperture_m0(planes, 5, LAM, DX, Z), acfg)
     assert O.rel_l2(op.m0().cpu().numpy(), em0) < 5e-5  # the high-pass leaves a smaller norm
+
+
+def drifting_doppler_frames(n_frames, T, side, k0, a4_0, a4_rate, seed=9):
+    """Frames x_t = Re(A(t) exp(2 pi i k0 t / T)) whose defocus drifts, a4(t) = a4_0 + a4_rate t:
+    every window sees a slightly different aberration, so a sliding average differs from one window."""
+    rng = np.random.default_rng(seed)
+    lens = O.fresnel_lens(side, side, LAM, Z, DX)
+    y, x = (np.mgrid[0:side, 0:side] - (side - 1) / 2.0) / (side / 2.0)
+    pts = np.zeros((side, side), np.complex128)
+    for _ in range(8):
+        pts[rng.integers(side // 4, 3 * side // 4), rng.integers(side // 4, 3 * side // 4)] = np.exp(
+            2j * math.pi * rng.random()) * (1.0 + rng.random())
+    base = np.conj(lens) * np.fft.ifft2(pts) * side * 100.0
+    z4 = SH.zernike_value(4, x, y)
+    out = np.empty((n_frames, side, side), np.float32)
+    for t in range(n_frames):
+        out[t] = np.real(base * np.exp(1j * (a4_0 + a4_rate * t) * z4) * np.exp(2j * math.pi * k0 * t / T))
+    return out
+
+
+@pytest.mark.parametrize("form,n,pairwise", [(0, 3, False), (1, 3, False), (1, 5, False), (1, 3, True)])
+def test_pipeline_sliding_correction_of_the_delayed_window(cuda, form, n, pairwise):
+    """pp_accumulation = n (graph_builder.cc:128-153, 348): window w's sub-aperture images are
+    averaged causally over the last n windows and the fit corrects window w - (n - 1) / 2, which
+    the plan keeps across calls (the dual reader's delayed window); the first (n - 1) / 2 outputs
+    are zero images.  Two calls (3 + 4 windows) against the oracle's sequence, optionally with the
+    full-pairwise slopes."""
+    import torch
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    T, hop, side, nb = 32, 8, 256, 5
+    nwin = 7
+    frames = drifting_doppler_frames(T + hop * (nwin - 1), T, side, 5, 3.0, 0.02)
+    ring = torch.from_numpy(frames).to(cuda)
+    cfg = pl.PipelineConfig(height=side, width=side, frames=T, hop=hop, z_begin=3, z_end=9, input_dtype=hf.HF_F32,
+                            lam=LAM, pitch=DX, z=Z, form=form, max_batch=4, autofocus_nb_subaps=nb,
+                            autofocus_orders=(4, 5, 6), autofocus_pp_accumulation=n,
+                            autofocus_full_pairwise=int(pairwise))
+    p = pl.Pipeline(cfg)
+    got = np.concatenate([p.run(ring, frames.shape[0], 0, 3).cpu().numpy(),
+                          p.run(ring, frames.shape[0], 3 * hop, 4).cpu().numpy()])
+    assert p.status() == 0
+    ocfg = O.PathConfig(side, side, T, hop, 3, 9, lam=LAM, pitch=DX, z=Z,
+                        autofocus=dict(nb=nb, orders=[4, 5, 6], pp_accumulation=n, full_pairwise=pairwise))
+    exp = O.reconstruct_sequence([frames[w * hop: w * hop + T].astype(np.float64) for w in range(nwin)], ocfg)
+    d = (n - 1) // 2
+    tol = 1e-4 if form == 0 else 1e-3
+    for w in range(nwin):
+        if w < d:
+            assert not got[w].any(), w
+            continue
+        for m in range(3):
+            assert O.rel_l2(got[w, m], exp[w][m]) < tol, (w, m, O.rel_l2(got[w, m], exp[w][m]))
+    # a new sequence starts over: the first d outputs are zero again and the rest repeat
+    p.autofocus_reset()
+    again = p.run(ring, frames.shape[0], 0, 3).cpu().numpy()
+    assert np.array_equal(again, got[:3])
+
+
+def test_pipeline_sliding_correction_validation(cuda):
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    cfg = dict(height=256, width=256, frames=32, hop=8, z_begin=3, z_end=9, input_dtype=hf.HF_F32, lam=LAM, pitch=DX,
+               z=Z, max_batch=2, autofocus_nb_subaps=5, autofocus_orders=(4,))
+    with pytest.raises(hf.HfError, match="only supports one autofocus iteration"):
+        pl.Pipeline(pl.PipelineConfig(**cfg, autofocus_pp_accumulation=3, autofocus_n_iter=2))

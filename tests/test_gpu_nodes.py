@@ -54,6 +54,28 @@ def test_fresnel_node_and_z_update(cuda, rng):
     node.close()
 
 
+@pytest.mark.parametrize("shape,axes", [((64, 128, 3), [0, 1]), ((2, 64, 3, 128), [1, 3]), ((3, 64, 128), [-2, -1])])
+def test_fresnel_node_over_any_two_axes(cuda, rng, shape, axes):
+    """Axes other than the last two (fresnel_diffraction.cu:118-200, 519-570): the planes spanned by
+    (axes[0], axes[1]) at every index of the other dimensions, one batch group per launch plus a
+    launch per remaining index; equal to the last-two-axes transform of the permuted tensor."""
+    import torch
+    N = _n()
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    dev = torch.from_numpy(x).to(cuda)
+    s = {"lambda": LAM, "dx": DX, "dy": DX, "z": 0.05, "axes": axes}
+    (got,) = N.run_sync_factory("FresnelDiffraction", s, [dev])
+    (mag,) = N.run_sync_factory("FresnelDiffraction", {**s, "output_magnitude": True}, [dev])
+    a0, a1 = (a % len(shape) for a in axes)
+    perm = [d for d in range(len(shape)) if d not in (a0, a1)] + [a0, a1]
+    xp = np.ascontiguousarray(x.transpose(perm))
+    exp = O.fresnel(xp, LAM, DX, DX, 0.05, output_magnitude=False, skip_phase_shift=False)
+    inv = np.argsort(perm)
+    tol = 2e-6 * math.log2(shape[a0] * shape[a1])
+    assert rel(got.cpu().numpy(), exp.transpose(inv)) < tol
+    assert rel(mag.cpu().numpy(), np.abs(exp).transpose(inv)) < tol
+
+
 def test_angular_spectrum_node_kats(cuda, rng):
     """angular_spectrum_test.cu:146-283: z = 0 scales a real input by H*W and centres it in the
     padding; with a filter the result matches the oracle."""
@@ -216,3 +238,154 @@ def test_holofile_gpu_cached_source_feeds_doppler_moments(cuda, tmp_path):
         assert torch.equal(got, ref), b
     dop.close()
     src.close()
+
+
+# ---- the thin holonp kinds and the queues --------------------------------------------------------
+def test_thin_kinds_against_the_reference_oracle_goldens(cuda):
+    """Slice (a view), Copy, Arange, Multiply and Abs through hf_node_* against the outputs of the
+    reference's own NumPy test oracle (tests/golden/holonp_ops.npz)."""
+    import torch
+    N = _n()
+    st, (x,), y = _gold("slice_band_4_32")
+    dev = torch.from_numpy(x).to(cuda)
+    # numpy pads missing trailing items with ':'; the node takes one item per dimension
+    # (slice.cu:199-200)
+    st = {"slices": st["slices"] + [{}] * (x.ndim - len(st["slices"]))}
+    (v,) = N.run_sync_factory("Slice", st, [dev])
+    assert v.data_ptr() == dev[:, 4:32].data_ptr() and tuple(v.shape) == y.shape   # a view, no copy
+    (c,) = N.run_sync_factory("Copy", {}, [v])
+    assert c.is_contiguous() and np.array_equal(c.cpu().numpy(), y)
+    st, _, y = _gold("arange_band_t64")
+    (a,) = N.run_sync_factory("Arange", st, [])
+    assert np.array_equal(a.cpu().numpy(), y)
+    st, (p, q), y = _gold("multiply_weights")
+    (m,) = N.run_sync_factory("Multiply", st, [torch.from_numpy(p).to(cuda), torch.from_numpy(q).to(cuda)])
+    assert rel(m.cpu().numpy(), y) < 1e-7
+    st, (z,), y = _gold("abs_cf32")
+    (b,) = N.run_sync_factory("Abs", st, [torch.from_numpy(z).to(cuda)])
+    assert rel(b.cpu().numpy(), y) < 1e-6
+
+
+def test_reshape_concatenate_and_causal_average(cuda, rng):
+    import torch
+    N = _n()
+    x = torch.from_numpy(rng.standard_normal((2, 6, 10)).astype(np.float32)).to(cuda)
+    (r,) = N.run_sync_factory("Reshape", {"shape": [1, 2, 6, -1]}, [x])
+    assert r.data_ptr() == x.data_ptr() and torch.equal(r, x.reshape(1, 2, 6, 10))
+    t = x.transpose(1, 2)                                       # [2, 10, 6], not viewable flat
+    (r2,) = N.run_sync_factory("Reshape", {"shape": [120]}, [t])
+    assert r2.data_ptr() != t.data_ptr() and torch.equal(r2, t.reshape(120))
+    a = torch.from_numpy((rng.standard_normal((2, 3, 5)) + 1j * rng.standard_normal((2, 3, 5))).astype(np.complex64))
+    b = torch.from_numpy((rng.standard_normal((2, 4, 5)) + 1j * rng.standard_normal((2, 4, 5))).astype(np.complex64))
+    (c,) = N.run_sync_factory("Concatenate", {"axis": -2}, [a.to(cuda), b.to(cuda)])
+    assert torch.equal(c.cpu(), torch.cat([a, b], dim=1))
+    from oracle import shack as SH
+    node = N.Node("CausalSlidingAverage", {"window_size": 3}, [N.desc_of(x)])
+    avg = SH.CausalSlidingAverage(3)
+    for k in range(5):
+        inp = torch.from_numpy(rng.standard_normal((2, 6, 10)).astype(np.float32)).to(cuda)
+        out = torch.empty_like(inp)
+        node.execute([inp], [out])
+        torch.cuda.synchronize()
+        assert np.allclose(out.cpu().numpy(), avg(inp.cpu().numpy()), rtol=1e-6, atol=1e-6), k
+    node.close()
+
+
+def test_batch_queue_and_dual_reader(cuda, rng):
+    """BatchQueue windows of output_size elements every output_stride pushes (zero-copy views into
+    its ring), and the DualReaderBatchQueue's current / delayed elements and valid flag
+    (dual_reader_batch_queue.cc:104-156)."""
+    import torch
+    N = _n()
+    el = N.desc_of(torch.empty((1, 4, 3), device=cuda))
+    bq = N.async_node("BatchQueue", {"target_capacity": 4, "output_size": 2, "output_stride": 2}, [el])
+    vals = [torch.full((1, 4, 3), float(k), device=cuda) for k in range(6)]
+    got = []
+    for k in range(6):
+        slot = bq.acquire_input()
+        assert slot is not None
+        slot.copy_(vals[k])
+        assert bq.try_push() == 0
+        if bq.try_pop() == 0:
+            got.append(bq.output().clone())
+            bq.release_output()
+    torch.cuda.synchronize()
+    assert [g[:, 0, 0].tolist() for g in got] == [[0.0, 1.0], [2.0, 3.0], [4.0, 5.0]]
+    bq.close()
+    d = N.desc_of(torch.empty((2, 3, 4), device=cuda))
+    dr = N.async_node("DualReaderBatchQueue", {"target_capacity": 4, "window_size": 5}, [d])   # delay 2
+    flag = torch.zeros(1, dtype=torch.uint8)
+    seen = []
+    for k in range(3):                                        # pushes of 2 elements: values 2k, 2k + 1
+        slot = dr.acquire_input()
+        slot.copy_(torch.stack([torch.full((3, 4), 2.0 * k, device=cuda), torch.full((3, 4), 2.0 * k + 1, device=cuda)]))
+        assert dr.try_push() == 0
+        while dr.try_pop([None, None, flag]) == 0:
+            torch.cuda.synchronize()
+            seen.append((dr.output(0)[0, 0, 0].item(), dr.output(1)[0, 0, 0].item(), int(flag.item())))
+            dr.release_output(0)
+            dr.release_output(1)
+    # element w, delayed element w - 2 (zero before), valid once 4 elements were popped before
+    assert seen == [(0, 0, 0), (1, 0, 0), (2, 0, 0), (3, 1, 0), (4, 2, 1), (5, 3, 1)]
+    dr.close()
+
+
+def test_reference_graph_node_by_node_equals_the_fused_node(cuda):
+    """The node sequence GraphBuilder emits for the RFFT time method with Fresnel and M0/M1/M2
+    (graph_builder.cc:245-305, 522-566, 578-631): Conversion -> Reshape [1, T, H, W] -> BatchQueue
+    -> RFFT(axis 1) -> Slice [z0, z1) -> Copy -> DualReaderBatchQueue -> FresnelDiffraction (|.|) ->
+    Mean(-3) for M0, Arange -> Reshape -> Multiply -> Mean for M1 and M2; against the fused
+    DopplerMoments node on the same frames (the weights with fs = 37 kHz, as the reference's)."""
+    import torch
+    N = _n()
+    T, H, W, z0, z1, NPRE = 32, 64, 64, 6, 16, 2
+    frames = S.Interferograms(S.config0(T * NPRE)).frames(0, T * NPRE)[:, :H, :W]
+    # 8-bit frames: the reference's Conversion takes U8 -> F32 Real only (conversion.cu:140-147)
+    u8 = torch.from_numpy((frames >> 4).astype(np.uint8)).to(cuda)
+    fres = {"lambda": LAM, "dx": DX, "dy": DX, "z": 0.3, "output_magnitude": True, "skip_phase_shift": True}
+    desc = N.desc_of
+    bq = N.async_node("BatchQueue", {"target_capacity": 2 * NPRE, "output_size": NPRE, "output_stride": NPRE},
+                      [desc(torch.empty((1, T, H, W), device=cuda))])
+    for w in range(NPRE):                                     # one window of T frames per push
+        (f32,) = N.run_sync_factory("Conversion", {"target": "F32", "strategy": "Real"}, [u8[w * T:(w + 1) * T]])
+        (win,) = N.run_sync_factory("Reshape", {"shape": [1, T, H, W]}, [f32])
+        slot = bq.acquire_input()
+        slot.copy_(win)
+        assert bq.try_push() == 0
+    assert bq.try_pop() == 0
+    batch = bq.output()                                       # [NPRE, T, H, W]
+    (spec,) = N.run_sync_factory("RFFT", {"axis": 1}, [batch])
+    (band,) = N.run_sync_factory("Slice", {"slices": [{}, {"start": z0, "stop": z1}, {}, {}]}, [spec])
+    (band,) = N.run_sync_factory("Copy", {}, [band])
+    bq.release_output()
+    dr = N.async_node("DualReaderBatchQueue", {"target_capacity": 4, "window_size": 1}, [desc(band)])
+    slot = dr.acquire_input()
+    slot.copy_(band)
+    assert dr.try_push() == 0
+    df = 37e3 / T
+    (freqs,) = N.run_sync_factory("Arange", {"start": z0 * df, "stop": z1 * df, "step": df, "dtype": "F32"}, [])
+    (fw,) = N.run_sync_factory("Reshape", {"shape": [1, z1 - z0, 1, 1]}, [freqs])
+    (fw2,) = N.run_sync_factory("Multiply", {}, [fw, fw])
+    flag = torch.zeros(1, dtype=torch.uint8)
+    graph = []
+    while dr.try_pop([None, None, flag]) == 0:
+        cur = dr.output(0)                                    # [1, Nz, H, W]
+        (mag,) = N.run_sync_factory("FresnelDiffraction", fres, [cur])
+        (m0,) = N.run_sync_factory("Mean", {"axis": [-3], "keepdims": True}, [mag])
+        (w1,) = N.run_sync_factory("Multiply", {}, [fw, mag])
+        (m1,) = N.run_sync_factory("Mean", {"axis": [-3], "keepdims": True}, [w1])
+        (w2,) = N.run_sync_factory("Multiply", {}, [fw2, mag])
+        (m2,) = N.run_sync_factory("Mean", {"axis": [-3], "keepdims": True}, [w2])
+        graph.append(torch.cat([m0, m1, m2], dim=1)[0].cpu().numpy())
+        dr.release_output(0)
+        dr.release_output(1)
+    assert len(graph) == NPRE
+    s = {"time_z_begin": z0, "time_z_end": z1, "propagation": "fresnel", "lambda": LAM, "dx": DX, "z": 0.3,
+         "input_format": "u8", "fs": 37e3, "form": "plain"}
+    for w in range(NPRE):
+        (fused,) = N.run_sync_factory("DopplerMoments", s, [u8[w * T:(w + 1) * T].reshape(1, T, H, W)])
+        f = fused.cpu().numpy()[0]
+        for m in range(3):
+            assert rel(f[m], graph[w][m]) < 1e-5, (w, m, rel(f[m], graph[w][m]))
+    bq.close()
+    dr.close()

@@ -41,7 +41,9 @@ def test_reference_kinds_are_registered():
     assert set(N.kinds()) == {"FresnelDiffraction", "AngularSpectrum", "Pca", "FFT", "RFFT", "Mean", "MeanAbs",
                               "Conversion", "Holofile", "FFTShiftNp", "Flatfield", "Filter2D", "PctClip",
                               "DopplerMoments", "ShortTimeFresnelDiffraction", "ShackHartmannSlopes",
-                              "ZernikeFromSlopes", "ZernikePhase", "CorrectPhase", "Wrap2Pi", "ZernikeDefocusZProp"}
+                              "ZernikeFromSlopes", "ZernikePhase", "CorrectPhase", "Wrap2Pi", "ZernikeDefocusZProp",
+                              "Slice", "Reshape", "Copy", "Concatenate", "Arange", "Multiply", "Abs",
+                              "CausalSlidingAverage", "BatchQueue", "DualReaderBatchQueue", "SlidingAverage"}
 
 
 def test_unknown_kind_and_bad_settings():
@@ -61,6 +63,10 @@ def test_fresnel_infer():
     invalid("FresnelDiffraction", FRESNEL, [desc([8, 8], CF32, device=False)], p + "input must be in device memory")
     invalid("FresnelDiffraction", {**FRESNEL, "axes": [0]}, [desc([8, 8], CF32)], p + "axes must contain exactly two")
     invalid("FresnelDiffraction", {**FRESNEL, "axes": [-1, -1]}, [desc([8, 8], CF32)], p + "axes must be distinct")
+    # any two axes whose strides nest (fresnel_diffraction.cu:482-484)
+    assert out_of("FresnelDiffraction", {**FRESNEL, "axes": [0, 1]}, [desc([64, 32, 3], CF32)]) == ((64, 32, 3), CF32)
+    invalid("FresnelDiffraction", {**FRESNEL, "axes": [1, 0]}, [desc([64, 32], CF32)],
+            p + "stride of ax0 (H) must be a multiple of stride of ax1 (W)")
     invalid("FresnelDiffraction", FRESNEL, [desc([2, 8, 8], CF32)] * 2, p + "expected exactly one input")
 
 
@@ -247,3 +253,61 @@ def test_doppler_moments_autofocus_settings():
     invalid("DopplerMoments", {**s, "autofocus_nb_subaps": 4}, [desc([1, 32, 256, 256])], p + "autofocus_nb_subaps must be odd")
     invalid("DopplerMoments", {**s, "propagation": "angular_spectrum"}, [desc([1, 32, 256, 256])],
             p + "Shack-Hartmann autofocus needs fresnel propagation")
+
+
+# ---- the thin holonp kinds and the queues GraphBuilder wires around the path -------------------
+def test_slice_is_a_strided_view():
+    """Slice (slice.cu:185-250): [8, 33, 4, 6] CF32 with [:, 4:32] is a view: shape [8, 28, 4, 6],
+    the input's byte strides, offset 4 x stride(1); an integer item drops its dimension."""
+    d = desc([8, 33, 4, 6], CF32)
+    (o,) = N.infer("Slice", {"slices": [{}, {"start": 4, "stop": 32}, {}, {}]}, [d])
+    assert N.shape_of(o) == (8, 28, 4, 6) and o.dtype == CF32
+    assert [o.strides[i] for i in range(4)] == [33 * 24 * 8, 24 * 8, 6 * 8, 8] and o.offset == 4 * 24 * 8
+    (o,) = N.infer("Slice", {"slices": [1, {"start": -3, "step": 2}, {}, {}]}, [d])
+    assert N.shape_of(o) == (2, 4, 6) and o.offset == 33 * 24 * 8 + 30 * 24 * 8
+    invalid("Slice", {"slices": [{}, {}]}, [d], "Slice: number of slice items must match input ndim")
+    invalid("Slice", {"slices": [{}, {"step": -1}, {}, {}]}, [d], "Slice: only positive step is supported")
+
+
+def test_reshape_copy_concatenate_infer():
+    (o,) = N.infer("Reshape", {"shape": [1, 32, 4, -1]}, [desc([32, 4, 8])])
+    assert N.shape_of(o) == (1, 32, 4, 8)
+    invalid("Reshape", {"shape": [-1, -1]}, [desc([4, 8])], "Reshape: Only one dimension can be -1")
+    invalid("Reshape", {"shape": [5, 7]}, [desc([4, 8])], "Reshape: Total elements mismatch")
+    strided = desc([4, 8], F32, strides=[64, 4])          # rows 16 floats apart: no flat view
+    invalid("Reshape", {"shape": [32], "copy": False}, [strided], "a view is not possible")
+    (o,) = N.infer("Reshape", {"shape": [32]}, [strided])   # falls back to a contiguous copy
+    assert N.shape_of(o) == (32,) and o.strides[0] == 4
+    assert out_of("Copy", {}, [strided]) == ((4, 8), F32)
+    invalid("Copy", {}, [desc([4, 8], F32, device=False)], "Copy: only Device tensors are supported")
+    assert out_of("Concatenate", {"axis": 1}, [desc([2, 3, 5], CF32), desc([2, 4, 5], CF32)]) == ((2, 7, 5), CF32)
+    invalid("Concatenate", {"axis": 1}, [desc([2, 3, 5], CF32), desc([2, 4, 5], F32)],
+            "Concatenate: all inputs must share the same dtype")
+    invalid("Concatenate", {"axis": 3}, [desc([2, 3, 5])], "Concatenate: axis out of range")
+
+
+def test_arange_multiply_abs_infer():
+    df = 37e3 / 64
+    assert out_of("Arange", {"start": 4 * df, "stop": 32 * df, "step": df, "dtype": "F32"}, []) == ((28,), F32)
+    invalid("Arange", {"start": 0.0, "stop": 1.0, "step": 0.0}, [], "ArangeFactory inference error: step must be non-zero")
+    assert out_of("Multiply", {}, [desc([1, 28, 1, 1]), desc([1, 28, 16, 16], CF32)]) == ((1, 28, 16, 16), CF32)
+    invalid("Multiply", {}, [desc([1, 28, 1, 1]), desc([1, 27, 16, 16])], "Multiply: input shapes are not broadcastable")
+    assert out_of("Abs", {}, [desc([1, 28, 8, 8], CF32)]) == ((1, 28, 8, 8), F32)
+    invalid("Abs", {}, [desc([4, 8], CF32, strides=[128, 8])], "Abs: input tensor must be contiguous")
+
+
+def test_queue_kinds_infer():
+    """BatchQueue (batch_queue.cc:188-222) and DualReaderBatchQueue (dual_reader_batch_queue.cc:
+    231-262): owned inputs and outputs, the reference's messages."""
+    (o,) = N.infer("BatchQueue", {"target_capacity": 16, "output_size": 8, "output_stride": 8}, [desc([1, 32, 8, 8])])
+    assert N.shape_of(o) == (8, 32, 8, 8)
+    invalid("BatchQueue", {"target_capacity": 16, "output_size": 8, "output_stride": 4}, [desc([1, 32, 8, 8])],
+            "BatchQueueFactory inference error: BatchQueue task output stride must be a multiple of output size")
+    outs = N.infer("DualReaderBatchQueue", {"target_capacity": 16, "window_size": 3}, [desc([8, 28, 8, 8], CF32)])
+    assert [N.shape_of(o) for o in outs] == [(1, 28, 8, 8), (1, 28, 8, 8), (1,)]
+    assert outs[2].dtype == U8 and outs[2].mem_loc == 0
+    invalid("DualReaderBatchQueue", {"target_capacity": 16, "window_size": 0}, [desc([8, 28, 8, 8], CF32)],
+            "DualReaderBatchQueueFactory inference error: window_size must be positive")
+    assert out_of("SlidingAverage", {"target_capacity": 4, "window_size": 3}, [desc([1, 16, 16])]) == ((1, 16, 16), F32)
+    invalid("CausalSlidingAverage", {"window_size": 2}, [desc([1, 16, 16], CF32)],
+            "CausalSlidingAverageFactory inference error: input dtype must be F32")

@@ -133,3 +133,64 @@ def test_wrap_and_defocus():
     assert np.all((w >= 0) & (w < 2 * math.pi + 1e-6))
     d_inv, z_new, dz = SH.defocus_z(0.0, 850e-9, 0.3, 3e-3)
     assert d_inv == 0.0 and z_new == pytest.approx(0.3) and dz == pytest.approx(0.0, abs=1e-9)
+
+
+# ---- FullPairwise (graph-Laplacian) slope recovery --------------------------------------------
+def test_full_pairwise_matches_star_graph_signs_gauge():
+    """MatchesStarGraphSignsGaugeAndBatchSizes (shack_hartmann_test.cu:656-710): integer
+    translations recovered within 0.035 px, within 0.025 px of the single-reference mode, zero sum."""
+    shifts = [(-2, 1), (-1, 0), (0, -1), (-1, 1), (0, 0), (1, -1), (0, 1), (1, 0), (2, -1)]
+    img = translated(3, 3, 40, 40, shifts)
+    single = SH.shack_hartmann_slopes(img, skip_outside=False, **slope_args(40, 40)).reshape(-1, 2)
+    full = SH.full_pairwise_slopes(img, skip_outside=False, **slope_args(40, 40)).reshape(-1, 2)
+    for i, (dx, dy) in enumerate(shifts):
+        assert abs(full[i, 0] - dx) < 0.035 and abs(full[i, 1] - dy) < 0.035
+        assert abs(full[i, 0] - single[i, 0]) < 0.025 and abs(full[i, 1] - single[i, 1]) < 0.025
+    assert abs(full[:, 0].sum()) < 4e-6 and abs(full[:, 1].sum()) < 4e-6
+
+
+def test_full_pairwise_subpixel_and_periodic_peaks():
+    """PreservesSubpixelAndPeriodicPeakConventions (shack_hartmann_test.cu:712-739): translations
+    up to the unambiguous periodic interval (an 18-pixel endpoint-to-endpoint edge) and sub-pixel
+    shifts, compared in the zero-mean gauge."""
+    shifts = [(-9.0, 7.0), (-0.40, 0.35), (9.0, -7.0)]
+    img = translated(1, 3, 48, 48, shifts)
+    s = SH.full_pairwise_slopes(img, skip_outside=False, **slope_args(48, 48)).reshape(-1)
+    mx = sum(v[0] for v in shifts) / 3.0
+    my = sum(v[1] for v in shifts) / 3.0
+    for i, (dx, dy) in enumerate(shifts):
+        assert abs(s[2 * i] - (dx - mx)) < 0.08 and abs(s[2 * i + 1] - (dy - my)) < 0.08
+    assert abs((s[0] - s[4]) + 18.0) < 0.2 and abs((s[1] - s[5]) - 14.0) < 0.2
+
+
+def test_full_pairwise_noiseless_defocus_matches_single_reference():
+    """NoiselessDefocusMatchesSingleReferenceAndZernikeFit (shack_hartmann_test.cu:803-850): a
+    defocus wavefront's sub-aperture shifts on the active 5 x 5 samples; both modes agree to
+    0.025 px and inactive samples are 0."""
+    h = w = 48
+    radius = 0.5 * 5 * w
+    coeff_m = radius / (4.0 * math.sqrt(3.0) * 0.4)
+    shifts = [(0.0, 0.0)] * 25
+    for iy in range(5):
+        for ix in range(5):
+            xn, yn = (ix - 2.0) / 2.5, (iy - 2.0) / 2.5
+            dzx, dzy = SH.zernike_derivative(4, xn, yn)
+            shifts[iy * 5] = (coeff_m * dzx / radius, coeff_m * dzy / radius)  # as the test writes it
+    img = translated(5, 5, h, w, shifts)
+    single = SH.shack_hartmann_slopes(img, skip_outside=True, **slope_args(h, w)).reshape(-1, 2)
+    full = SH.full_pairwise_slopes(img, skip_outside=True, **slope_args(h, w)).reshape(-1, 2)
+    for iy in range(5):
+        for ix in range(5):
+            i = iy * 5 + ix
+            if active_5x5(iy, ix):
+                assert abs(full[i, 0] - single[i, 0]) < 0.025 and abs(full[i, 1] - single[i, 1]) < 0.025
+            else:
+                assert full[i, 0] == 0.0 and full[i, 1] == 0.0
+
+
+def test_causal_sliding_average():
+    """CausalSlidingAverage (causal_sliding_average.cu:35-90): the first outputs average what has
+    arrived (divisor min(k + 1, n)), then the last n; float32 running sum."""
+    avg = SH.CausalSlidingAverage(3)
+    got = [float(avg(np.array([v], np.float32))[0]) for v in (1.0, 2.0, 3.0, 4.0, 8.0)]
+    assert got == [1.0, 1.5, 2.0, 3.0, 5.0]
