@@ -8,15 +8,18 @@
 // square-root approximation and fuses the weighted sums, which removes about a seventh of the
 // pass's instructions for a relative change far below its 1e-3 error budget.
 //
-// A CTA owns a strip of C = 8 columns of one window for all Nz planes:
+// A CTA owns a strip of C = kColMomCols (4) columns of one window for all Nz planes, and two
+// CTAs share an SM (128 threads, under 255 registers, 74 KB of shared memory each), so one CTA's
+// barrier or stage wait is covered by the other's work (strips of 8 columns in one CTA per SM took
+// 8 % longer):
 //  - one thread issues 2D TMA tile loads of a plane's [H][C] strip into one of two shared-memory
 //    stages, so the next plane streams in while this one is transformed;
 //  - thread (n2, c) loads its column's samples n2 + 32 n1 from the stage, runs the N1-point DFT in
 //    registers, twiddles by w_N^(n2 k1) from a [N1][32] table (one shared load, no index math)
-//    and writes the exchange back into the same stage at k1 * (32 C + 8) + n2 * C + c: the 8-entry
-//    pad per k1 row puts the two k1 rows a half-warp reads on opposite bank halves, so the
-//    transposed reads are conflict-free, and every address is the thread's base plus a
-//    compile-time offset;
+//    and writes the exchange back into the same stage at k1 * (32 C + C) + n2 * C + c: a warp
+//    reads 32 / C rows k1 of C entries each, and the C-entry pad per row shifts consecutive rows
+//    by C bank pairs, so the transposed reads are conflict-free, and every address is the
+//    thread's base plus a compile-time offset;
 //  - thread (k1, c) reads Y[0..31][k1], runs the 32-point DFT and accumulates |X| f^j for its 32
 //    output rows k1 + N1 k2 in registers.
 // Waits on the stage barriers are bounded: an expired wait sets the status word and every thread
@@ -29,7 +32,7 @@
 namespace hf {
 namespace {
 
-constexpr int kColC = 8; // columns per CTA strip
+constexpr int kColC = kColMomCols; // columns per CTA strip
 
 __device__ __forceinline__ bool wait_stage(uint64_t *mbar, uint32_t parity, volatile int *abort, int *status) {
   const uint64_t t0 = tc::globaltimer_ns();
@@ -55,7 +58,7 @@ __global__ void __launch_bounds__(32 * C, 1)
   constexpr int      kBoxRows = N < 256 ? N : 256;
   constexpr int      kBoxes   = N / kBoxRows;
   constexpr uint32_t kStage   = (uint32_t)N * C * sizeof(float2); // bytes one plane's boxes bring
-  constexpr int      kXRow    = 32 * C + 8;                      // exchange row (one k1) in float2
+  constexpr int      kXRow    = 32 * C + C;                      // exchange row (one k1) in float2
   constexpr int      kSlot    = (N1 * kXRow + 15) / 16 * 16;    // stage slot (128-byte multiple)
   extern __shared__ __align__(128) uint8_t smem[];
   float2   *stage      = reinterpret_cast<float2 *>(smem);     // [2][kSlot]
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(32 * C, 1)
 template <int N1> int launch_n1(const CUtensorMap &tmap, const ColMomArgs &a, const MomentSpec &m, int nwin,
                                 cudaStream_t s) {
   constexpr int N    = N1 * 32;
-  const size_t  slot = (size_t)(N1 * (32 * kColC + 8) + 15) / 16 * 16;
+  const size_t  slot = (size_t)(N1 * (32 * kColC + kColC) + 15) / 16 * 16;
   const size_t  smem = 2 * slot * sizeof(float2) + (size_t)N * sizeof(float2) + 32;
   auto          kern = a.fast ? col_moments_tma_kernel<N1, kColC, true> : col_moments_tma_kernel<N1, kColC, false>;
   HF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

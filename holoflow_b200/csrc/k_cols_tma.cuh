@@ -17,8 +17,11 @@ struct ColMomArgs {
   int     fast;          // chosen form: hardware square-root approximation, fused moment sums
 };
 
+// Columns per CTA strip of the pass.
+constexpr int kColMomCols = 4;
+
 // `tmap`: 2D float32 tensor map over the band planes viewed as [rows][2 * W] (complex as two
-// floats), box [H or 256 rows][16 floats], so window w, plane k, row r is tensor row
+// floats), box [H or 256 rows][2 * kColMomCols floats], so window w, plane k, row r is tensor row
 // w * rows_per_win + k * H + r.
 bool col_moments_tma_supported(int H, int W);
 int  launch_col_moments_tma(const CUtensorMap &tmap, const ColMomArgs &a, const MomentSpec &m, int nwin,

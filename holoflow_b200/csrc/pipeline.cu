@@ -543,7 +543,8 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
     p->raw_tc  = tc_band && (p->filter2d || p->af);
     if (d.propagation == HF_PROP_FRESNEL && p->fast && col_moments_tma_supported(d.height, d.width)) {
       const uint64_t rows = (uint64_t)B * p->nz * d.height;
-      if ((rc = make_tmap_2d_f32(&p->band_tmap, p->band, 2 * (uint64_t)d.width, rows, 8 * (uint64_t)d.width, 16,
+      if ((rc = make_tmap_2d_f32(&p->band_tmap, p->band, 2 * (uint64_t)d.width, rows, 8 * (uint64_t)d.width,
+                                 2 * kColMomCols,
                                  (uint32_t)std::min(d.height, 256))))
         break;
       p->cols_tma = true;

@@ -19,6 +19,13 @@ LOG="$OUT/build_attempt.log"
 INC=(-I "$REF/src/curaii/include" -I "$REF/src/holoflow/include" -I "$REF/src/holoflow/src"
      -I "$REF/src/holoflow_event/include" -I "$REF/src/holonp/include" -I "$REF/src/holonp/src"
      -I "$REF/src/holotask/include" -I "$REF/src/holotask/src")
+# Header-only copies of two of the fetched dependencies ship inside installed Python packages
+# (nlohmann/json with cudnn_frontend, spdlog with flashinfer); use them when present, so that the
+# attempt gets past the first missing header.
+SITE="$(python3 -c 'import sysconfig; print(sysconfig.get_paths()["purelib"])' 2>/dev/null)"
+for d in "$SITE/include/cudnn_frontend/thirdparty" "$SITE/flashinfer/data/spdlog/include"; do
+  if [ -d "$d" ]; then INC+=(-I "$d"); echo "include $d" >> "$LOG"; fi
+done
 FILES=(src/holotask/src/syncs/fresnel_diffraction.cu src/holotask/src/syncs/angular_spectrum.cu
        src/holotask/src/syncs/pca.cc src/holotask/src/syncs/pca_heev.cc
        src/holonp/src/fft.cu src/holonp/src/rfft.cu src/holonp/src/mean.cu
