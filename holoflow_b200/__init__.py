@@ -24,6 +24,8 @@ HF_NORM_BACKWARD, HF_NORM_FORWARD, HF_NORM_ORTHO = 0, 1, 2
 HF_PROP_NONE, HF_PROP_FRESNEL, HF_PROP_ANGULAR_SPECTRUM = 0, 1, 2
 HF_M0, HF_M1, HF_M2 = 1, 2, 4
 HF_FORM_PLAIN, HF_FORM_CHOSEN = 0, 1
+# band-DFT pass of a plan (hf_plan_band_pass)
+HF_BAND_FP32, HF_BAND_TC_ROWS, HF_BAND_TC_RAW_ROWS, HF_BAND_TC_SEGMENTS = 0, 1, 2, 3
 HF_STFD_LOCAL, HF_STFD_GLOBAL = 0, 1
 HF_STFD_COMPLEX, HF_STFD_MAGNITUDE, HF_STFD_MEAN_MAGNITUDE = 0, 1, 2
 HF_SHSLOPES_SINGLE_REFERENCE, HF_SHSLOPES_FULL_PAIRWISE = 0, 1
@@ -107,6 +109,7 @@ _PROTOS = {
     "hf_plan_set_z": (C.c_int, [_vp, _f32, _vp]),
     "hf_plan_output_shape": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
     "hf_plan_device_bytes": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "hf_plan_band_pass": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "hf_pipeline_exec": (C.c_int, [_vp, _vp, _i64, _i64, C.c_int, _vp, _vp]),
     "hf_pipeline_inspect": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "hf_plan_timing": (C.c_int, [_vp, C.c_int]),

@@ -29,4 +29,10 @@ struct BandRowsArgs {
 bool band_rows_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes);
 int  launch_band_rows_tc(const BandRowsArgs &a, int fmt, cudaStream_t s);
 
+// Raw band planes (no lens, no row FFT) in row segments on the tensor cores (k_tc_band_seg.cu):
+// T = 32, 64 or 128, W a multiple of 128, Nz <= 64.  Uses ring, T, H, W, nz, wmat, wmat_stride,
+// out, out_win / out_plane / out_row, nwin, shift, status, max_ctas and row_counter of `a`.
+bool band_seg_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes);
+int  launch_band_seg_tc(const BandRowsArgs &a, int fmt, cudaStream_t s);
+
 } // namespace hf

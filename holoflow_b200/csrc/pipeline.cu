@@ -100,6 +100,7 @@ struct hf_plan {
   bool       cov_tc = false;   // tensor-core Gram matrix (chosen form)
   bool       rows_tc = false;  // tensor-core band DFT fused with lens + row FFT (chosen form)
   bool       raw_tc = false;   // tensor-core band DFT storing raw planes (chosen form, Filter2D or autofocus)
+  bool       seg_tc = false;   // tensor-core raw band planes in row segments (chosen form, other shapes)
   bool       cols_tma = false; // TMA-fed column FFT + moments over `band` through band_tmap
   CUtensorMap band_tmap{};
   size_t     bytes = 0;
@@ -238,9 +239,12 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     return cols_moments(p, nwin, out, s);
   }
 
-  int rec = p->timer.begin(s, ST_BAND);
-  if (p->raw_tc && (reinterpret_cast<uintptr_t>(fr.base) & 15) == 0) {
-    // chosen form with a step before the lens: the tensor-core band DFT stores the raw planes
+  int        rec        = p->timer.begin(s, ST_BAND);
+  const bool aligned16  = (reinterpret_cast<uintptr_t>(fr.base) & 15) == 0;
+  bool       lens_fused = false; // the band pass multiplied the planes by the Fresnel lens
+  if ((p->raw_tc || p->seg_tc) && aligned16) {
+    // chosen form, raw planes on the tensor cores: whole rows (T = 64, before Filter2D or the
+    // autofocus) or row segments (the other shapes)
     BandRowsArgs br{};
     br.ring = fr, br.T = d.frames, br.H = d.height, br.W = d.width, br.nz = p->nz;
     br.wmat = wmat, br.wmat_stride = wstride, br.lens = nullptr, br.out = p->band, br.raw = 1;
@@ -248,7 +252,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     br.out_win = win_px, br.out_plane = p->P, br.out_row = d.width, br.nwin = nwin, br.shift = 2048.f;
     br.status = p->status, br.max_ctas = std::max(1, sm_count() - reserve_sms);
     br.row_counter = p->row_counter;
-    HF_TRY(launch_band_rows_tc(br, d.input_dtype, s));
+    HF_TRY(p->raw_tc ? launch_band_rows_tc(br, d.input_dtype, s) : launch_band_seg_tc(br, d.input_dtype, s));
   } else {
     BandArgs ba{};
     ba.ring = fr, ba.T = d.frames, ba.P = p->P, ba.H = d.height, ba.W = d.width, ba.nz = p->nz;
@@ -257,6 +261,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     ba.out = p->band, ba.OH = d.height, ba.OW = d.width, ba.oy = 0, ba.ox = 0;
     ba.out_plane = p->P, ba.out_win = win_px, ba.scale = 1.0f;
     HF_TRY(launch_band_dft(ba, d.input_dtype, nwin, s));
+    lens_fused = ba.lens != nullptr;
   }
   if (p->filter2d) // band planes -> FFT2 x annulus -> IFFT2, in place, before the lens
     HF_TRY(launch_filter2d(p->f2d, (int64_t)nwin * p->nz, d.height, d.width, 0, p->band, p->band, p->band2, nullptr, s));
@@ -278,7 +283,7 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     rp.in = p->band, rp.in_real = 0, rp.in_win = win_px, rp.in_plane = p->P, rp.in_row = d.width, rp.in_col = 1;
     rp.IH = d.height, rp.IW = d.width, rp.H = d.height, rp.N = d.width, rp.nplanes = p->nz, rp.inverse = 0;
     rp.out = p->fast ? p->band : p->band2, rp.out_win = win_px, rp.out_plane = p->P, rp.out_row = d.width;
-    rp.pre = p->filter2d ? p->lens : nullptr; // the lens, when the band pass could not fuse it
+    rp.pre = lens_fused ? nullptr : p->lens; // the lens, when the band pass did not fuse it
     int64_t zero_first = 0;                   // leading windows without a delayed window
     if (p->af) {
       // per window: passes 1..n-1 correct the planes in place, the last pass's correction is
@@ -541,6 +546,10 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
                          band_rows_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
     p->rows_tc = tc_band && !p->filter2d && !p->af;
     p->raw_tc  = tc_band && (p->filter2d || p->af);
+    // every other chosen-form shape the segment pass takes (T = 32 / 128, wide rows, two-sided
+    // band, angular spectrum): raw band planes on the tensor cores, the lens in the row pass
+    p->seg_tc = d.form == HF_FORM_CHOSEN && !p->rows_tc && !p->raw_tc &&
+                band_seg_tc_supported(d.input_dtype, T, d.width, p->nz, p->frame_bytes);
     if (d.propagation == HF_PROP_FRESNEL && p->fast && col_moments_tma_supported(d.height, d.width)) {
       const uint64_t rows = (uint64_t)B * p->nz * d.height;
       if ((rc = make_tmap_2d_f32(&p->band_tmap, p->band, 2 * (uint64_t)d.width, rows, 8 * (uint64_t)d.width,
@@ -600,6 +609,12 @@ int hf_plan_output_shape(const hf_plan *p, int32_t *oh, int32_t *ow, int32_t *nm
 int hf_plan_device_bytes(const hf_plan *p, size_t *bytes) {
   HF_CHECK_ARG(p != nullptr && bytes != nullptr, "hf_plan_device_bytes: null argument");
   *bytes = p->bytes;
+  return HF_OK;
+}
+
+int hf_plan_band_pass(const hf_plan *p, int *kind) {
+  HF_CHECK_ARG(p != nullptr && kind != nullptr, "hf_plan_band_pass: null argument");
+  *kind = p->rows_tc ? HF_BAND_TC_ROWS : p->raw_tc ? HF_BAND_TC_RAW_ROWS : p->seg_tc ? HF_BAND_TC_SEGMENTS : HF_BAND_FP32;
   return HF_OK;
 }
 

@@ -141,6 +141,13 @@ class Pipeline:
         check(lib().hf_plan_device_bytes(self._plan, C.byref(b)))
         return b.value
 
+    def band_pass(self) -> int:
+        """Which band-DFT pass the plan runs: HF_BAND_FP32, HF_BAND_TC_ROWS, HF_BAND_TC_RAW_ROWS or
+        HF_BAND_TC_SEGMENTS."""
+        k = C.c_int()
+        check(lib().hf_plan_band_pass(self._plan, C.byref(k)))
+        return k.value
+
     def set_z(self, z: float, stream=None) -> None:
         check(lib().hf_plan_set_z(self._plan, z, _stream(stream)))
 

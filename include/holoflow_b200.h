@@ -235,6 +235,16 @@ int hf_plan_set_z(hf_plan *plan, float z, hf_stream_t s);
 int hf_plan_output_shape(const hf_plan *plan, int32_t *out_h, int32_t *out_w, int32_t *n_moments);
 /* Bytes of device memory the plan holds. */
 int hf_plan_device_bytes(const hf_plan *plan, size_t *bytes);
+/* Which band-DFT pass the plan runs (for 16-byte-aligned frame rings; a misaligned ring takes the
+ * FP32 pass): HF_BAND_FP32 (the plain form's tiled SIMT DFT), HF_BAND_TC_ROWS (tensor cores fused
+ * with the lens and the row FFT), HF_BAND_TC_RAW_ROWS (tensor cores, raw planes of whole rows, before
+ * Filter2D or the autofocus) or HF_BAND_TC_SEGMENTS (tensor cores, raw planes in row segments: the
+ * other chosen-form shapes). */
+#define HF_BAND_FP32 0
+#define HF_BAND_TC_ROWS 1
+#define HF_BAND_TC_RAW_ROWS 2
+#define HF_BAND_TC_SEGMENTS 3
+int hf_plan_band_pass(const hf_plan *plan, int *kind);
 
 /* Runs `nwin` (<= max_batch) windows.  Window w consists of frames
  * ring + ((first_frame + w*hop + t) mod ring_frames) * frame_bytes, t = 0..T-1, i.e. windows of

@@ -326,3 +326,28 @@ def test_two_sided_fft_time_method(cuda, form, prop, H):
     one = pl.Pipeline(pl.PipelineConfig(**{**cfg.__dict__, "time_method": hf.HF_TIME_RFFT}))
     got1 = one.run(ring, n, 0, nwin).cpu().numpy()
     assert O.rel_l2(got1[0, 1], got[0, 1]) > 0.1
+
+
+@pytest.mark.parametrize("T,hop,H,W,prop,fmt,lo,hi,fs", [
+    (32, 32, 128, 256, 2, "u16", 6e3, 18e3, 37e3),        # config-0 shape class: T = 32, angular spectrum
+    (128, 32, 64, 384, 1, "mono12p", 4e3, 33e3, 67e3),    # T = 128: 56 bins (N = 112), 3 tiles
+    (64, 16, 64, 1536, 1, "mono12p", 4e3, 33e3, 67e3),    # 12 tiles: segments of 8 and 4
+    (32, 8, 96, 1280, 0, "u16", 6e3, 18e3, 37e3),         # no propagation, 10 tiles in one segment
+])
+def test_chosen_form_segment_band_pass(cuda, T, hop, H, W, prop, fmt, lo, hi, fs):
+    """Shapes the fused row pass does not take run the tensor-core band DFT in row segments (raw
+    planes, lens in the row pass); the moments match the FP64 oracle within the chosen form's
+    tolerance, and the plain form's FP32 band DFT within its own."""
+    import holoflow_b200 as hf
+    from holoflow_b200 import pipeline as pl
+    nwin = 3
+    n = T + hop * (nwin - 1)
+    z0, z1 = O.band_bins(lo, hi, fs, T)
+    frames = S.Interferograms(S.SynthConfig(H, W, n, fs, int(0.8 * min(H, W)), 0.25, seed=1077)).frames(0, n)
+    kw = dict(height=H, width=W, frames=T, hop=hop, z_begin=z0, z_end=z1, fs=fs, z=0.25, clutter_rank=4,
+              propagation=prop)
+    for form, tol, kind in ((hf.HF_FORM_CHOSEN, 1e-3, hf.HF_BAND_TC_SEGMENTS), (hf.HF_FORM_PLAIN, 1e-4, hf.HF_BAND_FP32)):
+        got, p = _run(cuda, frames, dict(kw, form=form), nwin, fmt=fmt)
+        assert p.band_pass() == kind
+        assert p.status() == 0
+        _check(got, frames, kw, nwin, tol)
