@@ -71,8 +71,10 @@ template <int N, bool INV> __device__ __forceinline__ float2 twmul_c(float2 b, i
   return cmul(b, w);
 }
 
-// Radix-2 butterfly (a, b) <- (a + w b, a - w b), w = exp(-+2 pi i k/N).  Trivial angles cost
-// adds only; the others six fused multiply-adds through the tangent form of w.
+// Radix-2 butterfly (a, b) <- (a + w b, a - w b), w = exp(-+2 pi i k/N).  w = +-1 and w = -+i cost
+// one packed fp32x2 add and one packed subtract (of b or its swapped, negated pair); the other
+// angles go through the tangent form of w: two scalar fused multiply-adds for (u, v) = w b / m,
+// then two packed ones for a +- m (u, v).  Every lane rounds exactly as the scalar form would.
 template <int N, bool INV> __device__ __forceinline__ void bfly(float2 &a, float2 &b, int k) {
   k %= N;
   if (k == 0 || 4 * k == N || 2 * k == N || 4 * k == 3 * N) {
@@ -82,15 +84,15 @@ template <int N, bool INV> __device__ __forceinline__ void bfly(float2 &a, float
   } else if (tw_near_real(k, N)) { // w = m (1 + i t); the inverse uses w* = m (1 - i t)
     const float2 mt = ctwt<N>(k);
     const float  m = mt.x, t = INV ? -mt.y : mt.y;
-    const float  u = fmaf(-t, b.y, b.x), v = fmaf(t, b.x, b.y);
-    b              = make_float2(fmaf(-m, u, a.x), fmaf(-m, v, a.y));
-    a              = make_float2(fmaf(m, u, a.x), fmaf(m, v, a.y));
+    const float2 uv = make_float2(fmaf(-t, b.y, b.x), fmaf(t, b.x, b.y));
+    b               = cfma2(make_float2(-m, -m), uv, a);
+    a               = cfma2(make_float2(m, m), uv, a);
   } else { // w = m (t + i); the inverse uses w* = (-m)(-t + i)
     const float2 mt = ctwt<N>(k);
     const float  m = INV ? -mt.x : mt.x, t = INV ? -mt.y : mt.y;
-    const float  u = fmaf(t, b.x, -b.y), v = fmaf(t, b.y, b.x);
-    b              = make_float2(fmaf(-m, u, a.x), fmaf(-m, v, a.y));
-    a              = make_float2(fmaf(m, u, a.x), fmaf(m, v, a.y));
+    const float2 uv = make_float2(fmaf(t, b.x, -b.y), fmaf(t, b.y, b.x));
+    b               = cfma2(make_float2(-m, -m), uv, a);
+    a               = cfma2(make_float2(m, m), uv, a);
   }
 }
 
