@@ -281,8 +281,8 @@ __global__ void __launch_bounds__(kBandTcThr, 1) band_rows_tc_kernel(BandRowsArg
         for (int j = 0; j < NTILE; ++j)
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
-            const float2 sv = make_float2(__uint_as_float(v[j][2 * b]) + cs[8 * g + 2 * b],
-                                          __uint_as_float(v[j][2 * b + 1]) + cs[8 * g + 2 * b + 1]);
+            const float2 sv = cadd(make_float2(__uint_as_float(v[j][2 * b]), __uint_as_float(v[j][2 * b + 1])),
+                                   reinterpret_cast<const float2 *>(cs)[4 * g + b]);
             tbuf[b * RS + 128 * j + 32 * q + lane] = cmul(sv, L[j]);
           }
         named_bar(bar, 128);

@@ -261,8 +261,9 @@ __global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(BandRowsArgs a,
             for (int b = 0; b < 4; ++b) {
               const int bin = 4 * (g0 + gi) + b;
               if (gi < ng && bin < a.nz)
-                op[(int64_t)bin * a.out_plane] = make_float2(__uint_as_float(v[gi][2 * b]) + cs[2 * bin],
-                                                             __uint_as_float(v[gi][2 * b + 1]) + cs[2 * bin + 1]);
+                op[(int64_t)bin * a.out_plane] =
+                    cadd(make_float2(__uint_as_float(v[gi][2 * b]), __uint_as_float(v[gi][2 * b + 1])),
+                         reinterpret_cast<const float2 *>(cs)[bin]);
             }
         }
       }
