@@ -89,6 +89,7 @@ _PROTOS = {
     "hf_covariance": (C.c_int, [_vp, C.c_int, _i64, C.c_int, _i64, _vp, _vp, _vp]),
     "hf_covariance_noalloc": (C.c_int, [_vp, C.c_int, _i64, C.c_int, _i64, _vp, _vp]),
     "hf_eigh_jacobi_f64": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _i64, _vp]),
+    "hf_eigh_top_f64": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _i64, _vp]),
     "hf_pca_project": (C.c_int, [_vp, _i64, C.c_int, _i64, _vp, C.c_int, C.c_int, _vp, _vp]),
     "hf_band_matrix": (C.c_int, [_vp, _i64, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),
     "hf_fresnel_plan_create": (C.c_int, [_i64, C.c_int, C.c_int, C.c_int, _f32, _f32, _f32, C.c_int,

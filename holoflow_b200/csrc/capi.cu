@@ -139,6 +139,13 @@ int hf_eigh_jacobi_f64(const double *a, double *evecs, double *evals, int *info,
   return launch_jacobi(a, evecs, evals, info, n, batch, s);
 }
 
+int hf_eigh_top_f64(const double *a, double *evecs, double *evals, int *info, int n, int r, int64_t batch,
+                    hf_stream_t s) {
+  clear_error();
+  HF_CHECK_ARG(a != nullptr && evecs != nullptr && evals != nullptr, "hf_eigh_top_f64: null pointer");
+  return launch_eig_top(a, evecs, evals, info, n, r, batch, s);
+}
+
 int hf_pca_project(const float *in, int64_t batch, int T, int64_t P, const double *evecs,
                    int begin, int end, float *out, hf_stream_t s) {
   clear_error();

@@ -42,6 +42,15 @@ int launch_covariance_fixed_scratch(const FrameRing &ring, int fmt, int T, int64
 int launch_jacobi(const double *a, double *evecs, double *evals, int *info, int n, int64_t batch,
                   cudaStream_t s);
 
+// The r largest eigenpairs of symmetric n x n float64 matrices (k_eig_top.cu): Householder
+// tridiagonalisation, Sturm multisection, inverse iteration, back-transformation.  Writes
+// evals[n - r .. n - 1] (ascending) and the matching columns of evecs ([n][n]); info 0, or 1 for a
+// non-finite input.
+bool   eig_top_supported(int n, int r);
+size_t eig_top_smem_bytes(int n);
+int    launch_eig_top(const double *a, double *evecs, double *evals, int *info, int n, int r, int64_t batch,
+                      cudaStream_t s);
+
 // W = (I - V V^T) D[:, z0:z1] as complex64 [batch][T][nz]; V = last `rank` columns of evecs.
 // two_sided: columns for bins [z0, z1) then [T - z1, T - z0) (2 (z1 - z0) columns)
 int launch_band_matrix(const double *evecs, int64_t batch, int T, int rank, int z0, int z1,

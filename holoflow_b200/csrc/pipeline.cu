@@ -184,7 +184,12 @@ static int phase_cov(hf_plan *p, const FrameRing &fr, int nwin, double *gram, cu
 static int phase_eigen(hf_plan *p, const FilterSet &fs, int nwin, cudaStream_t s) {
   const hf_desc &d   = p->d;
   const int      rec = p->timer.begin(s, ST_EIGEN);
-  HF_TRY(launch_jacobi(fs.gram, fs.evecs, fs.evals, fs.info, d.frames, nwin, s));
+  // the filter needs the clutter_rank largest eigenvectors only: tridiagonalisation + multisection +
+  // inverse iteration; the full Jacobi solve for ranks beyond that solver's limit
+  if (eig_top_supported(d.frames, d.clutter_rank))
+    HF_TRY(launch_eig_top(fs.gram, fs.evecs, fs.evals, fs.info, d.frames, d.clutter_rank, nwin, s));
+  else
+    HF_TRY(launch_jacobi(fs.gram, fs.evecs, fs.evals, fs.info, d.frames, nwin, s));
   HF_TRY(launch_band_matrix(fs.evecs, nwin, d.frames, d.clutter_rank, d.z_begin, d.z_end, fs.wmat, s,
                             d.time_method == HF_TIME_FFT));
   p->timer.end(s, rec);

@@ -71,6 +71,17 @@ def eigh_jacobi(a: torch.Tensor):
     return evals, evecs, info
 
 
+def eigh_top(a: torch.Tensor, r: int):
+    """The r largest eigenpairs: (evals [batch][r] ascending, evecs [batch][n][r], info)."""
+    batch, n, _ = a.shape
+    a = a.contiguous()
+    evecs = torch.zeros_like(a)
+    evals = torch.zeros((batch, n), dtype=torch.float64, device=a.device)
+    info = torch.empty((batch,), dtype=torch.int32, device=a.device)
+    check(lib().hf_eigh_top_f64(_ptr(a), _ptr(evecs), _ptr(evals), _ptr(info), n, r, batch, _stream()))
+    return evals[:, n - r:], evecs[:, :, n - r:], info
+
+
 @dataclass
 class PipelineConfig:
     height: int

@@ -126,6 +126,12 @@ int    hf_covariance_noalloc(const void *in, int in_dtype, int64_t batch, int T,
  * convergence, else the number of sweeps run (non-converged). */
 int hf_eigh_jacobi_f64(const double *a, double *evecs, double *evals, int *info, int n,
                        int64_t batch, hf_stream_t s);
+/* The r largest eigenpairs only (the clutter filter's need), n <= 128, 1 <= r <= min(16, n):
+ * Householder tridiagonalisation, Sturm multisection, inverse iteration, back-transformation, one
+ * CTA per matrix.  Same layout as hf_eigh_jacobi_f64, but only evals[b][n - r .. n - 1] (ascending)
+ * and the matching columns of evecs[b] are written.  info[b] = 0, or 1 when a[b] is not finite. */
+int hf_eigh_top_f64(const double *a, double *evecs, double *evals, int *info, int n, int r, int64_t batch,
+                    hf_stream_t s);
 
 /* Projection onto eigenvectors [begin, end) (pca.cc:106-116): out[b][c][p] =
  * sum_t X_b[t][p] * evecs_b[t][begin + c].  in: float32 [batch][T][P]. */

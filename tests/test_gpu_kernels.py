@@ -181,6 +181,51 @@ def test_jacobi_matches_eigh(cuda, rng, n):
         assert np.abs(V[b].T @ V[b] - np.eye(n)).max() < 1e-12
 
 
+@pytest.mark.parametrize("n,r", [(64, 4), (128, 4), (64, 16), (17, 3), (2, 2), (1, 1)])
+def test_top_eigenpairs_match_eigh(cuda, rng, n, r):
+    """The clutter filter's top-r solver (tridiagonalisation, Sturm multisection, inverse
+    iteration): eigenvalues, residuals, orthonormality and the top-r projector against numpy, on
+    Gram matrices of 12-bit-like data (magnitudes ~1e12) and on indefinite symmetric matrices."""
+    import torch
+    hf, pl = _hf()
+    B = 3
+    x = rng.integers(0, 4096, size=(B, n, 2000)).astype(np.float64) - 2048
+    a = np.einsum("bij,bkj->bik", x, x)
+    m = rng.standard_normal((B, n, n))
+    a[1] = m[1] + m[1].T
+    ev, V, info = pl.eigh_top(torch.from_numpy(a).to(cuda), r)
+    ev, V, info = ev.cpu().numpy(), V.cpu().numpy(), info.cpu().numpy()
+    assert (info == 0).all()
+    for b in range(B):
+        w, U = np.linalg.eigh(a[b])
+        scale = np.abs(w).max()
+        assert np.abs(ev[b] - w[n - r:]).max() <= 1e-12 * scale
+        assert np.all(np.diff(ev[b]) >= 0)
+        assert np.abs(V[b].T @ V[b] - np.eye(r)).max() < 1e-12
+        assert np.abs(a[b] @ V[b] - V[b] * ev[b]).max() <= 1e-12 * scale
+        if n > r and (w[n - r] - w[n - r - 1]) > 1e-6 * scale:  # a separated top-r subspace
+            P, Q = V[b] @ V[b].T, U[:, n - r:] @ U[:, n - r:].T
+            assert np.abs(P - Q).max() < 1e-9
+
+
+def test_top_eigenpairs_repeated_and_nonfinite(cuda, rng):
+    """A repeated top eigenvalue gets an orthonormal basis of its eigenspace; a non-finite input
+    reports info = 1 and leaves the outputs alone."""
+    import torch
+    hf, pl = _hf()
+    q, _ = np.linalg.qr(rng.standard_normal((64, 64)))
+    lam = np.concatenate([np.arange(60.0), [100.0, 100.0, 200.0, 300.0]])
+    a = np.stack([q @ np.diag(lam) @ q.T, np.full((64, 64), np.nan)])
+    ev, V, info = pl.eigh_top(torch.from_numpy(a).to(cuda), 4)
+    ev, V, info = ev.cpu().numpy(), V.cpu().numpy(), info.cpu().numpy()
+    assert list(info) == [0, 1]
+    assert np.abs(ev[0] - [100, 100, 200, 300]).max() < 1e-11
+    assert np.abs(V[0].T @ V[0] - np.eye(4)).max() < 1e-12
+    P, Q = V[0] @ V[0].T, q[:, 60:] @ q[:, 60:].T
+    assert np.abs(P - Q).max() < 1e-10
+    assert not V[1].any() and not ev[1].any()
+
+
 def test_jacobi_reference_pca_kat(cuda):
     """pca_test.cu:134-145 through the GPU Gram + Jacobi: energies of the projections are the
     ascending eigenvalues {1, 3}."""
