@@ -979,7 +979,10 @@ int hf_stream_process(hf_stream *st, int max_windows, float *out, int out_is_hos
       st->look_base  = base + n;
       st->look_n     = n2;
       st->look_set   = nxt;
-      reserve        = n2; // one SM per lookahead Jacobi
+      // the full Jacobi solve (ranks beyond the top-r solver) takes ~1 ms per 64 x 64 matrix: keep
+      // one SM per lookahead matrix free of the persistent band pass; the top-r solver finishes
+      // within the columns pass that follows, so the band pass takes every SM
+      reserve = eig_top_supported(d.frames, d.clutter_rank) ? 0 : n2;
     }
     // 3. this batch's propagation
     HF_TRY(phase_propagate(p, win_ring(base), n, p->set[cur].wmat, wstride, dst, s, reserve));
