@@ -11,8 +11,8 @@
 //     32 shifts at once, each lane counting the sign changes of the leading-minor sequence
 //     p_j = (d_j - x) p_{j-1} - e_{j-1}^2 p_{j-2} (rescaled by powers of two, no division), and the
 //     bracket shrinks 33x per round;
-//  3. their eigenvectors of T by inverse iteration (Wilkinson): two solves with the tridiagonal LU
-//     factorisation of T - lambda I with partial pivoting, pivots floored at eps ||T||, from
+//  3. their eigenvectors of T by inverse iteration (Wilkinson): three solves with the tridiagonal
+//     LU factorisation of T - lambda I with partial pivoting, pivots floored at eps ||T||, from
 //     distinct starting vectors, orthonormalised (modified Gram-Schmidt) within clusters of close
 //     eigenvalues after each solve;
 //  4. back-transformation V_r = Q Y by the reflectors in reverse order, a warp per column.
