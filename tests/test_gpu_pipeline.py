@@ -66,14 +66,18 @@ def test_pipeline_config0_angular_spectrum(cuda):
     _check(got, frames, kw, 2, 1e-4)
 
 
-def test_pipeline_variants_fftshift_m0_none_padding(cuda):
+@pytest.mark.parametrize("form,tol", [(0, 1e-4), (1, 1e-3)])
+def test_pipeline_variants_fftshift_m0_none_padding(cuda, form, tol):
+    """Display and propagation variants in both forms (the chosen form runs them through the
+    tensor-core segment pass at T = 32)."""
     frames = S.Interferograms(S.config0(48)).frames(0, 48)[:, :128, :128].copy()
     base = dict(height=128, width=128, frames=32, hop=16, z_begin=6, z_end=16, fs=37e3, z=0.3)
     for extra in (dict(fftshift=1), dict(moment_mask=1), dict(propagation=0), dict(clutter_rank=2),
                   dict(propagation=2, pad_w=256, pad_h=256), dict(propagation=2, fftshift=1, moment_mask=5)):
         kw = {**base, **extra}
-        got, _ = _run(cuda, frames, kw, 2)
-        _check(got, frames, kw, 2, 1e-4)
+        got, p = _run(cuda, frames, dict(kw, form=form), 2)
+        assert p.status() == 0
+        _check(got, frames, kw, 2, tol)
 
 
 def test_pipeline_ring_wraparound(cuda):
