@@ -35,8 +35,8 @@ RING_FRAMES = 256               # 403 MB of packed frames (> 126 MB L2)
 METRIC = "1024²×64 M0 images/s and p99 frame-to-image latency, chosen vs plain form"
 E2E_STEPS = 200                 # end-to-end steps timed (p99 over this many latency samples)
 DTYPE = {"chosen": "u12 frames; i8 Gram and f16 hi+lo band DFT on tcgen05 tensor cores (f32 accumulate); "
-                   "f32 FFTs and moments; f64 Jacobi",
-         "plain": "u12 frames; f32 Gram, band DFT, FFTs and moments; f64 Jacobi"}
+                   "f32 FFTs and moments; f64 top-r eigenpairs",
+         "plain": "u12 frames; f32 Gram, band DFT, FFTs and moments; f64 top-r eigenpairs"}
 WORKLOAD = "config1: 1024x1024 12-bit packed, T=64 hop=16, fs=67kHz, top-4 SVD clutter filter, Fresnel z=0.25m, M0/M1/M2 4-33kHz"
 
 
@@ -269,6 +269,7 @@ def run_batched(args, local, steps=None):
     # one graph launch, chosen form, tuned schedule
     m = Multi([cfg(a, 1) for a in acqs])
     streams, tuned_ms = m.tune(rings, nfr, first, outs, reps=3)
+    schedule = m.schedule()
     for _ in range(args.warmup):
         m.exec(rings, nfr, first, outs)
     torch.cuda.synchronize()
@@ -287,7 +288,10 @@ def run_batched(args, local, steps=None):
         "baseline_plain_per_acquisition": {"value": round(nwin / (plain_ms / 1000.0), 2), "ms_per_step":
                                            round(plain_ms, 4)},
         "speedup_vs_plain_per_acquisition": round(plain_ms / graph_ms, 3),
-        "schedule": {"branches": abs(streams), "assignment": "largest-first" if streams > 0 else "round-robin",
+        "schedule": {"branches": schedule["branches"],
+                     "assignment": "largest-first" if schedule["largest_first"] else "round-robin",
+                     "fused_segment_passes": bool(schedule["fused"]),
+                     "seg_tiles": schedule["seg_tiles"] or "max", "band_ctas": schedule["band_ctas"] or "all",
                      "tuned_ms": round(tuned_ms, 4)},
         "config": {"workload": "config3: 16 seeded acquisitions, sizes 256^2..1536x1024, T 32/64/128 hop T/4, "
                                "z 0.15-0.40 m, fs 37/67 kHz, top-4 clutter filter, Fresnel, M0/M1/M2",

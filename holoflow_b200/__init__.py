@@ -75,6 +75,12 @@ class HfTDesc(C.Structure):
     _fields_ = [("rank", C.c_int32), ("dtype", C.c_int32), ("mem_loc", C.c_int32), ("reserved", C.c_int32),
                 ("shape", C.c_int64 * 8), ("strides", C.c_int64 * 8), ("offset", C.c_int64)]
 
+class HfMultiSchedule(C.Structure):
+    """hf_multi_schedule: branches, assignment, fusion of the segment band passes and its tile
+    parameters."""
+    _fields_ = [("branches", C.c_int32), ("largest_first", C.c_int32), ("fused", C.c_int32),
+                ("seg_tiles", C.c_int32), ("band_ctas", C.c_int32)]
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "hf_last_error": (C.c_char_p, []),
@@ -141,6 +147,8 @@ _PROTOS = {
     "hf_multi_tune": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(C.c_int),
                                 C.POINTER(_vp), C.c_int, _vp, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "hf_multi_plan": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "hf_multi_get_schedule": (C.c_int, [_vp, C.POINTER(HfMultiSchedule)]),
+    "hf_multi_set_schedule": (C.c_int, [_vp, C.POINTER(HfMultiSchedule)]),
     "hf_node_kinds": (C.c_int, [C.c_char_p, _sz]),
     "hf_node_infer": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(HfTDesc), C.POINTER(C.c_int),
                                 C.POINTER(HfTDesc), C.c_int]),

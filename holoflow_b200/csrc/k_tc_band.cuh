@@ -35,4 +35,12 @@ int  launch_band_rows_tc(const BandRowsArgs &a, int fmt, cudaStream_t s);
 bool band_seg_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes);
 int  launch_band_seg_tc(const BandRowsArgs &a, int fmt, cudaStream_t s);
 
+// One persistent segment pass over up to kMaxSegJobs acquisitions of the same T and format: the
+// units of all jobs form one work list taken from `counter` (zeroed by the launcher).  seg_cap > 0
+// caps the tiles per segment; max_ctas > 0 caps the grid.  Each job uses the fields of `a` listed
+// above except status, max_ctas and row_counter.
+constexpr int kMaxSegJobs = 16;
+int launch_band_seg_tc_multi(const BandRowsArgs *jobs, int njobs, int fmt, int seg_cap, int max_ctas, int *counter,
+                             int *status, cudaStream_t s);
+
 } // namespace hf

@@ -21,6 +21,11 @@
 //                adds the DC correction and stores each bin's 32 pixels as one coalesced row.
 // mbarriers `full` (MMAs of a segment complete: TMEM readable, A/B reusable) and `free` (the 8
 // epilogue warps finished reading TMEM), with bounded waits as in the fused pass.
+//
+// One launch can serve several acquisitions of the same window length and sample format (the
+// batched uneven acquisitions): each is a job with its own ring, W, planes and geometry, and the
+// units of all jobs form one work list, (job, window, row, segment) in order, taken from the one
+// counter.
 #include <algorithm>
 #include <initializer_list>
 
@@ -53,8 +58,38 @@ struct SegGeom {
   int spr;  // segments per row
 };
 
+// One acquisition of a launch.
+struct SegJob {
+  FrameRing     ring;
+  const float2 *wmat;
+  int64_t       wmat_stride;
+  float2       *out;
+  int64_t       out_win, out_plane, out_row;
+  int64_t       unit0; // first unit of this job in the launch's work list
+  int           H, W, nz, nwin;
+  float         shift;
+  SegGeom       g;
+};
+
+struct SegJobs {
+  int     njob;
+  int     bpart_max; // bytes of one W part at the largest N of the launch
+  int64_t nunits;    // units of all jobs
+  int    *status;
+  int    *counter;
+  SegJob  job[kMaxSegJobs];
+};
+
+// Job of unit u (the jobs' first units ascend).
+__device__ __forceinline__ int job_of(const SegJobs &J, int64_t u) {
+  int ji = 0;
+  while (ji + 1 < J.njob && u >= J.job[ji + 1].unit0)
+    ++ji;
+  return ji;
+}
+
 template <int FMT, int T>
-__global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(BandRowsArgs a, SegGeom g) {
+__global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(const __grid_constant__ SegJobs J) {
   constexpr int KA   = (T + 63) / 64; // 64-frame K atoms of B
   constexpr int KS   = T / 16;        // k-steps per W part
   constexpr int TILE = T * 256;       // A tile bytes: [T][128] f16
@@ -64,8 +99,7 @@ __global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(BandRowsArgs a,
   uint8_t  *smem   = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t  *sA     = smem;                                        // g.seg tiles
   uint8_t  *sB     = sA + kSegABytes;                             // hi [KA][N][128 B], then lo
-  const int bpart  = KA * g.N * 128;
-  float    *colsum = reinterpret_cast<float *>(sB + 2 * bpart);   // [2][128], by window parity
+  float    *colsum = reinterpret_cast<float *>(sB + 2 * J.bpart_max); // [2][128], by window parity
   int64_t  *foff   = reinterpret_cast<int64_t *>(colsum + 256);   // [T] frame offsets of the window
   int64_t  *unitbuf = foff + 128;                                 // [2] unit of iteration k, by parity
   uint64_t *mbar   = reinterpret_cast<uint64_t *>(unitbuf + 2);   // [0] full, [1] free
@@ -86,35 +120,40 @@ __global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(BandRowsArgs a,
   tc::fence_after_sync();
   const uint32_t tbase  = *tslot;
   volatile int  *abortv = abort_flag;
-  const int      ntile  = a.W / 128;
-  const int64_t  nunits = (int64_t)a.nwin * a.H * g.spr;
+  const int64_t  nunits = J.nunits;
 
   if (tid < kSegLoaders) {
     // ------------------------------------------------------------------ loader / MMA warps
-    int k = 0, cur_w = -1, wpar = 1;
+    int k = 0, cur_ji = -1, cur_w = -1, wpar = 1;
     for (;; ++k) {
       if (k > 0) // MMAs of the previous segment done: A and B may be overwritten
-        wait_or_abort(&mbar[0], (uint32_t)((k - 1) & 1), abortv, a.status, 31);
+        wait_or_abort(&mbar[0], (uint32_t)((k - 1) & 1), abortv, J.status, 31);
       if (tid == 0)
-        unitbuf[k & 1] = atomicAdd(a.row_counter, 1);
+        unitbuf[k & 1] = atomicAdd(J.counter, 1);
       named_bar(1, kSegLoaders);
       const int64_t u = unitbuf[k & 1];
       if (u >= nunits) { // no segments left: complete this phase empty so that the epilogue ends too
         if (tid == 0) {
           // only after the epilogue has released the previous segment (see the fused pass)
           if (k > 0)
-            wait_or_abort(&mbar[1], (uint32_t)((k - 1) & 1), abortv, a.status, 34);
+            wait_or_abort(&mbar[1], (uint32_t)((k - 1) & 1), abortv, J.status, 34);
           mbar_arrive_cnt(&mbar[0], 2);
         }
         break;
       }
-      const int     w   = (int)(u / ((int64_t)a.H * g.spr));
-      const int64_t rem = u % ((int64_t)a.H * g.spr);
+      const int     ji  = job_of(J, u);
+      const SegJob &a   = J.job[ji];
+      const SegGeom g   = a.g;
+      const int     bpart = KA * g.N * 128;
+      const int64_t uj  = u - a.unit0;
+      const int     w   = (int)(uj / ((int64_t)a.H * g.spr));
+      const int64_t rem = uj % ((int64_t)a.H * g.spr);
       const int     r = (int)(rem / g.spr), sg = (int)(rem % g.spr);
-      const int     j0 = sg * g.seg, nt = min(g.seg, ntile - j0);
-      const bool    new_w = w != cur_w;
+      const int     j0 = sg * g.seg, nt = min(g.seg, a.W / 128 - j0);
+      const bool    new_w = w != cur_w || ji != cur_ji;
       if (new_w) { // per window: frame offsets and B = (Wh, Wl) rows n = 2 bin + {re, im}
-        cur_w = w;
+        cur_ji = ji;
+        cur_w  = w;
         wpar ^= 1;
         for (int t = tid; t < T; t += kSegLoaders)
           foff[t] = a.ring.frame(w, t) - a.ring.base;
@@ -206,7 +245,7 @@ __global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(BandRowsArgs a,
       named_bar(1, kSegLoaders);
       if (tid == 0) {
         if (k > 0) // the epilogue has read the previous segment out of TMEM
-          wait_or_abort(&mbar[1], (uint32_t)((k - 1) & 1), abortv, a.status, 32);
+          wait_or_abort(&mbar[1], (uint32_t)((k - 1) & 1), abortv, J.status, 32);
         tc::fence_after_sync();
         if (!*abortv) {
           const uint32_t idesc = tc::idesc_f16(128, g.N, true, false);
@@ -227,20 +266,25 @@ __global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(BandRowsArgs a,
   } else {
     // ------------------------------------------------------------------ epilogue warps
     const int e = warp - 4, q = warp & 3, half = e >> 2;
-    const int ngrp = (2 * a.nz + 7) / 8; // 8-column groups = 4 bins
-    int       k = 0, cur_w = -1, wpar = 1;
+    int       k = 0, cur_ji = -1, cur_w = -1, wpar = 1;
     for (;; ++k) {
-      wait_or_abort(&mbar[0], (uint32_t)(k & 1), abortv, a.status, 33);
+      wait_or_abort(&mbar[0], (uint32_t)(k & 1), abortv, J.status, 33);
       tc::fence_after_sync();
       const int64_t u = unitbuf[k & 1];
       if (u >= nunits || *abortv)
         break;
-      const int     w   = (int)(u / ((int64_t)a.H * g.spr));
-      const int64_t rem = u % ((int64_t)a.H * g.spr);
+      const int     ji   = job_of(J, u);
+      const SegJob &a    = J.job[ji];
+      const SegGeom g    = a.g;
+      const int     ngrp = (2 * a.nz + 7) / 8; // 8-column groups = 4 bins
+      const int64_t uj   = u - a.unit0;
+      const int     w    = (int)(uj / ((int64_t)a.H * g.spr));
+      const int64_t rem  = uj % ((int64_t)a.H * g.spr);
       const int     r = (int)(rem / g.spr), sg = (int)(rem % g.spr);
-      const int     j0 = sg * g.seg, nt = min(g.seg, ntile - j0);
-      if (w != cur_w) {
-        cur_w = w;
+      const int     j0 = sg * g.seg, nt = min(g.seg, a.W / 128 - j0);
+      if (w != cur_w || ji != cur_ji) {
+        cur_ji = ji;
+        cur_w  = w;
         wpar ^= 1;
       }
       const float *cs   = colsum + wpar * 128;
@@ -281,37 +325,28 @@ __global__ void __launch_bounds__(kSegThr, 1) band_seg_tc_kernel(BandRowsArgs a,
   }
 }
 
-SegGeom seg_geom(int T, int W, int nz) {
+// seg_cap > 0 caps the tiles per segment (the autotuner's tile parameter); 0 takes the most that A
+// and TMEM hold.
+SegGeom seg_geom(int T, int W, int nz, int seg_cap) {
   SegGeom g{};
   g.N    = 16 * ((2 * nz + 15) / 16);
   g.ncol = g.N <= 32 ? 32 : (g.N <= 64 ? 64 : 128);
   g.seg  = std::min({512 / g.ncol, kSegABytes / (T * 256), W / 128});
+  if (seg_cap > 0)
+    g.seg = std::min(g.seg, seg_cap);
   g.spr  = (W / 128 + g.seg - 1) / g.seg;
   return g;
 }
 
-template <int FMT, int T> int launch_t(const BandRowsArgs &a, cudaStream_t s) {
-  constexpr int KA   = (T + 63) / 64;
-  const SegGeom g    = seg_geom(T, a.W, a.nz);
-  const size_t  smem = 1024 + (size_t)kSegABytes + 2 * (size_t)KA * g.N * 128 + 256 * 4 + 128 * 8 + 2 * 8 + 2 * 8 +
-                      16;
+template <int FMT, int T> int launch_t(SegJobs &J, int max_ctas, cudaStream_t s) {
+  const size_t smem = 1024 + (size_t)kSegABytes + 2 * (size_t)J.bpart_max + 256 * 4 + 128 * 8 + 2 * 8 + 2 * 8 + 16;
   HF_CUDA(cudaFuncSetAttribute(band_seg_tc_kernel<FMT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int64_t nunits = (int64_t)a.nwin * a.H * g.spr;
-  const int     cap    = a.max_ctas > 0 ? std::min(a.max_ctas, sm_count()) : sm_count();
-  const int     grid   = (int)std::min<int64_t>(nunits, cap);
-  HF_CHECK_ARG(a.row_counter != nullptr, "band segments: row counter missing");
-  HF_CUDA(cudaMemsetAsync(a.row_counter, 0, sizeof(int), s));
-  band_seg_tc_kernel<FMT, T><<<grid, kSegThr, smem, s>>>(a, g);
+  const int cap  = max_ctas > 0 ? std::min(max_ctas, sm_count()) : sm_count();
+  const int grid = (int)std::min<int64_t>(J.nunits, cap);
+  HF_CUDA(cudaMemsetAsync(J.counter, 0, sizeof(int), s));
+  band_seg_tc_kernel<FMT, T><<<grid, kSegThr, smem, s>>>(J);
   note_launch();
   return launch_status("band_seg_tc_kernel");
-}
-
-template <int FMT> int launch_fmt(const BandRowsArgs &a, cudaStream_t s) {
-  switch (a.T) {
-  case 32: return launch_t<FMT, 32>(a, s);
-  case 64: return launch_t<FMT, 64>(a, s);
-  default: return launch_t<FMT, 128>(a, s);
-  }
 }
 
 } // namespace
@@ -321,11 +356,39 @@ bool band_seg_tc_supported(int fmt, int T, int W, int nz, int64_t frame_bytes) {
          nz >= 1 && 2 * nz <= kSegMaxN && frame_bytes % 16 == 0;
 }
 
+int launch_band_seg_tc_multi(const BandRowsArgs *jobs, int njobs, int fmt, int seg_cap, int max_ctas, int *counter,
+                             int *status, cudaStream_t s) {
+  HF_CHECK_ARG(jobs != nullptr && njobs >= 1 && njobs <= kMaxSegJobs, "band segments: 1 to 16 jobs per launch");
+  HF_CHECK_ARG(counter != nullptr, "band segments: unit counter missing");
+  const int T = jobs[0].T;
+  SegJobs   J{};
+  J.njob = njobs, J.status = status, J.counter = counter;
+  for (int i = 0; i < njobs; ++i) {
+    const BandRowsArgs &a = jobs[i];
+    HF_CHECK_ARG(a.T == T, "band segments: the jobs of one launch share the window length");
+    HF_CHECK_ARG(band_seg_tc_supported(fmt, a.T, a.W, a.nz, a.ring.frame_bytes),
+                 "band segments (tensor core): unsupported shape");
+    HF_CHECK_ARG(((uintptr_t)a.ring.base & 15) == 0, "band segments (tensor core): ring must be 16-byte aligned");
+    HF_CHECK_ARG(a.nwin >= 1 && a.H >= 1, "band segments: empty job");
+    SegJob &j = J.job[i];
+    j.ring = a.ring, j.wmat = a.wmat, j.wmat_stride = a.wmat_stride, j.out = a.out;
+    j.out_win = a.out_win, j.out_plane = a.out_plane, j.out_row = a.out_row;
+    j.H = a.H, j.W = a.W, j.nz = a.nz, j.nwin = a.nwin, j.shift = a.shift;
+    j.g     = seg_geom(T, a.W, a.nz, seg_cap);
+    j.unit0 = J.nunits;
+    J.nunits += (int64_t)a.nwin * a.H * j.g.spr;
+    J.bpart_max = std::max(J.bpart_max, ((T + 63) / 64) * j.g.N * 128);
+  }
+  switch (T) {
+  case 32: return fmt == HF_MONO12P ? launch_t<HF_MONO12P, 32>(J, max_ctas, s) : launch_t<HF_U16, 32>(J, max_ctas, s);
+  case 64: return fmt == HF_MONO12P ? launch_t<HF_MONO12P, 64>(J, max_ctas, s) : launch_t<HF_U16, 64>(J, max_ctas, s);
+  default:
+    return fmt == HF_MONO12P ? launch_t<HF_MONO12P, 128>(J, max_ctas, s) : launch_t<HF_U16, 128>(J, max_ctas, s);
+  }
+}
+
 int launch_band_seg_tc(const BandRowsArgs &a, int fmt, cudaStream_t s) {
-  HF_CHECK_ARG(band_seg_tc_supported(fmt, a.T, a.W, a.nz, a.ring.frame_bytes),
-               "band segments (tensor core): unsupported shape");
-  HF_CHECK_ARG(((uintptr_t)a.ring.base & 15) == 0, "band segments (tensor core): ring must be 16-byte aligned");
-  return fmt == HF_MONO12P ? launch_fmt<HF_MONO12P>(a, s) : launch_fmt<HF_U16>(a, s);
+  return launch_band_seg_tc_multi(&a, 1, fmt, 0, a.max_ctas, a.row_counter, a.status, s);
 }
 
 } // namespace hf

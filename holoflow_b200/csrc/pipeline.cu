@@ -220,14 +220,16 @@ static int cols_moments(hf_plan *p, int nwin, float *out, cudaStream_t s) {
   return HF_OK;
 }
 
+static int phase_band(hf_plan *p, const FrameRing &fr, int nwin, const float2 *wmat, int64_t wstride, cudaStream_t s,
+                      int reserve_sms, bool *lens_fused, int *rec);
+static int phase_after_band(hf_plan *p, int nwin, float *out, cudaStream_t s, bool lens_fused, int rec);
+
 // Band DFT with W (per window, or shared when wstride == 0), propagation and moments.
 // `reserve_sms` SMs are left to concurrently running work by the persistent tensor-core pass.
 static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const float2 *wmat, int64_t wstride,
                            float *out, cudaStream_t s, int reserve_sms) {
   const hf_desc &d      = p->d;
   const int64_t  win_px = (int64_t)p->nz * p->P;
-  const int64_t  oplane = (int64_t)p->OH * p->OW;
-  const int64_t  owin   = (int64_t)p->nmom * oplane;
   const bool     rows_tc = p->rows_tc && (reinterpret_cast<uintptr_t>(fr.base) & 15) == 0;
 
   if (rows_tc) { // chosen form: tensor-core band DFT + lens + row FFT, then columns + moments
@@ -244,9 +246,21 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     return cols_moments(p, nwin, out, s);
   }
 
-  int        rec        = p->timer.begin(s, ST_BAND);
+  bool lens_fused = false;
+  int  rec        = -1;
+  HF_TRY(phase_band(p, fr, nwin, wmat, wstride, s, reserve_sms, &lens_fused, &rec));
+  return phase_after_band(p, nwin, out, s, lens_fused, rec);
+}
+
+// The band DFT of the paths other than the fused row pass, into p->band.  `lens_fused`: the pass
+// multiplied the planes by the Fresnel lens.  `rec` is the band stage's open timer record.
+static int phase_band(hf_plan *p, const FrameRing &fr, int nwin, const float2 *wmat, int64_t wstride, cudaStream_t s,
+                      int reserve_sms, bool *lens_fused, int *rec) {
+  const hf_desc &d      = p->d;
+  const int64_t  win_px = (int64_t)p->nz * p->P;
+  *rec                  = p->timer.begin(s, ST_BAND);
   const bool aligned16  = (reinterpret_cast<uintptr_t>(fr.base) & 15) == 0;
-  bool       lens_fused = false; // the band pass multiplied the planes by the Fresnel lens
+  *lens_fused           = false;
   if ((p->raw_tc || p->seg_tc) && aligned16) {
     // chosen form, raw planes on the tensor cores: whole rows (T = 64, before Filter2D or the
     // autofocus) or row segments (the other shapes)
@@ -266,8 +280,18 @@ static int phase_propagate(hf_plan *p, const FrameRing &fr, int nwin, const floa
     ba.out = p->band, ba.OH = d.height, ba.OW = d.width, ba.oy = 0, ba.ox = 0;
     ba.out_plane = p->P, ba.out_win = win_px, ba.scale = 1.0f;
     HF_TRY(launch_band_dft(ba, d.input_dtype, nwin, s));
-    lens_fused = ba.lens != nullptr;
+    *lens_fused = ba.lens != nullptr;
   }
+  return HF_OK;
+}
+
+// Everything after the band DFT: Filter2D, the autofocus, propagation and moments of the band
+// planes in p->band.  `rec`: the band stage's timer record, closed after Filter2D.
+static int phase_after_band(hf_plan *p, int nwin, float *out, cudaStream_t s, bool lens_fused, int rec) {
+  const hf_desc &d      = p->d;
+  const int64_t  win_px = (int64_t)p->nz * p->P;
+  const int64_t  oplane = (int64_t)p->OH * p->OW;
+  const int64_t  owin   = (int64_t)p->nmom * oplane;
   if (p->filter2d) // band planes -> FFT2 x annulus -> IFFT2, in place, before the lens
     HF_TRY(launch_filter2d(p->f2d, (int64_t)nwin * p->nz, d.height, d.width, 0, p->band, p->band, p->band2, nullptr, s));
   p->timer.end(s, rec);
@@ -1025,3 +1049,46 @@ int hf_stream_output_wait(hf_stream *st, hf_stream_t s, int host_block) {
 }
 
 } // extern "C"
+
+// ---- split form of hf_pipeline_exec for the multi-acquisition executor --------------------------
+namespace hf {
+
+int pipeline_front(hf_plan *p, const void *ring, int64_t ring_frames, int64_t first, int nwin, cudaStream_t s) {
+  HF_CHECK_ARG(p != nullptr && ring != nullptr, "pipeline front: null argument");
+  HF_CHECK_ARG(nwin >= 1 && nwin <= p->d.max_batch, "pipeline front: nwin must be in [1, max_batch]");
+  HF_CHECK_ARG(ring_frames >= p->d.frames && first >= 0, "pipeline front: the ring must hold at least one window");
+  if (p->d.clutter_rank > 0) {
+    const FrameRing fr = ring_of(p, ring, ring_frames, first);
+    HF_TRY(phase_cov(p, fr, nwin, p->set[0].gram, s));
+    HF_TRY(phase_eigen(p, p->set[0], nwin, s));
+  }
+  return HF_OK;
+}
+
+bool pipeline_seg_eligible(const hf_plan *p, const void *ring) {
+  return p != nullptr && p->seg_tc && (reinterpret_cast<uintptr_t>(ring) & 15) == 0;
+}
+
+int pipeline_seg_job(hf_plan *p, const void *ring, int64_t ring_frames, int64_t first, int nwin, BandRowsArgs *job) {
+  HF_CHECK_ARG(job != nullptr && pipeline_seg_eligible(p, ring), "pipeline segment job: the plan does not take the segment pass");
+  HF_CHECK_ARG(nwin >= 1 && nwin <= p->d.max_batch, "pipeline segment job: nwin must be in [1, max_batch]");
+  const hf_desc &d = p->d;
+  BandRowsArgs   br{};
+  br.ring = ring_of(p, ring, ring_frames, first), br.T = d.frames, br.H = d.height, br.W = d.width, br.nz = p->nz;
+  br.wmat        = d.clutter_rank > 0 ? p->set[0].wmat : p->wmat_plain;
+  br.wmat_stride = d.clutter_rank > 0 ? (int64_t)d.frames * p->nz : 0;
+  br.lens = nullptr, br.out = p->band, br.raw = 1;
+  br.out_win = (int64_t)p->nz * p->P, br.out_plane = p->P, br.out_row = d.width, br.nwin = nwin, br.shift = 2048.f;
+  br.status = p->status, br.row_counter = p->row_counter;
+  *job = br;
+  return HF_OK;
+}
+
+int pipeline_back(hf_plan *p, int nwin, float *out, cudaStream_t s) {
+  HF_CHECK_ARG(p != nullptr && out != nullptr, "pipeline back: null argument");
+  return phase_after_band(p, nwin, out, s, false, -1);
+}
+
+int *plan_status_word(hf_plan *p) { return p ? p->status : nullptr; }
+
+} // namespace hf

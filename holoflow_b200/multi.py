@@ -1,5 +1,6 @@
 """Many acquisitions of uneven size in one CUDA graph launch (hf_multi_*), with the schedule
-autotuner."""
+autotuner: branches and assignment, and the fused segment band pass (one persistent launch per
+window length and format) with its tiles per segment and grid cap."""
 from __future__ import annotations
 
 import ctypes as C
@@ -7,7 +8,7 @@ from typing import Optional, Sequence
 
 import torch
 
-from . import HfDesc, check, lib
+from . import HfDesc, HfMultiSchedule, check, lib
 from .pipeline import PipelineConfig, _stream
 
 
@@ -38,6 +39,16 @@ class Multi:
         bs, bm = C.c_int(), C.c_float()
         check(lib().hf_multi_tune(self._m, r, rf, f, nw, o, reps, _stream(stream), C.byref(bs), C.byref(bm)))
         return bs.value, bm.value
+
+    def schedule(self) -> dict:
+        sch = HfMultiSchedule()
+        check(lib().hf_multi_get_schedule(self._m, C.byref(sch)))
+        return {f: getattr(sch, f) for f, _ in HfMultiSchedule._fields_}
+
+    def set_schedule(self, branches: int = 1, largest_first: int = 1, fused: int = 0, seg_tiles: int = 0,
+                     band_ctas: int = 0) -> None:
+        sch = HfMultiSchedule(branches, largest_first, fused, seg_tiles, band_ctas)
+        check(lib().hf_multi_set_schedule(self._m, C.byref(sch)))
 
     def close(self) -> None:
         if self._m:

@@ -351,12 +351,24 @@ int     hf_server_open_count(const hf_server *server);
  * may all differ).  hf_multi_exec reconstructs nwin[i] (NULL: max_batch) windows of every
  * acquisition i from its device ring (rings[i], ring_frames[i], first window frame first[i]) into
  * outs[i] ([nwin][n_moments][OH][OW] float32) as ONE CUDA graph launch on `s`: the graph forks
- * into branches that each run a share of the acquisitions and joins at the end.  hf_multi_tune
- * times candidate schedules (number of branches; largest-first or round-robin assignment) on the
- * given buffers and keeps the fastest; *best_streams receives the branch count (negative for
- * round-robin) and *best_ms the time of one launch.  The graph is captured on the first exec (and
- * again whenever the buffers or the schedule change): make that call outside any other capture. */
+ * into branches that each run a share of the acquisitions and joins at the end.  With a fused
+ * schedule, the acquisitions whose band pass is the tensor-core segment pass (hf_plan_band_pass
+ * HF_BAND_TC_SEGMENTS) and that share a window length and sample format run that pass as ONE
+ * persistent launch over all their (window, row, segment) units, between their Gram/eigen/W
+ * fronts and their row/column backs; the images are the same as without fusion.  hf_multi_tune
+ * times candidate schedules on the given buffers and keeps the fastest: the number of branches and
+ * the assignment (largest-first or round-robin), then fusion with its tile parameters (tiles per
+ * segment, grid cap).  *best_streams receives the branch count (negative for round-robin) and
+ * *best_ms the time of one launch.  The graph is captured on the first exec (and again whenever
+ * the buffers or the schedule change): make that call outside any other capture. */
 typedef struct hf_multi hf_multi;
+typedef struct hf_multi_schedule {
+  int32_t branches;      /* 1 .. 6 */
+  int32_t largest_first; /* 1: acquisitions dealt largest-first to the least-loaded branch; 0: round-robin */
+  int32_t fused;         /* 1: one segment-pass launch per (window length, format) */
+  int32_t seg_tiles;     /* tiles per segment of the fused launch; 0 = the most A and TMEM hold */
+  int32_t band_ctas;     /* grid cap of the fused launch; 0 = every SM */
+} hf_multi_schedule;
 int hf_multi_create(int n_acquisitions, const hf_desc *descs, hf_multi **multi);
 int hf_multi_destroy(hf_multi *multi);
 int hf_multi_exec(hf_multi *multi, const void *const *rings, const int64_t *ring_frames, const int64_t *first,
@@ -365,6 +377,10 @@ int hf_multi_tune(hf_multi *multi, const void *const *rings, const int64_t *ring
                   const int *nwin, float *const *outs, int reps, hf_stream_t s, int *best_streams, float *best_ms);
 /* The plan of acquisition i (owned by the multi). */
 int hf_multi_plan(hf_multi *multi, int i, hf_plan **plan);
+/* Read or set the schedule (hf_multi_tune sets it; a set schedule is checked and used from the next
+ * exec). */
+int hf_multi_get_schedule(const hf_multi *multi, hf_multi_schedule *schedule);
+int hf_multi_set_schedule(hf_multi *multi, const hf_multi_schedule *schedule);
 
 /* ---- node layer: compute nodes by kind string (ISyncTaskFactory / ISyncTask, tasks.hh:182-304;
  * kinds registered by string, registry.hh:24-68, manager.cc:159-237) ---------------------------

@@ -18,6 +18,7 @@ STRUCTS = {
     "hf_ellipse": (hf.HfEllipse, {}),
     "hf_holo_header": (hf.HoloHeader, {}),
     "hf_tdesc": (hf.HfTDesc, {}),
+    "hf_multi_schedule": (hf.HfMultiSchedule, {}),
 }
 
 
