@@ -99,10 +99,12 @@ __global__ void __launch_bounds__(32 * C, 1)
       issue(1, 1);
   }
 
-  float acc0[32], acc1[32], acc2[32];
+  // moment sums of output rows (k2, k2 + 1) as packed pairs: each fp32x2 add / multiply / FMA
+  // rounds every lane as its scalar form, so the sums are those of the scalar sequence
+  float2 acc0[16], acc1[16], acc2[16];
 #pragma unroll
-  for (int k2 = 0; k2 < 32; ++k2)
-    acc0[k2] = acc1[k2] = acc2[k2] = 0.f;
+  for (int i = 0; i < 16; ++i)
+    acc0[i] = acc1[i] = acc2[i] = make_float2(0.f, 0.f);
   volatile int *abortv = abort_flag;
 
   for (int plane = 0; plane < a.nz; ++plane) {
@@ -130,20 +132,24 @@ __global__ void __launch_bounds__(32 * C, 1)
       for (int j = 0; j < 32; ++j)
         y[j] = st[k1 * kXRow + j * C + c];
       dft_reg<32, false>(y);
-      const float f1 = m.w1[plane], f2 = m.w2[plane];
+      const float2 f1 = make_float2(m.w1[plane], m.w1[plane]), f2 = make_float2(m.w2[plane], m.w2[plane]);
 #pragma unroll
-      for (int k2 = 0; k2 < 32; ++k2) {
+      for (int i = 0; i < 16; ++i) {
+        float2 mag;
         if constexpr (FAST) { // sqrt.approx (relative error ~2^-22) and fused weighted sums
-          float mag;
-          asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(mag) : "f"(fmaf(y[k2].x, y[k2].x, y[k2].y * y[k2].y)));
-          acc0[k2] += mag;
-          acc1[k2] = fmaf(f1, mag, acc1[k2]);
-          acc2[k2] = fmaf(f2, mag, acc2[k2]);
+          asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(mag.x) : "f"(fmaf(y[2 * i].x, y[2 * i].x, y[2 * i].y * y[2 * i].y)));
+          asm("sqrt.approx.ftz.f32 %0, %1;"
+              : "=f"(mag.y)
+              : "f"(fmaf(y[2 * i + 1].x, y[2 * i + 1].x, y[2 * i + 1].y * y[2 * i + 1].y)));
+          acc0[i] = cadd(acc0[i], mag);
+          acc1[i] = cfma2(f1, mag, acc1[i]);
+          acc2[i] = cfma2(f2, mag, acc2[i]);
         } else { // the reference's float32 sequence: sqrtf(x*x + y*y), then sums in band order
-          const float mag = __fsqrt_rn(__fmaf_rn(y[k2].x, y[k2].x, __fmul_rn(y[k2].y, y[k2].y)));
-          acc0[k2]        = __fadd_rn(acc0[k2], mag);
-          acc1[k2]        = __fadd_rn(acc1[k2], __fmul_rn(f1, mag));
-          acc2[k2]        = __fadd_rn(acc2[k2], __fmul_rn(f2, mag));
+          mag.x   = __fsqrt_rn(__fmaf_rn(y[2 * i].x, y[2 * i].x, __fmul_rn(y[2 * i].y, y[2 * i].y)));
+          mag.y   = __fsqrt_rn(__fmaf_rn(y[2 * i + 1].x, y[2 * i + 1].x, __fmul_rn(y[2 * i + 1].y, y[2 * i + 1].y)));
+          acc0[i] = cadd(acc0[i], mag);
+          acc1[i] = cadd(acc1[i], pmul2(f1, mag));
+          acc2[i] = cadd(acc2[i], pmul2(f2, mag));
         }
       }
     }
@@ -163,12 +169,12 @@ __global__ void __launch_bounds__(32 * C, 1)
   for (int mo = 0; mo < 3; ++mo) {
     if (!(m.mask & (1 << mo)))
       continue;
-    const float *acc = mo == 0 ? acc0 : (mo == 1 ? acc1 : acc2);
+    const float2 *acc = mo == 0 ? acc0 : (mo == 1 ? acc1 : acc2);
 #pragma unroll
     for (int k2 = 0; k2 < 32; ++k2) {
       const int row = k1 + N1 * k2;
       const int rr  = m.fftshift ? (row + N / 2) % N : row;
-      out[mi * a.out_plane + (int64_t)rr * a.out_row + cc] = __fdiv_rn(acc[k2], nzf);
+      out[mi * a.out_plane + (int64_t)rr * a.out_row + cc] = __fdiv_rn((k2 & 1) ? acc[k2 >> 1].y : acc[k2 >> 1].x, nzf);
     }
     ++mi;
   }
