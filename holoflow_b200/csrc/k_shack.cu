@@ -24,9 +24,11 @@
 //    taper inside the correlation ROI; normalised cross power against the reference spectrum),
 //    transformed in shared memory and stored contiguously.
 //  - shk_cols_kernel<MODE>: a strip of C columns of one image, transposed into shared memory,
-//    transformed along the height, with the post-operation of MODE (complex, |.|, mean of |.| over
-//    the band planes with the per-sub-aperture fftshift fused into the store, or real part x
+//    transformed along the height, with the post-operation of MODE (complex, |.|, or real part x
 //    scale).
+//  - shk_cols_mean_kernel: the same for the mean of |.| over the band planes, kMeanPlanes planes'
+//    strips per transform, the next group's strips arriving by cp.async into a third buffer while
+//    the current group is transformed, and the per-sub-aperture fftshift fused into the store.
 //  - shk_roi_mean_kernel, shk_peak_kernel (first maximum + parabolic refinement, one CTA per map),
 //    shk_slopes_kernel and shk_zfit_kernel (one thread each: the reference's float32 sequences),
 //    shk_zernike_phase_kernel, shk_correct_phase_kernel, shk_wrap2pi_kernel.
@@ -584,13 +586,13 @@ struct ColArgs {
   FastDiv       by_hc;   // h C (plane index of a strip element)
 };
 
+// One image's strip (COL_COMPLEX, COL_MAG, COL_REAL): loads, transform, post-operation.
 template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_cols_kernel(ColArgs a) {
+  static_assert(MODE != COL_MEAN_MAG, "the band mean runs in shk_cols_mean_kernel");
   extern __shared__ __align__(16) float2 sm[];
   __shared__ GPlan spl;
-  const int        h = a.h, C = a.C, P = a.pitch;
-  constexpr int    GB = MODE == COL_MEAN_MAG ? kMeanPlanes : 1; // planes held per buffer
-  float2          *tw = sm, *b0 = sm + h, *b1 = b0 + (size_t)GB * C * P;
-  float           *acc = reinterpret_cast<float *>(b1 + (size_t)GB * C * P); // COL_MEAN_MAG: [h * C]
+  const int h = a.h, C = a.C, P = a.pitch;
+  float2   *tw = sm, *b0 = sm + h, *b1 = b0 + (size_t)C * P;
   for (int e = threadIdx.x; e < h; e += blockDim.x)
     tw[e] = a.tw[e];
   for (int i = threadIdx.x; i < (int)(sizeof(GPlan) / 4); i += blockDim.x)
@@ -598,73 +600,119 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_cols_k
   const int     strip = (int)(blockIdx.x % a.nstrip);
   const int64_t img   = blockIdx.x / a.nstrip;
   const int     x0 = strip * C, cw = min(C, a.w - x0);
-  const int     planes = MODE == COL_MEAN_MAG ? a.planes : 1;
-  const int     lc     = 31 - __clz(C); // C is a power of two
-  if constexpr (MODE == COL_MEAN_MAG)
-    for (int t = threadIdx.x; t < h * C; t += blockDim.x)
-      acc[t] = 0.f;
-  // COL_MEAN_MAG transforms G = 4 planes per call (more work between barriers, narrower strips
-  // and so more CTAs); the strip of plane g sits at rows [g C, g C + C) of the buffers
-  constexpr int G = MODE == COL_MEAN_MAG ? kMeanPlanes : 1;
-  for (int pl = 0; pl < planes; pl += G) {
-    const int ng = min(G, planes - pl);
-    __syncthreads(); // the previous planes' reads of b0/b1 are done
-    constexpr int U = MODE == COL_MEAN_MAG ? 4 : 8; // independent loads in flight per thread
-    for (int t0 = threadIdx.x; t0 < ng * h * C; t0 += U * blockDim.x) {
-      float2 ld[U];
+  const int     lc = 31 - __clz(C); // C is a power of two
+  constexpr int U  = 8;             // independent loads in flight per thread
+  for (int t0 = threadIdx.x; t0 < h * C; t0 += U * blockDim.x) {
+    float2 ld[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int t = t0 + u * blockDim.x;
-        if (t >= ng * h * C)
-          break;
-        const int     g = G > 1 ? fdiv(t, a.by_hc) : 0, r = t - g * h * C, y = r >> lc, c = r & (C - 1);
-        const int64_t src = MODE == COL_MEAN_MAG ? (int64_t)(pl + g) * a.nwin + img : img;
-        ld[u] = c < cw ? a.in[(src * h + y) * (int64_t)a.w + x0 + c] : make_float2(0.f, 0.f);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int t = t0 + u * blockDim.x;
-        if (t >= ng * h * C)
-          break;
-        const int g = G > 1 ? fdiv(t, a.by_hc) : 0, r = t - g * h * C, y = r >> lc, c = r & (C - 1);
-        b0[(g * C + c) * P + y] = ld[u];
-      }
-    }
-    __syncthreads();
-    const float2 *res = fft_rows_smem(b0, b1, P, ng * C, spl, tw, a.inv);
-    for (int t = threadIdx.x; t < h * C; t += blockDim.x) {
+    for (int u = 0; u < U; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= h * C)
+        break;
       const int y = t >> lc, c = t & (C - 1);
-      if (c >= cw)
-        continue;
-      const float2  v = res[c * P + y];
-      const int64_t o = (img * h + y) * (int64_t)a.w + x0 + c;
-      if constexpr (MODE == COL_COMPLEX)
-        a.outc[o] = a.post ? cmul(v, a.post[(int64_t)y * a.w + x0 + c]) : v;
-      else if constexpr (MODE == COL_MAG)
-        a.outf[o] = sqrtf(v.x * v.x + v.y * v.y);
-      else if constexpr (MODE == COL_MEAN_MAG) {
-        float s = acc[t] + sqrtf(v.x * v.x + v.y * v.y); // band order, float32
+      ld[u] = c < cw ? a.in[(img * h + y) * (int64_t)a.w + x0 + c] : make_float2(0.f, 0.f);
+    }
 #pragma unroll
-        for (int g = 1; g < G; ++g)
-          if (g < ng) {
-            const float2 u = res[(g * C + c) * P + y];
-            s += sqrtf(u.x * u.x + u.y * u.y);
-          }
-        acc[t] = s;
-      } else
-        a.outf[o] = v.x * a.scale;
+    for (int u = 0; u < U; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= h * C)
+        break;
+      const int y = t >> lc, c = t & (C - 1);
+      b0[c * P + y] = ld[u];
     }
   }
-  if constexpr (MODE == COL_MEAN_MAG) {
-    const float nz = (float)a.planes;
+  __syncthreads();
+  const float2 *res = fft_rows_smem(b0, b1, P, C, spl, tw, a.inv);
+  for (int t = threadIdx.x; t < h * C; t += blockDim.x) {
+    const int y = t >> lc, c = t & (C - 1);
+    if (c >= cw)
+      continue;
+    const float2  v = res[c * P + y];
+    const int64_t o = (img * h + y) * (int64_t)a.w + x0 + c;
+    if constexpr (MODE == COL_COMPLEX)
+      a.outc[o] = a.post ? cmul(v, a.post[(int64_t)y * a.w + x0 + c]) : v;
+    else if constexpr (MODE == COL_MAG)
+      a.outf[o] = sqrtf(v.x * v.x + v.y * v.y);
+    else
+      a.outf[o] = v.x * a.scale;
+  }
+}
+
+__device__ __forceinline__ void cp_async8(float2 *dst, const float2 *src, bool ok) {
+  // src-size 0 fills the 8 bytes with zeros (columns past the image edge)
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(ok ? 8 : 0)
+               : "memory");
+}
+
+// The band-mean column pass (COL_MEAN_MAG) with its loads overlapped: each group of kMeanPlanes
+// planes' strips arrives by cp.async into a third buffer while the previous group is transformed
+// and accumulated.  |.| = sqrtf(x^2 + y^2) summed in band order in float32, then divided by the
+// plane count.
+__global__ void __launch_bounds__(kShkThreads, 2) shk_cols_mean_kernel(ColArgs a) {
+  extern __shared__ __align__(16) float2 sm[];
+  __shared__ GPlan spl;
+  constexpr int G  = kMeanPlanes;
+  const int     h = a.h, C = a.C, P = a.pitch;
+  float2       *tw = sm, *bx = sm + h, *b1 = bx + (size_t)G * C * P, *by = b1 + (size_t)G * C * P;
+  float        *acc = reinterpret_cast<float *>(by + (size_t)G * C * P); // [h * C]
+  for (int e = threadIdx.x; e < h; e += blockDim.x)
+    tw[e] = a.tw[e];
+  for (int i = threadIdx.x; i < (int)(sizeof(GPlan) / 4); i += blockDim.x)
+    reinterpret_cast<int *>(&spl)[i] = reinterpret_cast<const int *>(a.pl)[i];
+  const int     strip = (int)(blockIdx.x % a.nstrip);
+  const int64_t img   = blockIdx.x / a.nstrip;
+  const int     x0 = strip * C, cw = min(C, a.w - x0);
+  const int     lc = 31 - __clz(C); // C is a power of two
+  for (int t = threadIdx.x; t < h * C; t += blockDim.x)
+    acc[t] = 0.f;
+  // the strip of plane g of a group sits at rows [g C, g C + C) of a buffer, transposed
+  const auto issue = [&](int pl, float2 *dst) {
+    const int ng = min(G, a.planes - pl);
+    for (int t = threadIdx.x; t < ng * h * C; t += blockDim.x) {
+      const int     g = fdiv(t, a.by_hc), r = t - g * h * C, y = r >> lc, c = r & (C - 1);
+      const int64_t src = (int64_t)(pl + g) * a.nwin + img;
+      const bool    ok  = c < cw;
+      cp_async8(dst + (g * C + c) * P + y, a.in + (src * h + y) * (int64_t)a.w + x0 + (ok ? c : 0), ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  float2 *cur = bx, *spare = by;
+  issue(0, cur);
+  for (int pl = 0; pl < a.planes; pl += G) {
+    const int ng = min(G, a.planes - pl);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads(); // every thread's copies of this group have landed
+    if (pl + G < a.planes)
+      issue(pl + G, spare); // the next group streams in during this group's transforms
+    const float2 *res = fft_rows_smem(cur, b1, P, ng * C, spl, tw, a.inv);
     for (int t = threadIdx.x; t < h * C; t += blockDim.x) {
       const int y = t >> lc, c = t & (C - 1);
       if (c >= cw)
         continue;
-      const int yy = a.shift ? (y + h / 2) % h : y;
-      const int xx = a.shift ? (x0 + c + a.w / 2) % a.w : x0 + c;
-      a.outf[(img * h + yy) * (int64_t)a.w + xx] = acc[t] / nz;
+      const float2 v = res[c * P + y];
+      float        s = acc[t] + sqrtf(v.x * v.x + v.y * v.y); // band order, float32
+#pragma unroll
+      for (int g = 1; g < G; ++g)
+        if (g < ng) {
+          const float2 u = res[(g * C + c) * P + y];
+          s += sqrtf(u.x * u.x + u.y * u.y);
+        }
+      acc[t] = s;
     }
+    __syncthreads(); // this group's buffers are read: `cur` takes the copies after next
+    float2 *tmp = cur;
+    cur         = spare;
+    spare       = tmp;
+  }
+  const float nz = (float)a.planes;
+  for (int t = threadIdx.x; t < h * C; t += blockDim.x) {
+    const int y = t >> lc, c = t & (C - 1);
+    if (c >= cw)
+      continue;
+    const int yy = a.shift ? (y + h / 2) % h : y;
+    const int xx = a.shift ? (x0 + c + a.w / 2) % a.w : x0 + c;
+    a.outf[(img * h + yy) * (int64_t)a.w + xx] = acc[t] / nz;
   }
 }
 
@@ -677,7 +725,9 @@ int    col_strip(int h, bool mean) {
 size_t cols_smem(int h, int C, bool mean) {
   const int P = h | 1; // odd pitch: the transposed loads spread over the banks
   const int G = mean ? kMeanPlanes : 1;
-  return (size_t)h * sizeof(float2) + 2 * (size_t)G * C * P * sizeof(float2) + (mean ? (size_t)h * C * sizeof(float) : 0);
+  // the band-mean pass holds a third buffer for the group in flight
+  return (size_t)h * sizeof(float2) + (mean ? 3 : 2) * (size_t)G * C * P * sizeof(float2) +
+         (mean ? (size_t)h * C * sizeof(float) : 0);
 }
 
 template <int MODE> int launch_rows(RowArgs a, cudaStream_t s) {
@@ -698,13 +748,20 @@ template <int MODE> int launch_cols(ColArgs a, int64_t images, cudaStream_t s) {
   a.nstrip        = (a.w + a.C - 1) / a.C;
   a.by_hc         = make_div((uint32_t)(a.h * a.C));
   const size_t sm = cols_smem(a.h, a.C, MODE == COL_MEAN_MAG);
-  HF_CUDA(cudaFuncSetAttribute(shk_cols_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int64_t grid = images * a.nstrip;
   if (grid > INT_MAX)
     return fail(HF_ERR_UNSUPPORTED, "short-time Fresnel: too many column strips");
-  shk_cols_kernel<MODE><<<(unsigned)grid, kShkThreads, sm, s>>>(a);
-  note_launch();
-  return launch_status("shk_cols_kernel");
+  if constexpr (MODE == COL_MEAN_MAG) {
+    HF_CUDA(cudaFuncSetAttribute(shk_cols_mean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    shk_cols_mean_kernel<<<(unsigned)grid, kShkThreads, sm, s>>>(a);
+    note_launch();
+    return launch_status("shk_cols_mean_kernel");
+  } else {
+    HF_CUDA(cudaFuncSetAttribute(shk_cols_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    shk_cols_kernel<MODE><<<(unsigned)grid, kShkThreads, sm, s>>>(a);
+    note_launch();
+    return launch_status("shk_cols_kernel");
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
