@@ -1058,17 +1058,42 @@ __global__ void shk_zernike_phase_kernel(const float *coeffs, ZModes zm, int ny,
 
 // correct_phase_cf32_kernel / correct_phase_f32_to_cf32_kernel (correct_phase.cu:76-106):
 // E exp(-i phi) with the phase map broadcast over the planes.
-__global__ void shk_correct_phase_kernel(const void *in, int complex_in, const float *phase, int64_t total, int64_t plane,
-                                         float2 *out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+// out = in x exp(-i phase) for every plane: one sine/cosine per pixel, then the planes' elements of
+// that pixel in turn (the same values, in place or not, as one sincosf per element)
+__global__ void shk_correct_phase_kernel(const void *in, int complex_in, const float *phase, int64_t planes,
+                                         int64_t plane, float2 *out) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < plane; p += (int64_t)gridDim.x * blockDim.x) {
     float sv, cv;
-    sincosf(phase[i % plane], &sv, &cv);
-    if (complex_in) {
-      const float2 v = static_cast<const float2 *>(in)[i];
-      out[i]         = make_float2(v.x * cv + v.y * sv, v.y * cv - v.x * sv);
-    } else {
-      const float v = static_cast<const float *>(in)[i];
-      out[i]        = make_float2(v * cv, -v * sv);
+    sincosf(phase[p], &sv, &cv);
+    int64_t k = 0;
+    for (; k + 3 < planes; k += 4) { // four independent loads in flight
+      if (complex_in) {
+        float2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          v[u] = static_cast<const float2 *>(in)[(k + u) * plane + p];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          out[(k + u) * plane + p] = make_float2(v[u].x * cv + v[u].y * sv, v[u].y * cv - v[u].x * sv);
+      } else {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          v[u] = static_cast<const float *>(in)[(k + u) * plane + p];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          out[(k + u) * plane + p] = make_float2(v[u] * cv, -v[u] * sv);
+      }
+    }
+    for (; k < planes; ++k) {
+      const int64_t i = k * plane + p;
+      if (complex_in) {
+        const float2 v = static_cast<const float2 *>(in)[i];
+        out[i]         = make_float2(v.x * cv + v.y * sv, v.y * cv - v.x * sv);
+      } else {
+        const float v = static_cast<const float *>(in)[i];
+        out[i]        = make_float2(v * cv, -v * sv);
+      }
     }
   }
 }
@@ -1744,8 +1769,8 @@ int hf_correct_phase(const void *in, int complex_input, const float *phase, int6
   clear_error();
   HF_CHECK_ARG(in != nullptr && phase != nullptr && out != nullptr, "CorrectPhase: null argument");
   HF_CHECK_ARG(planes >= 1 && height >= 1 && width >= 1, "CorrectPhaseFactory: input must not be empty");
-  const int64_t plane = (int64_t)height * width, total = planes * plane;
-  shk_correct_phase_kernel<<<grid_1d(total), 256, 0, s>>>(in, complex_input ? 1 : 0, phase, total, plane,
+  const int64_t plane = (int64_t)height * width;
+  shk_correct_phase_kernel<<<grid_1d(plane), 256, 0, s>>>(in, complex_input ? 1 : 0, phase, planes, plane,
                                                           static_cast<float2 *>(out));
   note_launch();
   return launch_status("shk_correct_phase_kernel");
