@@ -470,7 +470,7 @@ struct RowArgs {
   int64_t       pair0;
 };
 
-template <int MODE> __global__ void __launch_bounds__(kShkThreads, 3) shk_rows_kernel(RowArgs a) {
+template <int MODE> __global__ void __launch_bounds__(kShkThreads, 4) shk_rows_kernel(RowArgs a) {
   extern __shared__ __align__(16) float2 sm[];
   __shared__ GPlan spl;
   const int        n  = a.n;
