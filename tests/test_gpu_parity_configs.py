@@ -51,10 +51,11 @@ def _check_windows(got, frames, cfg, windows, tol, label):
     assert max(errs) < tol, errs
 
 
-@pytest.mark.parametrize("form,T,hop", [(0, 64, 16), (1, 64, 16), (0, 128, 32), (1, 128, 32)])
+@pytest.mark.parametrize("form,T,hop", [(0, 64, 16), (1, 64, 16), (0, 128, 32), (1, 128, 32), (0, 32, 8), (1, 32, 8)])
 def test_frames_1536x1024(cuda, form, T, hop):
     """1536 x 1024 frames (W x H), the largest size of the uneven and streaming workloads: the
-    band pass and row FFT at W = 1536 and the column pass at H = 1024, both forms, both (T, hop)."""
+    band pass and row FFT at W = 1536 and the column pass at H = 1024, both forms, every (T, hop)
+    of those workloads."""
     from holoflow_b200 import pipeline as pl
     H, W, nwin = 1024, 1536, 2
     n = T + hop * (nwin - 1)

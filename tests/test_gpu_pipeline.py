@@ -355,3 +355,4 @@ def test_chosen_form_segment_band_pass(cuda, T, hop, H, W, prop, fmt, lo, hi, fs
         assert p.band_pass() == kind
         assert p.status() == 0
         _check(got, frames, kw, nwin, tol)
+
