@@ -355,7 +355,9 @@ int     hf_server_open_count(const hf_server *server);
  * schedule, the acquisitions whose band pass is the tensor-core segment pass (hf_plan_band_pass
  * HF_BAND_TC_SEGMENTS) and that share a window length and sample format run that pass as ONE
  * persistent launch over all their (window, row, segment) units, between their Gram/eigen/W
- * fronts and their row/column backs; the images are the same as without fusion.  hf_multi_tune
+ * fronts and their row/column backs; the images are the same as without fusion (an expired
+ * bounded wait inside a fused launch sets the status word of the group's first acquisition,
+ * hf_plan_status on hf_multi_plan(multi, i)).  hf_multi_tune
  * times candidate schedules on the given buffers and keeps the fastest: the number of branches and
  * the assignment (largest-first or round-robin), then fusion with its tile parameters (tiles per
  * segment, grid cap).  *best_streams receives the branch count (negative for round-robin) and
