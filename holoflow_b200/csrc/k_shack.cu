@@ -461,7 +461,7 @@ struct RowArgs {
   // ROW_XPACK: images [n_img][h][n] float; ROW_CROSS: spectra [n_img][h][n] complex
   const float  *img;
   const float  *means; // [n_img]
-  Roi           roi;
+  const float  *taper; // [h][n]: the ROI's cosine taper, -1 outside
   int           h;
   const float2 *spec;
   int           ref_img;
@@ -546,9 +546,9 @@ template <int MODE> __global__ void __launch_bounds__(kShkThreads, 4) shk_rows_k
         v = cmul(ld[u], aux[u]);
       } else if constexpr (MODE == ROW_XPACK) {
         const int   r = fdiv(t, spl.by_n), i = t - r * n;
-        const float d = roi_sq_distance(i, s_y[r], n, a.h, a.roi);
+        const float tp = a.taper[(int64_t)s_y[r] * n + i];
         // (v - mean) * 0.5 (1 + cos(pi sqrt(d))) inside the ellipse, 0 outside
-        v = make_float2(d <= 1.0f ? (ld[u].x - a.means[s_off[r]]) * (0.5f * (1.0f + cospif(sqrtf(d)))) : 0.f, 0.f);
+        v = make_float2(tp >= 0.f ? (ld[u].x - a.means[s_off[r]]) * tp : 0.f, 0.f);
       } else { // ROW_CROSS / ROW_PAIR: unit-magnitude cross power moving x conj(reference)
         const float2 mv = ld[u], rf = aux[u];
         const float2 p   = make_float2(mv.x * rf.x + mv.y * rf.y, mv.y * rf.x - mv.x * rf.y);
@@ -804,13 +804,26 @@ int grid_1d(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n +
 // ------------------------------------------------------------------------------------------------
 // compute_means_kernel (cross_correlation2.cu:352-402): mean of the pixels inside the ROI, 0 when
 // none is.
-__global__ void __launch_bounds__(kRedThreads) shk_roi_mean_kernel(const float *img, float *means, int h, int w, Roi roi) {
+// The correlation ROI of every image, once per operator: the cosine taper
+// 0.5 (1 + cos(pi sqrt(d))) where the normalised elliptical distance d <= 1, -1 outside (the taper
+// is >= 0 inside, so the sign is the mask).  The same float32 expressions as evaluated per element
+// before, so the masked mean and the tapered images are unchanged.
+__global__ void shk_roi_taper_kernel(float *taper, int h, int w, Roi roi) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)h * w; i += (int64_t)gridDim.x * blockDim.x) {
+    const int   y = (int)(i / w), x = (int)(i - (int64_t)y * w);
+    const float d = roi_sq_distance(x, y, w, h, roi);
+    taper[i]      = d <= 1.0f ? 0.5f * (1.0f + cospif(sqrtf(d))) : -1.0f;
+  }
+}
+
+// Mean of each image over the ROI (the taper's mask), one CTA per image.
+__global__ void __launch_bounds__(kRedThreads) shk_roi_mean_kernel(const float *img, float *means, int h, int w,
+                                                                    const float *taper) {
   const float *im = img + (int64_t)blockIdx.x * h * w;
   float        sum = 0.f;
   int          cnt = 0;
   for (int i = threadIdx.x; i < h * w; i += blockDim.x) {
-    const int y = i / w, x = i - y * w;
-    if (roi_sq_distance(x, y, w, h, roi) <= 1.0f) {
+    if (taper[i] >= 0.f) {
       sum += im[i];
       ++cnt;
     }
@@ -838,28 +851,52 @@ __device__ __forceinline__ float signed_coord(int p, int n) { return p < (n + 1)
 // recover_phase_correlation_peaks (shack_hartmann_slopes.cu:124-158): the first maximum in
 // row-major order (a strict > scan), found here by a block reduction that keeps the smaller
 // index among equal values; then the parabolic refinement on the circular neighbours.
+// (value, index) of the larger value, the smaller index among equal values (INT_MAX: none yet)
+__device__ __forceinline__ void peak_combine(float &v, int &i, float v2, int i2) {
+  if (i2 != INT_MAX && (i == INT_MAX || v2 > v || (v2 == v && i2 < i)))
+    v = v2, i = i2;
+}
+
 __global__ void __launch_bounds__(kRedThreads) shk_peak_kernel(const float *maps, float2 *shifts, int h, int w) {
   const float *m    = maps + (int64_t)blockIdx.x * h * w;
+  const int    N    = h * w, B = blockDim.x;
   float        best = -FLT_MAX;
   int          bi   = INT_MAX;
-  for (int i = threadIdx.x; i < h * w; i += blockDim.x) {
+  int          i    = threadIdx.x;
+  for (; i + 3 * B < N; i += 4 * B) { // four loads in flight, compared in index order
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      v[u] = m[i + u * B];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (v[u] > best)
+        best = v[u], bi = i + u * B;
+  }
+  for (; i < N; i += B) {
     const float v = m[i];
     if (v > best)
       best = v, bi = i;
   }
-  __shared__ float sv[kRedThreads];
-  __shared__ int   si[kRedThreads];
-  sv[threadIdx.x] = best, si[threadIdx.x] = bi;
+  // the rule picks the same (value, index) in any combining order
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    peak_combine(best, bi, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o));
+  __shared__ float sv[kRedThreads / 32];
+  __shared__ int   si[kRedThreads / 32];
+  if ((threadIdx.x & 31) == 0)
+    sv[threadIdx.x >> 5] = best, si[threadIdx.x >> 5] = bi;
   __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st) {
-      const float v2 = sv[threadIdx.x + st];
-      const int   i2 = si[threadIdx.x + st];
-      if (i2 != INT_MAX && (si[threadIdx.x] == INT_MAX || v2 > sv[threadIdx.x] || (v2 == sv[threadIdx.x] && i2 < si[threadIdx.x])))
-        sv[threadIdx.x] = v2, si[threadIdx.x] = i2;
-    }
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    best = threadIdx.x < B / 32 ? sv[threadIdx.x] : -FLT_MAX;
+    bi   = threadIdx.x < B / 32 ? si[threadIdx.x] : INT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      peak_combine(best, bi, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o));
+    if (threadIdx.x == 0)
+      si[0] = bi;
   }
+  __syncthreads();
   if (threadIdx.x == 0) {
     const int p  = si[0] == INT_MAX ? 0 : si[0];
     const int py = p / w, px = p - py * w;
@@ -1322,6 +1359,7 @@ struct hf_shslopes {
   DevPlan  pw, ph;
   float2  *spec = nullptr, *cross = nullptr, *shifts = nullptr;
   float   *means = nullptr, *maps = nullptr;
+  float   *taper = nullptr; // [h][w]: the ROI's cosine taper inside the ellipse, -1 outside
   uint8_t *active = nullptr;
   std::vector<uint8_t> active_host;
   // FullPairwise mode: pairs (i < j) of active samples in the reference's edge order, processed
@@ -1341,7 +1379,7 @@ void release(hf_shslopes *p) {
     return;
   release(p->pw), release(p->ph);
   cudaFree(p->spec), cudaFree(p->cross), cudaFree(p->shifts);
-  cudaFree(p->means), cudaFree(p->maps), cudaFree(p->active);
+  cudaFree(p->means), cudaFree(p->maps), cudaFree(p->taper), cudaFree(p->active);
   cudaFree(p->pair_src), cudaFree(p->pair_dst), cudaFree(p->pair_srank), cudaFree(p->pair_drank);
   cudaFree(p->active_dense), cudaFree(p->pcross), cudaFree(p->pshift), cudaFree(p->rhs), cudaFree(p->pmaps);
   delete p;
@@ -1412,6 +1450,13 @@ int hf_shslopes_create_mode(int sy, int sx, int height, int width, int sub_h, in
     rc = cuda_status(cudaMalloc(&p->maps, px * sizeof(float)), "ShackHartmannSlopes: maps");
   if (rc == HF_OK)
     rc = cuda_status(cudaMalloc(&p->means, (size_t)p->count * sizeof(float)), "ShackHartmannSlopes: means");
+  if (rc == HF_OK)
+    rc = cuda_status(cudaMalloc(&p->taper, (size_t)height * width * sizeof(float)), "ShackHartmannSlopes: ROI taper");
+  if (rc == HF_OK) {
+    shk_roi_taper_kernel<<<grid_1d((int64_t)height * width), 256, 0, s>>>(p->taper, height, width, p->roi);
+    note_launch();
+    rc = launch_status("shk_roi_taper_kernel");
+  }
   if (rc == HF_OK)
     rc = cuda_status(cudaMalloc(&p->shifts, (size_t)p->count * sizeof(float2)), "ShackHartmannSlopes: shifts");
   if (rc == HF_OK)
@@ -1494,13 +1539,13 @@ int hf_shslopes_exec(hf_shslopes *p, const float *images, float *slopes, float *
   HF_CHECK_ARG(p != nullptr && images != nullptr && slopes != nullptr, "ShackHartmannSlopes: null argument");
   const int64_t rows = (int64_t)p->count * p->h;
   float        *mo   = maps ? maps : p->maps;
-  shk_roi_mean_kernel<<<p->count, kRedThreads, 0, s>>>(images, p->means, p->h, p->w, p->roi);
+  shk_roi_mean_kernel<<<p->count, kRedThreads, 0, s>>>(images, p->means, p->h, p->w, p->taper);
   note_launch();
   HF_TRY(launch_status("shk_roi_mean_kernel"));
   // forward transform of the prepared images: rows (mean removal + taper fused), then columns
   RowArgs ra{};
   ra.pl = p->pw.pl, ra.n = p->pw.n, ra.tw = p->pw.tw, ra.n_rows = rows, ra.inv = false, ra.out = p->spec;
-  ra.img = images, ra.means = p->means, ra.roi = p->roi, ra.h = p->h;
+  ra.img = images, ra.means = p->means, ra.taper = p->taper, ra.h = p->h;
   HF_TRY(launch_rows<ROW_XPACK>(ra, s));
   ColArgs ca{};
   ca.pl = p->ph.pl, ca.h = p->ph.n, ca.tw = p->ph.tw, ca.w = p->w, ca.inv = false, ca.in = p->spec, ca.outc = p->spec;
