@@ -1077,19 +1077,26 @@ __device__ __forceinline__ float zernike_value(int noll, float x, float y) {
 // zernike_phase_kernel (zernike_phase.cu:151-180): every pixel, pupil of radius min(ny, nx) / 2
 // centred on the grid.  `accumulate` adds the phase to `phase` (the cumulative map of repeated
 // passes) instead of overwriting it.
+// Rows over blockIdx.y, columns over the threads: no index division per pixel.
 __global__ void shk_zernike_phase_kernel(const float *coeffs, ZModes zm, int ny, int nx, float *phase, float *cumulative) {
-  const int64_t n  = (int64_t)ny * nx;
-  const float   cy = ((float)ny - 1.0f) * 0.5f, cx = ((float)nx - 1.0f) * 0.5f;
-  const float   r  = 0.5f * (float)(ny < nx ? ny : nx);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int   yi = (int)(i / nx), xi = (int)(i % nx);
-    const float x = ((float)xi - cx) / r, y = ((float)yi - cy) / r;
-    float       ph = 0.f;
-    for (int m = 0; m < zm.n; ++m)
-      ph += coeffs[m] * zernike_value(zm.idx[m], x, y);
-    phase[i] = ph;
-    if (cumulative)
-      cumulative[i] += ph;
+  const float cy = ((float)ny - 1.0f) * 0.5f, cx = ((float)nx - 1.0f) * 0.5f;
+  const float r  = 0.5f * (float)(ny < nx ? ny : nx);
+  float       c[kShkMaxModes];
+#pragma unroll
+  for (int m = 0; m < kShkMaxModes; ++m)
+    c[m] = m < zm.n ? coeffs[m] : 0.f;
+  for (int yi = blockIdx.y; yi < ny; yi += gridDim.y) {
+    const float y = ((float)yi - cy) / r;
+    for (int xi = blockIdx.x * blockDim.x + threadIdx.x; xi < nx; xi += gridDim.x * blockDim.x) {
+      const float   x  = ((float)xi - cx) / r;
+      float         ph = 0.f;
+      for (int m = 0; m < zm.n; ++m)
+        ph += c[m] * zernike_value(zm.idx[m], x, y);
+      const int64_t i = (int64_t)yi * nx + xi;
+      phase[i]        = ph;
+      if (cumulative)
+        cumulative[i] += ph;
+    }
   }
 }
 
@@ -1804,7 +1811,8 @@ int hf_zernike_phase(const float *coeffs, const int *indexes, int n_indexes, int
   zm.n = n_indexes;
   for (int i = 0; i < n_indexes; ++i)
     zm.idx[i] = indexes[i];
-  shk_zernike_phase_kernel<<<grid_1d((int64_t)ny * nx), 256, 0, s>>>(coeffs, zm, ny, nx, phase, cumulative);
+  const dim3 zg((unsigned)std::min(4, (nx + 255) / 256), (unsigned)std::min(ny, 65535));
+  shk_zernike_phase_kernel<<<zg, 256, 0, s>>>(coeffs, zm, ny, nx, phase, cumulative);
   note_launch();
   return launch_status("shk_zernike_phase_kernel");
 }
