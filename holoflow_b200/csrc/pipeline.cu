@@ -110,6 +110,12 @@ struct hf_plan {
   float2 *f2d      = nullptr; // [H][W] annulus mask in natural frequency order
   // Shack-Hartmann autofocus on every window's band planes before the lens (graph_builder.cc:139-153)
   hf_autofocus *af       = nullptr;
+  // without a sliding average across windows (pp_accumulation <= 1) the windows' measurements are
+  // independent: odd windows take a second instance on a side stream, so one window's slopes and
+  // fit (small, latency-bound kernels) run beside the next window's sub-aperture transforms
+  hf_autofocus *af2      = nullptr;
+  cudaStream_t  af_side  = nullptr;
+  cudaEvent_t   af_fork = nullptr, af_join = nullptr;
   float2       *lens_af  = nullptr; // [H][W] lens with the window's correction folded in
   float        *af_coeff = nullptr; // [max_batch][9] coefficients of the last exec
   // pp_accumulation > 1: the raw band planes of the last af_delay windows of the sequence (the
@@ -124,7 +130,15 @@ struct hf_plan {
 static void plan_free(hf_plan *p) {
   AllocScope scope(p->alloc.pool, p->alloc.stream); // free the way the buffers were allocated
   hf_autofocus_destroy(p->af);
-  p->af = nullptr;
+  hf_autofocus_destroy(p->af2);
+  p->af = p->af2 = nullptr;
+  if (p->af_side)
+    cudaStreamDestroy(p->af_side);
+  if (p->af_fork)
+    cudaEventDestroy(p->af_fork);
+  if (p->af_join)
+    cudaEventDestroy(p->af_join);
+  p->af_side = nullptr, p->af_fork = p->af_join = nullptr;
   dev_free(p->lens_af);
   dev_free(p->af_coeff);
   dev_free(p->af_hist[0]);
@@ -318,17 +332,28 @@ static int phase_after_band(hf_plan *p, int nwin, float *out, cudaStream_t s, bo
       // per window: passes 1..n-1 correct the planes in place, the last pass's correction is
       // folded into the lens of the window's row pass (no extra read and write of the planes)
       rec = p->timer.begin(s, ST_AUTOFOCUS);
+      const bool two = p->af2 != nullptr && nwin > 1; // odd windows on the second instance
+      if (two) {
+        HF_CUDA(cudaEventRecord(p->af_fork, s));
+        HF_CUDA(cudaStreamWaitEvent(p->af_side, p->af_fork, 0));
+      }
       for (int w = 0; w < nwin; ++w) {
-        float2 *planes = p->band + w * win_px;
-        HF_TRY(autofocus_begin(p->af, s));
-        for (int pass = 0; pass < autofocus_passes(p->af); ++pass) {
-          HF_TRY(autofocus_measure(p->af, planes, s));
-          if (pass + 1 < autofocus_passes(p->af))
-            HF_TRY(autofocus_correct(p->af, planes, planes, s));
+        float2            *planes = p->band + w * win_px;
+        hf_autofocus      *a      = two && (w & 1) ? p->af2 : p->af;
+        const cudaStream_t q      = two && (w & 1) ? p->af_side : s;
+        HF_TRY(autofocus_begin(a, q));
+        for (int pass = 0; pass < autofocus_passes(a); ++pass) {
+          HF_TRY(autofocus_measure(a, planes, q));
+          if (pass + 1 < autofocus_passes(a))
+            HF_TRY(autofocus_correct(a, planes, planes, q));
         }
-        HF_TRY(autofocus_fold_lens(p->af, p->lens, p->lens_af + (int64_t)w * p->P, s));
-        HF_CUDA(cudaMemcpyAsync(p->af_coeff + 9 * w, autofocus_cumulative_coeffs(p->af), 9 * sizeof(float),
-                                cudaMemcpyDeviceToDevice, s));
+        HF_TRY(autofocus_fold_lens(a, p->lens, p->lens_af + (int64_t)w * p->P, q));
+        HF_CUDA(cudaMemcpyAsync(p->af_coeff + 9 * w, autofocus_cumulative_coeffs(a), 9 * sizeof(float),
+                                cudaMemcpyDeviceToDevice, q));
+      }
+      if (two) {
+        HF_CUDA(cudaEventRecord(p->af_join, p->af_side));
+        HF_CUDA(cudaStreamWaitEvent(s, p->af_join, 0));
       }
       p->timer.end(s, rec);
       // Window w's correction applies to window w - dl (dl = 0 without pp_accumulation).  The
@@ -521,6 +546,23 @@ int hf_plan_create(const hf_desc *desc, hf_plan **out, hf_stream_t stream) {
                                             d.autofocus_roi_radius > 0.f ? d.autofocus_roi_radius : 0.5f,
                                             d.autofocus_keep_outside ? 0 : 1, d.lambda, d.pitch, d.z, stream)))
         break;
+      if (d.autofocus_pp_accumulation <= 1 && B > 1) { // the second instance for odd windows
+        if ((rc = hf_autofocus_create(p->nz, d.height, d.width, d.autofocus_nb_subaps, std::max(1, d.autofocus_n_iter),
+                                      d.lambda, d.pitch, d.z,
+                                      d.autofocus_roi_radius > 0.f ? d.autofocus_roi_radius : 0.5f,
+                                      d.autofocus_keep_outside ? 0 : 1, d.autofocus_orders, d.autofocus_n_orders,
+                                      d.autofocus_flatfield_period, stream, &p->af2)))
+          break;
+        if (d.autofocus_full_pairwise &&
+            (rc = hf_autofocus_set_slope_mode(p->af2, HF_SHSLOPES_FULL_PAIRWISE, 256,
+                                              d.autofocus_roi_radius > 0.f ? d.autofocus_roi_radius : 0.5f,
+                                              d.autofocus_keep_outside ? 0 : 1, d.lambda, d.pitch, d.z, stream)))
+          break;
+        if ((rc = cuda_status(cudaStreamCreateWithFlags(&p->af_side, cudaStreamNonBlocking), "autofocus stream")) ||
+            (rc = cuda_status(cudaEventCreateWithFlags(&p->af_fork, cudaEventDisableTiming), "autofocus event")) ||
+            (rc = cuda_status(cudaEventCreateWithFlags(&p->af_join, cudaEventDisableTiming), "autofocus event")))
+          break;
+      }
       if (d.autofocus_pp_accumulation > 1) {
         if ((rc = hf_autofocus_set_accumulation(p->af, d.autofocus_pp_accumulation, stream)))
           break;
@@ -621,6 +663,8 @@ int hf_plan_set_z(hf_plan *p, float z, hf_stream_t s) {
   HF_TRY(plan_tables(p, s));
   if (p->af) // the sub-aperture transform's input lens depends on z; the slopes and the fit do not
     HF_TRY(autofocus_set_z(p->af, z, s));
+  if (p->af2)
+    HF_TRY(autofocus_set_z(p->af2, z, s));
   return HF_OK;
 }
 
@@ -688,6 +732,8 @@ int hf_plan_autofocus_reset(hf_plan *p, hf_stream_t s) {
   p->af_seq = 0;
   if (p->af)
     HF_TRY(hf_autofocus_reset(p->af, s));
+  if (p->af2)
+    HF_TRY(hf_autofocus_reset(p->af2, s));
   return HF_OK;
 }
 
