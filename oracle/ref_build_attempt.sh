@@ -30,11 +30,17 @@ FILES=(src/holotask/src/syncs/fresnel_diffraction.cu src/holotask/src/syncs/angu
        src/holotask/src/syncs/pca.cc src/holotask/src/syncs/pca_heev.cc
        src/holonp/src/fft.cu src/holonp/src/rfft.cu src/holonp/src/mean.cu
        src/holoflow/src/core/tasks.cc src/holoflow/src/core/tensor.cc)
+# The syncs use logger() and HOLOVIBES_CHECK without including their headers (the reference's
+# CMake build supplies them); force-include both so the attempt reaches the next error.
+PRE=()
+for h in "$REF/src/holotask/src/logger.hh" "$REF/src/holotask/src/bug.hh"; do
+  if [ -f "$h" ]; then PRE+=(-include "$h"); fi
+done
 fail=0
 for f in "${FILES[@]}"; do
   obj="$OUT/$(basename "$f").o"
   one="$OUT/$(basename "$f").log"
-  if nvcc -std=c++20 -x cu -gencode arch=compute_100a,code=sm_100a "${INC[@]}" -c "$REF/$f" -o "$obj" > "$one" 2>&1; then
+  if nvcc -std=c++20 -x cu -gencode arch=compute_100a,code=sm_100a "${INC[@]}" "${PRE[@]}" -c "$REF/$f" -o "$obj" > "$one" 2>&1; then
     echo "ok      $f"
   else
     fail=1
