@@ -820,9 +820,23 @@ __global__ void shk_roi_taper_kernel(float *taper, int h, int w, Roi roi) {
 __global__ void __launch_bounds__(kRedThreads) shk_roi_mean_kernel(const float *img, float *means, int h, int w,
                                                                     const float *taper) {
   const float *im = img + (int64_t)blockIdx.x * h * w;
+  const int    N = h * w, B = blockDim.x;
   float        sum = 0.f;
   int          cnt = 0;
-  for (int i = threadIdx.x; i < h * w; i += blockDim.x) {
+  int          i   = threadIdx.x;
+  for (; i + 3 * B < N; i += 4 * B) { // four elements' loads in flight, summed in index order
+    float tp[4], v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      tp[u] = taper[i + u * B], v[u] = im[i + u * B];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (tp[u] >= 0.f) {
+        sum += v[u];
+        ++cnt;
+      }
+  }
+  for (; i < N; i += B) {
     if (taper[i] >= 0.f) {
       sum += im[i];
       ++cnt;
